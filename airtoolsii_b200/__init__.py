@@ -1,0 +1,20 @@
+"""B200-native engine for the AIR Tools II SIRT/ART hot path.
+
+Public API mirrors the reference MATLAB toolbox: ``sirt``/``art`` and the
+method wrappers, the ``paralleltomo``/``fanlineartomo`` test problems and the
+afun operator handle.  All iterations run in libairt.so (hand-written CUDA for
+sm_100a); the package raises on import if the library is missing.
+"""
+from ._lib import AirtError, lib as _load_lib
+from .afun import AirtOperator, afun_matrix, as_operator
+from .solvers import (art, calczeta, cav, cimmino, drop, kaczmarz, landweber, randkaczmarz,
+                      sart, sirt, symkaczmarz)
+from .testprobs import (add_noise, cosd, fanlineartomo, paralleltomo, phantomgallery,
+                        random_ellipses, sind)
+
+_load_lib()
+
+__all__ = ["AirtError", "AirtOperator", "afun_matrix", "as_operator", "art", "calczeta", "cav",
+           "cimmino", "drop", "kaczmarz", "landweber", "randkaczmarz", "sart", "sirt",
+           "symkaczmarz", "add_noise", "cosd", "fanlineartomo", "paralleltomo",
+           "phantomgallery", "random_ellipses", "sind"]

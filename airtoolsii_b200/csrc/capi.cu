@@ -1,0 +1,354 @@
+// extern "C" entry points of libairt (declared in include/airt.h).  Each one
+// converts C++ exceptions into a status code plus a thread-local message.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace airt {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+void prof_begin(Problem &P, int which, cudaEvent_t *ev0) {
+  (void)which;
+  *ev0 = nullptr;
+  if (!P.profiling) return;
+  cudaEvent_t e;
+  if (P.ev_pool.empty()) {
+    AIRT_CHECK_CUDA(cudaEventCreate(&e));
+  } else {
+    e = P.ev_pool.back();
+    P.ev_pool.pop_back();
+  }
+  AIRT_CHECK_CUDA(cudaEventRecord(e, P.stream));
+  *ev0 = e;
+}
+
+void prof_end(Problem &P, int which, cudaEvent_t ev0) {
+  if (!P.profiling || !ev0) return;
+  cudaEvent_t e;
+  if (P.ev_pool.empty()) {
+    AIRT_CHECK_CUDA(cudaEventCreate(&e));
+  } else {
+    e = P.ev_pool.back();
+    P.ev_pool.pop_back();
+  }
+  AIRT_CHECK_CUDA(cudaEventRecord(e, P.stream));
+  P.ev_pending.push_back({which, {ev0, e}});
+}
+
+void prof_collect(Problem &P) {
+  if (P.ev_pending.empty()) return;
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  for (auto &it : P.ev_pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, it.second.first, it.second.second);
+    P.prof_ms[it.first] += ms;
+    P.prof_launches[it.first] += 1;
+    P.ev_pool.push_back(it.second.first);
+    P.ev_pool.push_back(it.second.second);
+  }
+  P.ev_pending.clear();
+}
+
+static Problem *new_problem() {
+  Problem *P = new Problem();
+  cudaError_t e = cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete P;
+    set_error("cudaStreamCreate failed: %s", cudaGetErrorString(e));
+    throw Status{AIRT_ERR_CUDA};
+  }
+  return P;
+}
+
+static void free_problem(Problem *P) {
+  if (!P) return;
+  if (P->stream) cudaStreamSynchronize(P->stream);
+  for (auto &it : P->ev_pending) {
+    cudaEventDestroy(it.second.first);
+    cudaEventDestroy(it.second.second);
+  }
+  for (auto e : P->ev_pool) cudaEventDestroy(e);
+  if (P->h_state) cudaFreeHost(P->h_state);
+  cudaStream_t s = P->stream;
+  delete P;
+  if (s) cudaStreamDestroy(s);
+}
+
+}  // namespace airt
+
+using namespace airt;
+
+#define AIRT_API_BEGIN try {
+#define AIRT_API_END                                   \
+  }                                                    \
+  catch (const airt::Status &st) {                     \
+    return st.code;                                    \
+  }                                                    \
+  catch (const std::bad_alloc &) {                     \
+    airt::set_error("host allocation failed");         \
+    return AIRT_ERR_OOM;                               \
+  }                                                    \
+  catch (...) {                                        \
+    airt::set_error("unexpected internal error");      \
+    return AIRT_ERR_CUDA;                              \
+  }                                                    \
+  return AIRT_OK;
+
+extern "C" {
+
+const char *airt_last_error(void) { return g_last_error.c_str(); }
+
+int airt_version(void) { return 10000; }
+
+int airt_problem_from_csc(int64_t m, int64_t n, const uint64_t *jc, const uint64_t *ir,
+                          const double *pr, airt_problem **out) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(out && jc, "null pointer argument");
+  AIRT_REQUIRE(m >= 0 && n >= 0 && m < INT32_MAX && n < INT32_MAX, "matrix size out of range");
+  const int64_t nnz = (int64_t)jc[n];
+  AIRT_REQUIRE(jc[0] == 0, "jc[0] must be 0");
+  for (int64_t j = 0; j < n; ++j) AIRT_REQUIRE(jc[j + 1] >= jc[j], "jc must be nondecreasing");
+  AIRT_REQUIRE(nnz == 0 || (ir && pr), "null pointer argument");
+  Problem *P = new_problem();
+  try {
+    P->m = m;
+    P->n = n;
+    P->nnz = nnz;
+    build_csr_from_host_csc(*P, jc, ir, pr);
+  } catch (...) {
+    free_problem(P);
+    throw;
+  }
+  *out = reinterpret_cast<airt_problem *>(P);
+  AIRT_API_END
+}
+
+static int make_geometry(int kind, int N, int nA, const double *cos_t, const double *sin_t, int p,
+                         const double *offsets, const double *cos_w, const double *sin_w, double R,
+                         int matrix_free, airt_problem **out) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(out && cos_t && sin_t, "null pointer argument");
+  AIRT_REQUIRE(N >= 1 && N <= 46340 && nA >= 0 && p >= 0, "geometry size out of range");
+  AIRT_REQUIRE((int64_t)nA * p < INT32_MAX, "too many rays");
+  Problem *P = new_problem();
+  try {
+    P->geo_kind = kind;
+    P->N = N;
+    P->nA = nA;
+    P->p = p;
+    P->R = R;
+    P->m = (int64_t)nA * p;
+    P->n = (int64_t)N * N;
+    P->matrix_free = matrix_free != 0;
+    P->cos_t.upload(cos_t, nA, P->stream);
+    P->sin_t.upload(sin_t, nA, P->stream);
+    if (kind == GEO_PARALLEL) {
+      AIRT_REQUIRE(offsets || p == 0, "null pointer argument");
+      P->offsets.upload(offsets, p, P->stream);
+    } else {
+      AIRT_REQUIRE((cos_w && sin_w) || p == 0, "null pointer argument");
+      AIRT_REQUIRE(R >= std::sqrt(2.0) / 2.0 * N, "R must be greater than half squareroot 2");
+      P->cos_w.upload(cos_w, p, P->stream);
+      P->sin_w.upload(sin_w, p, P->stream);
+    }
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
+    if (!P->matrix_free) generate_matrix(*P);
+  } catch (...) {
+    free_problem(P);
+    throw;
+  }
+  *out = reinterpret_cast<airt_problem *>(P);
+  AIRT_API_END
+}
+
+int airt_problem_parallel(int N, int nA, const double *cos_t, const double *sin_t, int p,
+                          const double *offsets, int matrix_free, airt_problem **out) {
+  return make_geometry(GEO_PARALLEL, N, nA, cos_t, sin_t, p, offsets, nullptr, nullptr, 0.0,
+                       matrix_free, out);
+}
+
+int airt_problem_fan(int N, int nA, const double *cos_t, const double *sin_t, int p,
+                     const double *cos_w, const double *sin_w, double R, int matrix_free,
+                     airt_problem **out) {
+  return make_geometry(GEO_FAN, N, nA, cos_t, sin_t, p, nullptr, cos_w, sin_w, R, matrix_free, out);
+}
+
+int airt_problem_size(const airt_problem *h, int64_t *m, int64_t *n, int64_t *nnz) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h, "null problem handle");
+  const Problem *P = reinterpret_cast<const Problem *>(h);
+  if (m) *m = P->m;
+  if (n) *n = P->n;
+  if (nnz) *nnz = P->matrix_free ? -1 : P->nnz;
+  AIRT_API_END
+}
+
+int airt_problem_stream(const airt_problem *h, void **cuda_stream) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && cuda_stream, "null pointer argument");
+  *cuda_stream = (void *)reinterpret_cast<const Problem *>(h)->stream;
+  AIRT_API_END
+}
+
+int airt_problem_export_csc(airt_problem *h, uint64_t *jc, uint64_t *ir, double *pr) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && jc, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  AIRT_REQUIRE(P->nnz == 0 || (ir && pr), "null pointer argument");
+  export_csc(*P, jc, ir, pr);
+  AIRT_API_END
+}
+
+int airt_destroy(airt_problem *h) {
+  AIRT_API_BEGIN
+  free_problem(reinterpret_cast<Problem *>(h));
+  AIRT_API_END
+}
+
+int airt_apply(airt_problem *h, const double *in, double *out, int transp) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && in && out, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  const int64_t nin = transp ? P->m : P->n, nout = transp ? P->n : P->m;
+  P->vin.upload(in, nin, P->stream);
+  P->vout.ensure(nout);
+  apply_operator(*P, P->vin.p, P->vout.p, transp);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(out, P->vout.p, nout * sizeof(double), cudaMemcpyDeviceToHost,
+                                  P->stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
+  AIRT_API_END
+}
+
+int airt_apply_device(airt_problem *h, const double *d_in, double *d_out, int transp) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && d_in && d_out, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  apply_operator(*P, d_in, d_out, transp);
+  AIRT_API_END
+}
+
+int airt_weights(airt_problem *h, int method, double *M, double *D) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && M && D, "null pointer argument");
+  AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  P->M.ensure(P->m);
+  P->D.ensure(P->n);
+  compute_weights(*P, method, P->M.p, P->D.p);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(M, P->M.p, P->m * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(D, P->D.p, P->n * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
+  AIRT_API_END
+}
+
+int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *Dcustom, double tol,
+             int maxit, double *rho) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && rho, "null pointer argument");
+  AIRT_REQUIRE(maxit > 0 && tol >= 0, "invalid tolerance or iteration limit");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  P->M.ensure(P->m);
+  P->D.ensure(P->n);
+  if (method == AIRT_CUSTOM) {
+    std::vector<double> ones;
+    if (Mcustom) P->M.upload(Mcustom, P->m, P->stream);
+    else {
+      ones.assign(P->m, 1.0);
+      P->M.upload(ones.data(), P->m, P->stream);
+    }
+    if (Dcustom) P->D.upload(Dcustom, P->n, P->stream);
+    else {
+      ones.assign(P->n, 1.0);
+      P->D.upload(ones.data(), P->n, P->stream);
+    }
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
+  } else {
+    AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+    compute_weights(*P, method, P->M.p, P->D.p);
+  }
+  *rho = estimate_rho(*P, P->M.p, P->D.p, tol, maxit);
+  AIRT_API_END
+}
+
+int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *d_b,
+                     const double *d_x0, const int64_t *K, int64_t nK, double *d_X,
+                     double *resnorms, airt_info *info) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && opts && d_b && d_X, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  run_sirt(*P, *opts, d_b, d_x0, K, nK, d_X, resnorms, info);
+  AIRT_API_END
+}
+
+int airt_sirt(airt_problem *h, const airt_sirt_opts *opts, const double *b, const double *x0,
+              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && opts && b && X, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  cudaStream_t s = P->stream;
+  P->b64.upload(b, P->m, s);
+  if (x0) P->vin.upload(x0, P->n, s);
+  P->Xd.ensure((size_t)P->n * (nK > 0 ? nK : 1));
+  airt_info inf{};
+  run_sirt(*P, *opts, P->b64.p, x0 ? P->vin.p : nullptr, K, nK, P->Xd.p, resnorms, &inf);
+  if (inf.nsaved)
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(X, P->Xd.p, (size_t)inf.nsaved * P->n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (info) *info = inf;
+  AIRT_API_END
+}
+
+int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const double *x0,
+             const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && opts && b && X, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  cudaStream_t s = P->stream;
+  P->b64.upload(b, P->m, s);
+  if (x0) P->vin.upload(x0, P->n, s);
+  P->Xd.ensure((size_t)P->n * (nK > 0 ? nK : 1));
+  airt_info inf{};
+  run_art(*P, *opts, P->b64.p, x0 ? P->vin.p : nullptr, K, nK, P->Xd.p, resnorms, &inf);
+  if (inf.nsaved)
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(X, P->Xd.p, (size_t)inf.nsaved * P->n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (info) *info = inf;
+  AIRT_API_END
+}
+
+int airt_profile_enable(airt_problem *h, int on) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h, "null problem handle");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  prof_collect(*P);
+  P->profiling = on != 0;
+  P->prof_launches[0] = P->prof_launches[1] = 0;
+  P->prof_ms[0] = P->prof_ms[1] = 0;
+  AIRT_API_END
+}
+
+int airt_profile_read(airt_problem *h, int which, int64_t *launches, double *total_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && which >= 0 && which < 2, "invalid argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  prof_collect(*P);
+  if (launches) *launches = P->prof_launches[which];
+  if (total_ms) *total_ms = P->prof_ms[which];
+  AIRT_API_END
+}
+
+}  // extern "C"

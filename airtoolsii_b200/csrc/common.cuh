@@ -1,0 +1,236 @@
+// Internal types of libairt: device buffers, the problem handle, error
+// plumbing and small device helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/airt.h"
+
+namespace airt {
+
+// ---------------------------------------------------------------- errors
+struct Status {
+  int code;
+};
+
+void set_error(const char *fmt, ...);
+
+#define AIRT_CHECK_CUDA(call)                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      ::airt::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                         \
+      throw ::airt::Status{e_ == cudaErrorMemoryAllocation ? AIRT_ERR_OOM : AIRT_ERR_CUDA}; \
+    }                                                                                      \
+  } while (0)
+
+#define AIRT_REQUIRE(cond, ...)      \
+  do {                               \
+    if (!(cond)) {                   \
+      ::airt::set_error(__VA_ARGS__); \
+      throw ::airt::Status{AIRT_ERR_ARG}; \
+    }                                \
+  } while (0)
+
+#define AIRT_LAUNCH_CHECK() AIRT_CHECK_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------- buffers
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  // Grow-only allocation; contents are not preserved.
+  void ensure(size_t count) {
+    if (count <= n && p) return;
+    release();
+    size_t bytes = (count ? count : 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error("cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+      throw Status{AIRT_ERR_OOM};
+    }
+    n = count;
+  }
+  void upload(const T *host, size_t count, cudaStream_t s) {
+    ensure(count);
+    if (count)
+      AIRT_CHECK_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+};
+
+// ---------------------------------------------------------------- geometry
+enum GeoKind { GEO_NONE = 0, GEO_PARALLEL = 1, GEO_FAN = 2 };
+
+// Per-ray parameters of both geometries, prepared on the device:
+// ray r = angle*p + j starts at (x0t, y0t) with direction (a, b).
+struct RayGeom {
+  int kind;
+  int N, nA, p;
+  double R;
+  const double *cos_t, *sin_t;  // nA
+  const double *offsets;         // p (parallel)
+  const double *cos_w, *sin_w;  // p (fan)
+};
+
+// ---------------------------------------------------------------- SIRT state
+// Device-resident iteration state.  The control kernel is its only writer
+// between kernels; all other kernels only read it (and add to acc[]).
+struct SirtState {
+  int iter;       // iteration whose residual the next control step judges
+  int stop;       // 1 once a stopping rule fired
+  int stoprule;   // info.stoprule
+  int finaliter;  // info.finaliter
+  double acc[6];  // [0] sum r^2  [1] sum r.*M.*r  [2] sum rprev^2  [3] sum rprev.*r
+                  // [4] sum D.*g.^2 (line search)
+  double lam_cur; // relaxpar applied in the iteration being computed
+  double lam_last;
+  double rmr_prev;  // r'*M*r of the previous residual (line search numerator)
+};
+
+struct SirtParams {
+  int64_t kmax;
+  int stoprule;
+  double taudelta;
+  int relax_kind;
+  double relaxpar;
+  const double *relax_table;  // device, kmax entries
+  double *resn_hist;          // device, kmax+1
+  double *lam_hist;           // device, kmax+1
+};
+
+// ---------------------------------------------------------------- problem
+struct Problem {
+  int64_t m = 0, n = 0, nnz = 0;
+  bool matrix_free = false;
+  int geo_kind = GEO_NONE;
+  int N = 0, nA = 0, p = 0;
+  double R = 0;
+  DevBuf<double> cos_t, sin_t, offsets, cos_w, sin_w;
+
+  // stored matrix: CSR over rays (rows) and CSC over pixels (columns)
+  DevBuf<int64_t> rp, cp;
+  DevBuf<int> ci, ri;
+  DevBuf<float> rv, cv;
+
+  cudaStream_t stream = nullptr;
+
+  // solver work vectors
+  DevBuf<double> x64, r64, rprev, g64, b64, M, D, lbv, ubv, vin, vout, table, resn, lamh, Xd;
+  DevBuf<float> x32, mr32;
+  DevBuf<SirtState> state;
+  DevBuf<SirtParams> params;
+  DevBuf<int> save_slot;
+  SirtState *h_state = nullptr;  // pinned mirror
+
+  // instrumentation
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  int64_t prof_launches[2] = {0, 0};
+  double prof_ms[2] = {0, 0};
+
+  RayGeom geom() const {
+    RayGeom g;
+    g.kind = geo_kind;
+    g.N = N;
+    g.nA = nA;
+    g.p = p;
+    g.R = R;
+    g.cos_t = cos_t.p;
+    g.sin_t = sin_t.p;
+    g.offsets = offsets.p;
+    g.cos_w = cos_w.p;
+    g.sin_w = sin_w.p;
+    return g;
+  }
+};
+
+// ---------------------------------------------------------------- helpers
+inline int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+inline unsigned grid_for(int64_t work, int per_block, int blocks_per_sm = 8) {
+  int64_t need = (work + per_block - 1) / per_block;
+  int64_t cap = (int64_t)num_sms() * blocks_per_sm;
+  if (need < 1) need = 1;
+  return (unsigned)(need < cap ? need : cap);
+}
+
+// Profiling brackets around one kernel launch (no-ops unless enabled).
+void prof_begin(Problem &P, int which, cudaEvent_t *ev0);
+void prof_end(Problem &P, int which, cudaEvent_t ev0);
+void prof_collect(Problem &P);
+
+// Kernel drivers implemented in the .cu files.
+void build_csc_from_csr(Problem &P);
+void build_csr_from_host_csc(Problem &P, const uint64_t *jc, const uint64_t *ir, const double *pr);
+void generate_matrix(Problem &P);
+void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
+void compute_weights(Problem &P, int method, double *dM, double *dD);
+void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const double *d_x0,
+              const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
+void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double *d_x0,
+             const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
+double estimate_rho(Problem &P, const double *dM, const double *dD, double tol, int maxit);
+void export_csc(Problem &P, uint64_t *jc, uint64_t *ir, double *pr);
+
+// Exclusive scan of counts[0..n) into offs[0..n] (offs[n] = total), device.
+void exclusive_scan_i64(const int64_t *counts, int64_t *offs, int64_t n, cudaStream_t s);
+
+}  // namespace airt
+
+// ------------------------------------------------------------ device helpers
+__device__ __forceinline__ double warp_sum(double v, unsigned mask = 0xffffffffu) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+  return v;
+}
+
+template <int LANES>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, LANES);
+  return v;
+}
+
+// Block-wide sum of one double per thread; result valid in thread 0.
+template <int THREADS>
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[THREADS / 32];
+  v = warp_sum(v);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = (l < THREADS / 32) ? sh[l] : 0.0;
+    t = warp_sum(t);
+  }
+  __syncthreads();
+  return t;
+}

@@ -1,0 +1,588 @@
+// SIRT iteration on the GPU:  x <- P_C(x + lambda_k * D .* A'*(M .* (b - A*x)))
+// (sirt/sirt.m:198-261) with the stopping rules of
+// auxil/check_stoprules.m:54-94,153-161 evaluated on the device.
+//
+// Per iteration k the stream runs
+//   bwd : g = A'*(M.*r) over the CSC (gather of the FP32 copy of M.*r),
+//         fused with x += lambda*D.*g, the box projection (sirt.m:232-237),
+//         the FP32 copy of x for the next gather and the save of x into X
+//         when k is in K;
+//   fwd : r = b - A*x over the CSR (gather of the FP32 copy of x), fused
+//         with M.*r (FP32 copy for the next gather) and the FP64 sums
+//         ||r||^2, r'*M*r and, for ME, the previous-residual products;
+//   ctrl: one thread applies the stopping rule to the sums, records
+//         ||r_k|| and the relaxpar used, and selects the next relaxpar.
+// Kernels read the device stop flag first and return at once after a stop,
+// so the host can enqueue iterations in chunks and poll the flag lazily.
+//
+// Precision: matrix values and the two gathered vectors are FP32; products
+// are accumulated in FP64; x, r, b, M, D and all reductions are FP64.
+#include <cmath>
+
+#include "common.cuh"
+#include "spmv.cuh"
+#include "trace.cuh"
+
+namespace airt {
+
+void mf_backproject_f32(Problem &P, const float *u, double *g64, const int *stop_flag);
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct FwdOut {
+  const double *b;
+  const double *M;
+  float *mr32;
+  double *rprev;  // ME only
+  SirtState *st;
+};
+
+struct Acc4 {
+  double r2 = 0, rmr = 0, p2 = 0, pr = 0;
+};
+
+template <bool ME>
+__device__ __forceinline__ void resid_row(int64_t i, double s, const FwdOut &o, Acc4 &a) {
+  const double r = o.b[i] - s;
+  const double mr = o.M[i] * r;
+  o.mr32[i] = (float)mr;
+  a.r2 += r * r;
+  a.rmr += r * mr;
+  if (ME) {
+    const double p = o.rprev[i];
+    a.p2 += p * p;
+    a.pr += p * (p + r);
+    o.rprev[i] = r;
+  }
+}
+
+template <bool ME>
+__device__ __forceinline__ void flush(SirtState *st, Acc4 &a) {
+  double r2 = block_sum<kThreads>(a.r2);
+  double rmr = block_sum<kThreads>(a.rmr);
+  double p2 = 0, pr = 0;
+  if (ME) {
+    p2 = block_sum<kThreads>(a.p2);
+    pr = block_sum<kThreads>(a.pr);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&st->acc[0], r2);
+    atomicAdd(&st->acc[1], rmr);
+    if (ME) {
+      atomicAdd(&st->acc[2], p2);
+      atomicAdd(&st->acc[3], pr);
+    }
+  }
+}
+
+__device__ __forceinline__ bool stopped(const SirtState *st) {
+  return *(volatile const int *)&st->stop != 0;
+}
+
+template <int LANES, bool ME>
+__global__ void __launch_bounds__(kThreads)
+    k_sirt_fwd(int64_t m, const int64_t *__restrict__ rp, const int *__restrict__ ci,
+               const float *__restrict__ rv, const float *__restrict__ x32, FwdOut o) {
+  if (stopped(o.st)) return;
+  Acc4 a;
+  for_each_segment<LANES>(m, rp, ci, rv, x32, [&](int64_t i, double s, bool lead) {
+    if (lead) resid_row<ME>(i, s, o, a);
+  });
+  flush<ME>(o.st, a);
+}
+
+template <bool ME>
+__global__ void __launch_bounds__(128)
+    k_sirt_fwd_mf(RayGeom g, int64_t nrays, bool excl, const float *__restrict__ x32, FwdOut o) {
+  if (stopped(o.st)) return;
+  Acc4 a;
+  const int64_t nn = (int64_t)g.N * g.N;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const Ray q = ray_of(g, r);
+    double acc = 0.0;
+    trace_entries(g.N, q, excl, [&](int col, double v) {
+      if (col >= 0 && col < nn) acc = fma((double)(float)v, (double)x32[col], acc);
+    });
+    resid_row<ME>(r, acc, o, a);
+  }
+  double r2 = block_sum<128>(a.r2), rmr = block_sum<128>(a.rmr), p2 = 0, pr = 0;
+  if (ME) {
+    p2 = block_sum<128>(a.p2);
+    pr = block_sum<128>(a.pr);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&o.st->acc[0], r2);
+    atomicAdd(&o.st->acc[1], rmr);
+    if (ME) {
+      atomicAdd(&o.st->acc[2], p2);
+      atomicAdd(&o.st->acc[3], pr);
+    }
+  }
+}
+
+struct UpdArgs {
+  const double *D;
+  double *x64;
+  float *x32;
+  int lbk, ubk;
+  double lb, ub;
+  const double *lbv, *ubv;
+  double *X;
+  int64_t n;
+  const int *save_slot;
+  SirtState *st;
+  double *g64;
+};
+
+__device__ __forceinline__ void update_x(int64_t j, double g, double lam, const UpdArgs &u, int slot) {
+  double x = u.x64[j] + lam * (u.D[j] * g);
+  if (u.lbk == AIRT_BOUND_SCALAR) x = fmax(x, u.lb);
+  else if (u.lbk == AIRT_BOUND_VECTOR) x = fmax(x, u.lbv[j]);
+  if (u.ubk == AIRT_BOUND_SCALAR) x = fmin(x, u.ub);
+  else if (u.ubk == AIRT_BOUND_VECTOR) x = fmin(x, u.ubv[j]);
+  u.x64[j] = x;
+  u.x32[j] = (float)x;
+  if (slot >= 0) u.X[(int64_t)slot * u.n + j] = x;
+}
+
+// MODE 0: fused update with st->lam_cur.  MODE 1: line-search pass that
+// stores g and accumulates sum(D.*g.^2) (sirt.m:219-222).
+template <int LANES, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_sirt_bwd(int64_t n, const int64_t *__restrict__ cp, const int *__restrict__ ri,
+               const float *__restrict__ cv, const float *__restrict__ mr32, UpdArgs u) {
+  if (stopped(u.st)) return;
+  const int it = u.st->iter;
+  const int slot = u.save_slot[it];
+  const double lam = u.st->lam_cur;
+  double a4 = 0;
+  for_each_segment<LANES>(n, cp, ri, cv, mr32, [&](int64_t j, double g, bool lead) {
+    if (!lead) return;
+    if (MODE == 0) {
+      update_x(j, g, lam, u, slot);
+    } else {
+      u.g64[j] = g;
+      a4 += u.D[j] * (g * g);
+    }
+  });
+  if (MODE == 1) {
+    a4 = block_sum<kThreads>(a4);
+    if (threadIdx.x == 0) atomicAdd(&u.st->acc[4], a4);
+  }
+}
+
+// Elementwise update from a stored g (line search and matrix-free paths).
+template <bool LINE>
+__global__ void __launch_bounds__(kThreads) k_sirt_update(UpdArgs u) {
+  if (stopped(u.st)) return;
+  const int it = u.st->iter;
+  const int slot = u.save_slot[it];
+  double lam;
+  if (LINE) {
+    lam = u.st->rmr_prev / u.st->acc[4];
+  } else {
+    lam = u.st->lam_cur;
+  }
+  if (LINE && blockIdx.x == 0 && threadIdx.x == 0) u.st->lam_cur = lam;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < u.n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    update_x(j, u.g64[j], lam, u, slot);
+}
+
+// sum(D .* g.^2) for the line search on the matrix-free path.
+__global__ void __launch_bounds__(kThreads) k_dg2(int64_t n, const double *__restrict__ D,
+                                                   const double *__restrict__ g, SirtState *st) {
+  if (stopped(st)) return;
+  double a = 0;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    a += D[j] * (g[j] * g[j]);
+  a = block_sum<kThreads>(a);
+  if (threadIdx.x == 0) atomicAdd(&st->acc[4], a);
+}
+
+// Stopping rule of check_stoprules.m on the sums of the residual just
+// computed, then the relaxpar of the next iteration (sirt.m:216-226).
+__global__ void k_sirt_ctrl(SirtState *st, const SirtParams *p) {
+  if (threadIdx.x || blockIdx.x) return;
+  if (st->stop) return;
+  const int k = st->iter;
+  const double nrk = sqrt(st->acc[0]);
+  p->resn_hist[k] = nrk;
+  p->lam_hist[k] = st->lam_cur;
+  bool stop = false;
+  int rule = 0;
+  const int64_t kmax = p->kmax;
+  switch (p->stoprule) {
+    case AIRT_STOP_DP:  // check_stoprules.m:56-72
+      if (nrk <= p->taudelta || k >= kmax) {
+        stop = true;
+        rule = (k != kmax) ? 2 : 0;
+      }
+      break;
+    case AIRT_STOP_ME: {  // check_stoprules.m:74-94
+      const double np = sqrt(st->acc[2]);
+      const double dme = st->acc[3] / 2.0;
+      if (k > 0 && dme / np <= p->taudelta) {
+        stop = true;
+        rule = 3;
+      } else if (k >= kmax) {
+        stop = true;
+        rule = 0;
+      }
+      break;
+    }
+    default:  // NONE, check_stoprules.m:153-161
+      if (k >= kmax) stop = true;
+  }
+  st->rmr_prev = st->acc[1];
+  for (int q = 0; q < 6; ++q) st->acc[q] = 0.0;
+  if (stop) {
+    st->stop = 1;
+    st->stoprule = rule;
+    st->finaliter = k;
+    st->lam_last = st->lam_cur;
+  } else {
+    const int kn = k + 1;
+    if (p->relax_kind == AIRT_RELAX_CONST) st->lam_cur = p->relaxpar;
+    else if (p->relax_kind == AIRT_RELAX_TABLE) st->lam_cur = p->relax_table[kn - 1];
+    st->iter = kn;
+  }
+}
+
+__global__ void k_to_f32(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+__global__ void k_copy(int64_t n, const double *__restrict__ a, double *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+// ---------------------------------------------------------------- launchers
+template <bool ME>
+void launch_fwd_t(Problem &P, const FwdOut &o) {
+  cudaStream_t s = P.stream;
+  if (P.matrix_free) {
+    k_sirt_fwd_mf<ME><<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m,
+                                                              P.geo_kind == GEO_PARALLEL,
+                                                              P.x32.p, o);
+    return;
+  }
+  const int L = lanes_for(P.nnz, P.m);
+  const unsigned g = grid_for(P.m * L, kThreads);
+  switch (L) {
+    case 32: k_sirt_fwd<32, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    case 16: k_sirt_fwd<16, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    case 8: k_sirt_fwd<8, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    default: k_sirt_fwd<4, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+  }
+}
+
+void launch_fwd(Problem &P, const FwdOut &o, bool me) {
+  cudaEvent_t e0 = nullptr;
+  prof_begin(P, 0, &e0);
+  if (me) launch_fwd_t<true>(P, o);
+  else launch_fwd_t<false>(P, o);
+  AIRT_LAUNCH_CHECK();
+  prof_end(P, 0, e0);
+}
+
+template <int MODE>
+void launch_bwd_t(Problem &P, const UpdArgs &u) {
+  cudaStream_t s = P.stream;
+  const int L = lanes_for(P.nnz, P.n);
+  const unsigned g = grid_for(P.n * L, kThreads);
+  switch (L) {
+    case 32: k_sirt_bwd<32, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    case 16: k_sirt_bwd<16, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    case 8: k_sirt_bwd<8, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    default: k_sirt_bwd<4, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+  }
+}
+
+void launch_bwd(Problem &P, const UpdArgs &u, int relax_kind) {
+  cudaStream_t s = P.stream;
+  cudaEvent_t e0 = nullptr;
+  prof_begin(P, 1, &e0);
+  const unsigned ge = grid_for(P.n, kThreads);
+  if (P.matrix_free) {
+    mf_backproject_f32(P, P.mr32.p, P.g64.p, &P.state.p->stop);
+    if (relax_kind == AIRT_RELAX_LINE) {
+      k_dg2<<<ge, kThreads, 0, s>>>(P.n, P.D.p, P.g64.p, P.state.p);
+      k_sirt_update<true><<<ge, kThreads, 0, s>>>(u);
+    } else {
+      k_sirt_update<false><<<ge, kThreads, 0, s>>>(u);
+    }
+  } else if (relax_kind == AIRT_RELAX_LINE) {
+    launch_bwd_t<1>(P, u);
+    k_sirt_update<true><<<ge, kThreads, 0, s>>>(u);
+  } else {
+    launch_bwd_t<0>(P, u);
+  }
+  AIRT_LAUNCH_CHECK();
+  prof_end(P, 1, e0);
+}
+
+}  // namespace
+
+void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const double *d_x0,
+              const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info) {
+  cudaStream_t s = P.stream;
+  const int64_t m = P.m, n = P.n;
+  AIRT_REQUIRE(nK >= 1 && K, "Max no. of iterations must ALWAYS be specified.");
+  for (int64_t l = 1; l < nK; ++l)
+    AIRT_REQUIRE(K[l] > K[l - 1], "Elements of K must be strictly increasing.");
+  AIRT_REQUIRE(o.kmax == K[nK - 1], "kmax must equal K(end)");
+  AIRT_REQUIRE(o.kmax >= 0 && o.kmax < (int64_t)INT32_MAX, "kmax out of range");
+  AIRT_REQUIRE(K[0] >= 0, "iteration numbers must be nonnegative");
+  AIRT_REQUIRE(o.stoprule == AIRT_STOP_NONE || o.stoprule == AIRT_STOP_DP ||
+                   o.stoprule == AIRT_STOP_ME,
+               "The chosen stopping rule is not valid.");
+  AIRT_REQUIRE(o.relax_kind >= AIRT_RELAX_CONST && o.relax_kind <= AIRT_RELAX_TABLE,
+               "invalid relaxation strategy");
+  AIRT_REQUIRE(o.relax_kind != AIRT_RELAX_TABLE || o.relax_table || o.kmax == 0,
+               "relax_table required");
+  const int64_t kmax = o.kmax;
+  const bool me = o.stoprule == AIRT_STOP_ME;
+
+  cudaEvent_t t0, t1;
+  AIRT_CHECK_CUDA(cudaEventCreate(&t0));
+  AIRT_CHECK_CUDA(cudaEventCreate(&t1));
+  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
+
+  // weights (get_mfun_dfun.m)
+  P.M.ensure(m);
+  P.D.ensure(n);
+  if (o.method == AIRT_CUSTOM) {
+    std::vector<double> ones;
+    if (o.M) P.M.upload(o.M, m, s);
+    else {
+      ones.assign(m, 1.0);
+      P.M.upload(ones.data(), m, s);
+    }
+    if (o.D) P.D.upload(o.D, n, s);
+    else {
+      ones.assign(n, 1.0);
+      P.D.upload(ones.data(), n, s);
+    }
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  } else {
+    compute_weights(P, o.method, P.M.p, P.D.p);
+  }
+
+  // vectors
+  P.x64.ensure(n);
+  P.x32.ensure(n);
+  P.mr32.ensure(m);
+  if (me) P.rprev.ensure(m);
+  if (o.relax_kind == AIRT_RELAX_LINE || P.matrix_free) P.g64.ensure(n);
+  if (d_x0)
+    k_copy<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, d_x0, P.x64.p);
+  else
+    AIRT_CHECK_CUDA(cudaMemsetAsync(P.x64.p, 0, n * sizeof(double), s));
+  k_to_f32<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, P.x64.p, P.x32.p);
+  AIRT_LAUNCH_CHECK();
+  if (me) AIRT_CHECK_CUDA(cudaMemsetAsync(P.rprev.p, 0, m * sizeof(double), s));
+  if (o.lb_kind == AIRT_BOUND_VECTOR) {
+    AIRT_REQUIRE(o.lbv, "lbound vector missing");
+    P.lbv.upload(o.lbv, n, s);
+  }
+  if (o.ub_kind == AIRT_BOUND_VECTOR) {
+    AIRT_REQUIRE(o.ubv, "ubound vector missing");
+    P.ubv.upload(o.ubv, n, s);
+  }
+  if (o.relax_kind == AIRT_RELAX_TABLE && kmax > 0) P.table.upload(o.relax_table, kmax, s);
+  std::vector<int> slots(kmax + 1, -1);
+  for (int64_t l = 0; l < nK; ++l)
+    if (K[l] >= 1 && K[l] <= kmax) slots[K[l]] = (int)l;
+  P.save_slot.upload(slots.data(), kmax + 1, s);
+  P.resn.ensure(kmax + 1);
+  P.lamh.ensure(kmax + 1);
+
+  SirtState st0{};
+  st0.lam_cur = (o.relax_kind == AIRT_RELAX_CONST) ? o.relaxpar : NAN;
+  P.state.upload(&st0, 1, s);
+  SirtParams prm{};
+  prm.kmax = kmax;
+  prm.stoprule = o.stoprule;
+  prm.taudelta = o.taudelta;
+  prm.relax_kind = o.relax_kind;
+  prm.relaxpar = o.relaxpar;
+  prm.relax_table = P.table.p;
+  prm.resn_hist = P.resn.p;
+  prm.lam_hist = P.lamh.p;
+  P.params.upload(&prm, 1, s);
+
+  FwdOut fo{d_b, P.M.p, P.mr32.p, me ? P.rprev.p : nullptr, P.state.p};
+  UpdArgs ua{};
+  ua.D = P.D.p;
+  ua.x64 = P.x64.p;
+  ua.x32 = P.x32.p;
+  ua.lbk = o.lb_kind;
+  ua.ubk = o.ub_kind;
+  ua.lb = o.lb;
+  ua.ub = o.ub;
+  ua.lbv = P.lbv.p;
+  ua.ubv = P.ubv.p;
+  ua.X = d_X;
+  ua.n = n;
+  ua.save_slot = P.save_slot.p;
+  ua.st = P.state.p;
+  ua.g64 = P.g64.p;
+
+  // initial residual and stop check (sirt.m:153-162)
+  launch_fwd(P, fo, me);
+  k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
+  AIRT_LAUNCH_CHECK();
+
+  // main loop, enqueued in chunks; the flag of chunk c is read after chunk
+  // c+1 has been queued so the device never idles on the poll
+  if (!P.h_state) AIRT_CHECK_CUDA(cudaMallocHost(&P.h_state, 2 * sizeof(SirtState)));
+  cudaEvent_t ev[2];
+  AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  const int64_t chunk = 16;
+  int64_t c = 0;
+  for (int64_t it = 1; it <= kmax; ++c) {
+    const int64_t cnt = (kmax - it + 1 < chunk) ? (kmax - it + 1) : chunk;
+    for (int64_t j = 0; j < cnt; ++j) {
+      launch_bwd(P, ua, o.relax_kind);
+      launch_fwd(P, fo, me);
+      k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
+    }
+    AIRT_LAUNCH_CHECK();
+    it += cnt;
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(P.h_state + (c & 1), P.state.p, sizeof(SirtState),
+                                    cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaEventRecord(ev[c & 1], s));
+    if (c >= 1) {
+      AIRT_CHECK_CUDA(cudaEventSynchronize(ev[(c - 1) & 1]));
+      if (P.h_state[(c - 1) & 1].stop) break;
+    }
+  }
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(P.h_state, P.state.p, sizeof(SirtState), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  const SirtState st = P.h_state[0];
+  AIRT_REQUIRE(st.stop, "internal: SIRT loop ended without a stop");
+
+  // X keeps the iterates in K below finaliter plus the final one (sirt.m:270)
+  int64_t nsaved = 0;
+  if (st.finaliter > 0) {
+    int64_t below = 0;
+    for (int64_t l = 0; l < nK; ++l)
+      if (K[l] < st.finaliter) ++below;
+    nsaved = below + 1;
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(d_X + below * n, P.x64.p, n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, s));
+  }
+  AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
+  if (resn_host)
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(resn_host, P.resn.p, (st.finaliter + 1) * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+  double lam_final = o.relaxpar;
+  if (st.finaliter > 0)
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(&lam_final, P.lamh.p + st.finaliter, sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  prof_collect(P);
+  if (info) {
+    info->stoprule = st.stoprule;
+    info->finaliter = st.finaliter;
+    info->relaxpar = lam_final;
+    info->nsaved = nsaved;
+    info->gpu_ms = ms;
+  }
+}
+
+// ---------------------------------------------------------------- rho
+namespace {
+
+__global__ void k_sqrt_vec(int64_t n, const double *__restrict__ a, double *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = sqrt(a[i] > 0 ? a[i] : 0.0);
+}
+__global__ void k_mul(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
+                      double *__restrict__ c) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    c[i] = a[i] * b[i];
+}
+__global__ void k_dot2(int64_t n, const double *__restrict__ u, const double *__restrict__ w,
+                       double *__restrict__ out) {
+  double a = 0, b = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    a += u[i] * w[i];
+    b += w[i] * w[i];
+  }
+  a = block_sum<kThreads>(a);
+  b = block_sum<kThreads>(b);
+  if (threadIdx.x == 0) {
+    atomicAdd(out, a);
+    atomicAdd(out + 1, b);
+  }
+}
+__global__ void k_scale(int64_t n, const double *__restrict__ w, const double *__restrict__ nrm2,
+                        double *__restrict__ u) {
+  const double s = 1.0 / sqrt(nrm2[1]);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    u[i] = w[i] * s;
+}
+
+}  // namespace
+
+// Largest eigenvalue of D*A'*M*A by power iteration on the similar symmetric
+// operator D^(1/2)*A'*M*A*D^(1/2) (valid for nonnegative M, D), Rayleigh
+// quotient estimate; replaces eigs(...,'lm',tol=1e-4) of calc_relaxpar.m:91-103.
+double estimate_rho(Problem &P, const double *dM, const double *dD, double tol, int maxit) {
+  cudaStream_t s = P.stream;
+  const int64_t m = P.m, n = P.n;
+  DevBuf<double> sd, u, t, y, w, red;
+  sd.ensure(n);
+  u.ensure(n);
+  t.ensure(n);
+  y.ensure(m);
+  w.ensure(n);
+  red.ensure(2);
+  const unsigned gn = grid_for(n, kThreads), gm = grid_for(m, kThreads);
+  k_sqrt_vec<<<gn, kThreads, 0, s>>>(n, dD, sd.p);
+  std::vector<double> h(n, 1.0 / std::sqrt((double)(n ? n : 1)));
+  u.upload(h.data(), n, s);
+  double lam = 0, prev = 0;
+  for (int it = 0; it < maxit; ++it) {
+    k_mul<<<gn, kThreads, 0, s>>>(n, sd.p, u.p, t.p);
+    apply_operator(P, t.p, y.p, 0);
+    k_mul<<<gm, kThreads, 0, s>>>(m, dM, y.p, y.p);
+    apply_operator(P, y.p, t.p, 1);
+    k_mul<<<gn, kThreads, 0, s>>>(n, sd.p, t.p, w.p);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(red.p, 0, 2 * sizeof(double), s));
+    k_dot2<<<gn, kThreads, 0, s>>>(n, u.p, w.p, red.p);
+    k_scale<<<gn, kThreads, 0, s>>>(n, w.p, red.p, u.p);
+    AIRT_LAUNCH_CHECK();
+    double hr[2];
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hr, red.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    lam = hr[0];
+    if (!(hr[1] > 0)) break;
+    if (it > 0 && std::fabs(lam - prev) <= tol * std::fabs(lam)) break;
+    prev = lam;
+  }
+  return lam;
+}
+
+}  // namespace airt

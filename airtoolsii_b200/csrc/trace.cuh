@@ -1,0 +1,161 @@
+// Device ray tracer of the paralleltomo / fanlineartomo line model.
+//
+// One ray is one row of A.  The reference (testprobs/paralleltomo.m:207-263,
+// testprobs/fanlineartomo.m:271-318) computes the crossings with all x = const
+// and y = const grid lines, sorts them by the line parameter t (stable, NaN
+// last), keeps the points inside the square, drops a point whose successor is
+// within 1e-10 in both coordinates, and turns consecutive points into
+// (pixel, length) pairs.  Both crossing sequences are monotone in t, so the
+// sort is replaced here by a two-way merge that takes the x-crossing first on
+// equal t -- the same order the stable sort gives for every point that
+// survives the box filter (non-finite t values never survive it).  All FP64
+// arithmetic uses explicit round-to-nearest intrinsics, so no multiply-add is
+// contracted and the points, lengths and pixel indices are bit-identical to
+// the FP64 CPU restatement.
+#pragma once
+
+#include "common.cuh"
+
+namespace airt {
+
+struct Ray {
+  double x0t, y0t, a, b;
+};
+
+// Ray parameters, paralleltomo.m:195-200 / fanlineartomo.m:230-257.
+__device__ __forceinline__ Ray ray_of(const RayGeom &g, int64_t r) {
+  const int i = (int)(r / g.p);
+  const int j = (int)(r - (int64_t)i * g.p);
+  const double c = g.cos_t[i], s = g.sin_t[i];
+  Ray q;
+  if (g.kind == GEO_PARALLEL) {
+    const double x0 = g.offsets[j];
+    q.x0t = __dsub_rn(__dmul_rn(c, x0), __dmul_rn(s, 0.0));
+    q.y0t = __dadd_rn(__dmul_rn(s, x0), __dmul_rn(c, 0.0));
+    q.a = -s;
+    q.b = c;
+  } else {
+    q.x0t = __dadd_rn(__dmul_rn(c, 0.0), __dmul_rn(-s, g.R));
+    q.y0t = __dadd_rn(__dmul_rn(s, 0.0), __dmul_rn(c, g.R));
+    const double ab1 = __ddiv_rn(-q.x0t, g.R);
+    const double ab2 = __ddiv_rn(-q.y0t, g.R);
+    const double cw = g.cos_w[j], sw = g.sin_w[j];
+    q.a = __dadd_rn(__dmul_rn(cw, ab1), __dmul_rn(-sw, ab2));
+    q.b = __dadd_rn(__dmul_rn(sw, ab1), __dmul_rn(cw, ab2));
+  }
+  return q;
+}
+
+// Traces one ray and calls seg(col, len) for each segment in ray order
+// (before duplicate merging).  col is the 0-based column-major pixel index.
+template <class Seg>
+__device__ __forceinline__ void trace_segments(int N, const Ray &q, bool exclude_top_right,
+                                               Seg &&seg) {
+  const double h = 0.5 * (double)N;
+  if (exclude_top_right && ((q.b == 0.0 && fabs(__dsub_rn(q.y0t, h)) < 1e-15) ||
+                            (q.a == 0.0 && fabs(__dsub_rn(q.x0t, h)) < 1e-15)))
+    return;
+  // x-crossing sequence in ascending t
+  int nx = 0, ix = 0, sx = 1;
+  if (q.a > 0.0) { nx = N + 1; ix = 0; sx = 1; }
+  else if (q.a < 0.0) { nx = N + 1; ix = N; sx = -1; }
+  int ny = 0, iy = 0, sy = 1;
+  if (q.b > 0.0) { ny = N + 1; iy = 0; sy = 1; }
+  else if (q.b < 0.0) { ny = N + 1; iy = N; sy = -1; }
+  int cx = 0, cy = 0;
+  double tx = 0.0, ty = 0.0;
+  if (nx) tx = __ddiv_rn(__dsub_rn((double)ix - h, q.x0t), q.a);
+  if (ny) ty = __ddiv_rn(__dsub_rn((double)iy - h, q.y0t), q.b);
+
+  bool have_pend = false, have_last = false;
+  double px = 0, py = 0, lx = 0, ly = 0;
+  while (cx < nx || cy < ny) {
+    double xx, yy;
+    if (cy >= ny || (cx < nx && tx <= ty)) {
+      xx = (double)ix - h;
+      yy = __dadd_rn(__dmul_rn(q.b, tx), q.y0t);
+      ++cx;
+      ix += sx;
+      if (cx < nx) tx = __ddiv_rn(__dsub_rn((double)ix - h, q.x0t), q.a);
+    } else {
+      yy = (double)iy - h;
+      xx = __dadd_rn(__dmul_rn(q.a, ty), q.x0t);
+      ++cy;
+      iy += sy;
+      if (cy < ny) ty = __ddiv_rn(__dsub_rn((double)iy - h, q.y0t), q.b);
+    }
+    if (!(xx >= -h && xx <= h && yy >= -h && yy <= h)) continue;
+    if (have_pend) {
+      const bool close = fabs(__dsub_rn(xx, px)) <= 1e-10 && fabs(__dsub_rn(yy, py)) <= 1e-10;
+      if (!close) {
+        if (have_last) {
+          const double dx = __dsub_rn(px, lx), dy = __dsub_rn(py, ly);
+          const double len = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+          const double xm = __dadd_rn(__dmul_rn(0.5, __dadd_rn(lx, px)), h);
+          const double ym = __dadd_rn(__dmul_rn(0.5, __dadd_rn(ly, py)), h);
+          const int col = (int)floor(xm) * N + (N - 1 - (int)floor(ym));
+          seg(col, len);
+        }
+        lx = px;
+        ly = py;
+        have_last = true;
+      }
+    }
+    px = xx;
+    py = yy;
+    have_pend = true;
+  }
+  if (have_pend && have_last) {
+    const double dx = __dsub_rn(px, lx), dy = __dsub_rn(py, ly);
+    const double len = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+    const double xm = __dadd_rn(__dmul_rn(0.5, __dadd_rn(lx, px)), h);
+    const double ym = __dadd_rn(__dmul_rn(0.5, __dadd_rn(ly, py)), h);
+    const int col = (int)floor(xm) * N + (N - 1 - (int)floor(ym));
+    seg(col, len);
+  }
+}
+
+// Segments with duplicate pixels of the same ray merged, as MATLAB's
+// sparse() sums duplicate (row, col) pairs (paralleltomo.m:300).  A straight
+// ray meets a pixel in one segment; a duplicate can only come from a sliver
+// segment at a grid corner, so a window of the last few entries suffices.
+// emit(col, value) is called once per distinct pixel, in ray order of first
+// appearance, with the FP64 sum.
+constexpr int kMergeWindow = 4;
+
+template <class Emit>
+__device__ __forceinline__ void trace_entries(int N, const Ray &q, bool exclude_top_right,
+                                              Emit &&emit) {
+  int wc[kMergeWindow];
+  double wv[kMergeWindow];
+  int cnt = 0;  // entries held in the window (oldest at index 0)
+  trace_segments(N, q, exclude_top_right, [&](int col, double len) {
+#pragma unroll
+    for (int k = 0; k < kMergeWindow; ++k)
+      if (k < cnt && wc[k] == col) {
+        wv[k] = __dadd_rn(wv[k], len);
+        return;
+      }
+    if (cnt == kMergeWindow) {
+      emit(wc[0], wv[0]);
+#pragma unroll
+      for (int k = 0; k + 1 < kMergeWindow; ++k) {
+        wc[k] = wc[k + 1];
+        wv[k] = wv[k + 1];
+      }
+      cnt = kMergeWindow - 1;
+    }
+#pragma unroll
+    for (int k = 0; k < kMergeWindow; ++k)
+      if (k == cnt) {
+        wc[k] = col;
+        wv[k] = len;
+      }
+    ++cnt;
+  });
+#pragma unroll
+  for (int k = 0; k < kMergeWindow; ++k)
+    if (k < cnt) emit(wc[k], wv[k]);
+}
+
+}  // namespace airt

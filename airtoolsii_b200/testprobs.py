@@ -1,0 +1,198 @@
+"""Tomography test problems on the GPU: paralleltomo and fanlineartomo.
+
+The host side prepares the per-angle and per-detector tables in FP64 exactly
+as the reference does (cosd/sind of the angles, linspace ray offsets, the
+fan's atand detector angles); libairt traces every ray on the device and
+either stores A (FP32 CSR + CSC, bit-exact sparsity with the FP64 trace) or
+keeps the geometry for matrix-free projection.
+
+Also here: the reference's modified Shepp-Logan phantom and the random-ellipse
+phantom family (same rasterisation grid, testprobs/phantomgallery.m:188-214).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from ._lib import check, dptr, lib
+from .afun import AirtOperator
+
+
+def _mround(x: float) -> float:
+    return math.copysign(math.floor(abs(x) + 0.5), x)
+
+
+def _trigd(x: float):
+    """(cosd, sind) of one angle in degrees: exact 0/+-1 at multiples of 90,
+    otherwise one cos/sin of the angle reduced to [-45, 45] degrees."""
+    x = float(x)
+    n = _mround(x / 90.0)
+    r = x - 90.0 * n
+    rad = r * (math.pi / 180.0)
+    c, s = math.cos(rad), math.sin(rad)
+    q = int(n) % 4
+    cd, sd = ((c, s), (-s, c), (-c, -s), (s, -c))[q]
+    return cd + 0.0, sd + 0.0
+
+
+def cosd(x) -> np.ndarray:
+    return np.array([_trigd(v)[0] for v in np.atleast_1d(np.asarray(x, float))])
+
+
+def sind(x) -> np.ndarray:
+    return np.array([_trigd(v)[1] for v in np.atleast_1d(np.asarray(x, float))])
+
+
+def atand(x) -> np.ndarray:
+    return np.array([(180.0 / math.pi) * math.atan(v) for v in np.atleast_1d(np.asarray(x, float))])
+
+
+def _linspace(d1, d2, n):
+    n = int(n)
+    if n <= 0:
+        return np.zeros(0)
+    if n == 1:
+        return np.array([float(d2)])
+    y = d1 + (np.arange(n, dtype=float) * (d2 - d1)) / (n - 1)
+    y[0], y[-1] = d1, d2
+    return y
+
+
+# ------------------------------------------------------------------ phantoms
+_SHEPP = ((1, .69, .92, 0, 0, 0), (-.8, .6624, .8740, 0, -.0184, 0),
+          (-.2, .1100, .3100, .22, 0, -18), (-.2, .1600, .4100, -.22, 0, 18),
+          (.1, .2100, .2500, 0, .35, 0), (.1, .0460, .0460, 0, .1, 0),
+          (.1, .0460, .0460, 0, -.1, 0), (.1, .0460, .0230, -.08, -.605, 0),
+          (.1, .0230, .0230, 0, -.606, 0), (.1, .0230, .0460, .06, -.605, 0))
+
+
+def ellipse_image(N: int, ellipses, clip_hi=None) -> np.ndarray:
+    """Sum of filled ellipses (amplitude, a, b, x0, y0, phi[rad]) on the grid
+    of phantomgallery.m:188-190; negatives set to 0, optional upper clip."""
+    xn = (np.arange(N) - (N - 1) / 2.0) / ((N - 1) / 2.0)
+    Xn = np.tile(xn, (N, 1))
+    Yn = np.rot90(Xn)
+    X = np.zeros((N, N))
+    for A, ea, eb, x0, y0, phi in ellipses:
+        x = Xn - x0
+        y = Yn - y0
+        cph, sph = math.cos(phi), math.sin(phi)
+        inside = (((x * cph + y * sph) ** 2) / (ea * ea)
+                  + ((y * cph - x * sph)) ** 2 / (eb * eb)) <= 1
+        X[inside] += A
+    X[X < 0] = 0
+    if clip_hi is not None:
+        X[X > clip_hi] = clip_hi
+    return X
+
+
+def phantomgallery(name: str, N: int) -> np.ndarray:
+    """The 'shepplogan' image of testprobs/phantomgallery.m:155-214 (N x N)."""
+    if name != "shepplogan":
+        raise ValueError("only the 'shepplogan' phantom is provided")
+    return ellipse_image(N, [(a, b, c, d, e, f * math.pi / 180) for a, b, c, d, e, f in _SHEPP])
+
+
+def random_ellipses(N: int, count: int, seed: int, clip=(0.0, 1.0)) -> np.ndarray:
+    """Random-ellipse phantom as x(:) (column-major): centres U[-0.6,0.6]^2,
+    semi-axes U[0.05,0.4], rotation U[0,pi), intensity U[0.1,1], additive,
+    clipped to [0,1]."""
+    rng = np.random.default_rng(seed)
+    ell = []
+    for _ in range(count):
+        cx, cy = rng.uniform(-0.6, 0.6, 2)
+        a, b = rng.uniform(0.05, 0.4, 2)
+        phi = rng.uniform(0.0, math.pi)
+        amp = rng.uniform(0.1, 1.0)
+        ell.append((amp, a, b, cx, cy, phi))
+    X = ellipse_image(N, ell, clip_hi=clip[1])
+    return X.ravel(order="F")
+
+
+def add_noise(b: np.ndarray, eta: float, seed: int):
+    """b + e with Gaussian e scaled to ||e|| = eta*||b|| (demo_stoprules.m:43-46).
+    Returns (b_noisy, ||e||)."""
+    rng = np.random.default_rng(seed)
+    e = rng.standard_normal(b.size)
+    e = eta * np.linalg.norm(b) * e / np.linalg.norm(e)
+    return b + e, float(np.linalg.norm(e))
+
+
+# ------------------------------------------------------------------ geometries
+def parallel_tables(N, theta=None, p=None, d=None):
+    """paralleltomo.m:62-89,118,195-200: (theta, p, d, cos_t, sin_t, offsets)."""
+    theta = np.arange(180.0) if theta is None else np.asarray(theta, float).ravel()
+    if p is None:
+        p = int(_mround(math.sqrt(2.0) * N))
+    if d is None:
+        d = p - 1
+    return theta, int(p), float(d), cosd(theta), sind(theta), _linspace(-d / 2.0, d / 2.0, p)
+
+
+def fan_tables(N, theta=None, p=None, R=None, dw=None, sd=None):
+    """fanlineartomo.m:74-114,146-170: (theta, p, R, dw, sd, cos_t, sin_t,
+    cos_w, sin_w) with R, dw, sd already multiplied by N."""
+    sdv = (3.0 if sd is None else sd) * N
+    dwv = (2.5 if dw is None else dw) * N
+    Rv = (2.0 if R is None else R) * N
+    if p is None:
+        p = int(_mround(math.sqrt(2.0) * N))
+    theta = np.arange(0.0, 359.0, 2.0) if theta is None else np.asarray(theta, float).ravel()
+    if Rv < math.sqrt(2.0) / 2.0 * N:
+        raise ValueError("R must be greater than half squareroot 2")
+    dew = dwv / p
+    if p % 2:
+        depos = np.arange(1, (p - 1) // 2 + 1, dtype=float) * dew
+        om = 90.0 - atand(sdv / depos)
+        omega = np.concatenate([-om[::-1], [0.0], om])
+    else:
+        depos = (np.arange(1, p // 2 + 1, dtype=float) - 0.5) * dew
+        om = 90.0 - atand(sdv / depos)
+        omega = np.concatenate([-om[::-1], om])
+    return theta, int(p), Rv, dwv, sdv, cosd(theta), sind(theta), cosd(omega), sind(omega)
+
+
+def parallel_operator(N, cos_t, sin_t, offsets, matrix_free=False) -> AirtOperator:
+    ct = np.ascontiguousarray(cos_t, np.float64)
+    st = np.ascontiguousarray(sin_t, np.float64)
+    off = np.ascontiguousarray(offsets, np.float64)
+    h = C.c_void_p()
+    check(lib().airt_problem_parallel(int(N), ct.size, dptr(ct), dptr(st), off.size, dptr(off),
+                                      int(bool(matrix_free)), C.byref(h)))
+    return AirtOperator(h, "parallel", dict(N=N, nA=ct.size, p=off.size))
+
+
+def fan_operator(N, cos_t, sin_t, cos_w, sin_w, R, matrix_free=False) -> AirtOperator:
+    ct = np.ascontiguousarray(cos_t, np.float64)
+    st = np.ascontiguousarray(sin_t, np.float64)
+    cw = np.ascontiguousarray(cos_w, np.float64)
+    sw = np.ascontiguousarray(sin_w, np.float64)
+    h = C.c_void_p()
+    check(lib().airt_problem_fan(int(N), ct.size, dptr(ct), dptr(st), cw.size, dptr(cw), dptr(sw),
+                                 float(R), int(bool(matrix_free)), C.byref(h)))
+    return AirtOperator(h, "fan", dict(N=N, nA=ct.size, p=cw.size, R=R))
+
+
+def paralleltomo(N, theta=None, p=None, d=None, isDisp=0, isMatrix=1):
+    """[A,b,x,theta,p,d] = paralleltomo(N,theta,p,d,isDisp,isMatrix)
+    (testprobs/paralleltomo.m:1).  A is an AirtOperator: the stored system
+    matrix (isMatrix=1) or the matrix-free projector (isMatrix=0).  b = A*x for
+    the Shepp-Logan phantom x.  isDisp (ray animation) is not supported."""
+    theta, p, d, ct, st, off = parallel_tables(N, theta, p, d)
+    A = parallel_operator(N, ct, st, off, matrix_free=not isMatrix)
+    x = phantomgallery("shepplogan", N).ravel(order="F")
+    b = A(x, "notransp")
+    return A, b, x, theta, p, d
+
+
+def fanlineartomo(N, theta=None, p=None, R=None, dw=None, sd=None, isDisp=0, isMatrix=1):
+    """[A,b,x,theta,p,R,dw,sd] = fanlineartomo(N,theta,p,R,dw,sd,isDisp,isMatrix)
+    (testprobs/fanlineartomo.m:1-2).  R, dw, sd are in units of N as in the
+    reference; R is returned in units of N."""
+    theta, p, Rv, dwv, sdv, ct, st, cw, sw = fan_tables(N, theta, p, R, dw, sd)
+    A = fan_operator(N, ct, st, cw, sw, Rv, matrix_free=not isMatrix)
+    x = phantomgallery("shepplogan", N).ravel(order="F")
+    b = A(x, "notransp")
+    return A, b, x, theta, p, Rv / N, dwv, sdv

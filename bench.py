@@ -1,0 +1,349 @@
+"""Benchmark: plain GPU SIRT on the single large paralleltomo problem.
+
+Workload: paralleltomo N=512, 360 angles over [0,180) in 0.5-degree steps,
+p=724 rays (A: 260640 x 262144, 120,154,640 nonzeros, generated on the GPU,
+FP32 CSR + CSC); 30-ellipse random phantom, 0.5% Gaussian noise; cimmino,
+200 iterations, box constraint [0,1].  rho is estimated once before timing and
+passed as options.rho (as a user repeating solves would).
+
+One step = one sirt call (weights + 200 iterations).  value = SpMV traffic of
+the CSR+CSC model, (16*nnz + 16*m + 16*n) bytes per iteration, times 200,
+divided by the step's device time.  Inputs exceed L2 (A is ~1.9 GB), so no
+extra L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl airt|reference]
+                  [--small]  (N=128 case for ncu captures)
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="airt", choices=["airt", "reference"])
+    ap.add_argument("--method", default="cimmino")
+    ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--small", action="store_true", help="N=128 problem (profiling captures)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def workload(small: bool):
+    if small:
+        return dict(N=128, nA=180, p=181, step=1.0, ellipses=30, eta=0.005)
+    return dict(N=512, nA=360, p=724, step=0.5, ellipses=30, eta=0.005)
+
+
+def model_bytes(nnz, m, n):
+    return 16 * nnz + 16 * m + 16 * n
+
+
+def fwd_bytes(nnz, m, n):
+    # values + columns, row starts, gathered x (FP32, once), b, M (FP64), M.*r (FP32)
+    return 8 * nnz + 8 * (m + 1) + 4 * n + 8 * m + 8 * m + 4 * m
+
+
+def bwd_bytes(nnz, m, n):
+    # values + rows, column starts, gathered M.*r (FP32, once), D, x (FP64 r+w), x (FP32 w)
+    return 8 * nnz + 8 * (n + 1) + 4 * m + 8 * n + 16 * n + 4 * n
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_leg(A_csc, b, M, D, lam, iters, m, n, nnz):
+    """FP64 C restatement (OpenMP, all host threads) on a bounded sample."""
+    from oracle import cbind
+    t0 = time.perf_counter()
+    x, k, _ = cbind.sirt_csr(A_csc.tocsr(), b, M, D, lam, 0.0, 1.0, None, iters)
+    dt = time.perf_counter() - t0
+    return {"value": model_bytes(nnz, m, n) * iters / dt / 1e9, "unit": "GB/s",
+            "cores": cbind.num_threads(), "kind": "port",
+            "sample": f"{iters} cimmino iterations of the same problem, FP64 CSR+CSC "
+                      f"(C restatement, OpenMP), {dt:.2f} s"}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = workload(a.small)
+    cfg = {"workload": f"paralleltomo N={wl['N']}, {wl['nA']} angles x {wl['p']} rays, "
+                       f"{a.method} {a.iters} iterations, box [0,1], FP32 CSR+CSC",
+           "N": wl["N"], "angles": wl["nA"], "rays": wl["p"], "method": a.method,
+           "iterations": a.iters, "phantom": f"{wl['ellipses']} random ellipses",
+           "noise": wl["eta"], "l2": "inputs larger than L2 (A ~1.9 GB)" if not a.small else
+           "N=128 case", "parallelism": f"replicas x{a.gpus}"}
+    metric = "SIRT SpMV HBM GB/s (CSR+CSC byte model, plain GPU SIRT)"
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        reference_arm(a, wl, cfg, metric)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    import airtoolsii_b200 as airt
+    from airtoolsii_b200 import _lib
+    from airtoolsii_b200.testprobs import parallel_operator, parallel_tables
+
+    theta = np.arange(wl["nA"]) * wl["step"]
+    _, p, d, ct, st, off = parallel_tables(wl["N"], theta, wl["p"])
+    t_build = time.perf_counter()
+    A = parallel_operator(wl["N"], ct, st, off)
+    t_build = time.perf_counter() - t_build
+    m, n, nnz = A.m, A.n, A.nnz
+    x_true = airt.random_ellipses(wl["N"], wl["ellipses"], seed=100 + rank)
+    b_ex = A(x_true, "notransp")
+    b, enorm = airt.add_noise(b_ex, wl["eta"], seed=200 + rank)
+    code = _lib.METHODS[a.method]
+    rho = C.c_double()
+    t_rho = time.perf_counter()
+    _lib.check(_lib.lib().airt_rho(A.handle, code, None, None, 1e-7, 200, C.byref(rho)))
+    t_rho = time.perf_counter() - t_rho
+    lam = 1.9 / rho.value
+
+    o = _lib.SirtOpts()
+    o.method = code
+    o.relax_kind = _lib.RELAX_CONST
+    o.relaxpar = lam
+    o.stoprule = _lib.STOP["NONE"]
+    o.lb_kind, o.lb = _lib.BOUND_SCALAR, 0.0
+    o.ub_kind, o.ub = _lib.BOUND_SCALAR, 1.0
+    o.kmax = a.iters
+    K = np.array([a.iters], np.int64)
+    stream = torch.cuda.ExternalStream(A.stream_ptr())
+    d_b = torch.from_numpy(b).cuda()
+    d_X = torch.empty(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    info = _lib.Info()
+
+    def step_device():
+        _lib.check(_lib.lib().airt_sirt_device(A.handle, C.byref(o), C.c_void_p(d_b.data_ptr()),
+                                                None, _lib.i64ptr(K), 1,
+                                                C.c_void_p(d_X.data_ptr()), None, C.byref(info)))
+
+    h_b = torch.from_numpy(b).pin_memory()
+    h_X = torch.empty(n, dtype=torch.float64).pin_memory()
+    hb_np, hX_np = h_b.numpy(), h_X.numpy()
+
+    def step_e2e():
+        _lib.check(_lib.lib().airt_sirt(A.handle, C.byref(o), _lib.dptr(hb_np), None,
+                                         _lib.i64ptr(K), 1, _lib.dptr(hX_np), None,
+                                         C.byref(info)))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(max(a.warmup, 3)):
+        step_device()
+    clocks = Clocks(local)
+    clocks.start()
+    ms_dev = timed(step_device, a.steps)
+    ck = clocks.stop()
+    for _ in range(2):
+        step_e2e()
+    ms_e2e = timed(step_e2e, a.steps)
+    # per-kernel device times for the roofline (events around every launch)
+    _lib.check(_lib.lib().airt_profile_enable(A.handle, 1))
+    ms_prof = timed(step_device, a.steps)
+    kl, kms = [], []
+    for which in (0, 1):
+        L, T = C.c_int64(), C.c_double()
+        _lib.check(_lib.lib().airt_profile_read(A.handle, which, C.byref(L), C.byref(T)))
+        kl.append(int(L.value))
+        kms.append(float(T.value))
+    _lib.check(_lib.lib().airt_profile_enable(A.handle, 0))
+    x_gpu = d_X.cpu().numpy()
+
+    it = a.iters
+    bytes_step = model_bytes(nnz, m, n) * it
+    value = bytes_step * a.steps * world / (ms_dev / 1e3) / 1e9
+    e2e = bytes_step * a.steps * world / (ms_e2e / 1e3) / 1e9
+    fb, bb = fwd_bytes(nnz, m, n), bwd_bytes(nnz, m, n)
+    avg = [kms[i] / max(kl[i], 1) for i in range(2)]
+    dom = 0 if avg[0] >= avg[1] else 1
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    ach = (fb if dom == 0 else bb) / (avg[dom] / 1e3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        key = "sirt_fwd" if dom == 0 else "sirt_bwd"
+        if key in prof and not a.small:
+            traffic = prof[key]
+    except Exception:
+        pass
+    launches_per_step = 3 + 1 + 2 + 3 * it   # weights (3), x copy, initial fwd+ctrl, 3/iteration
+
+    if rank == 0:
+        line = {
+            "metric": metric, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+            "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": round(ms_dev / a.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random-ellipse phantom, Gaussian noise)",
+            "config": cfg,
+            "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * m,
+                    "d2h_bytes_per_step": 8 * n, "ms_per_step": round(ms_e2e / a.steps, 4)},
+            "roofline": {"bound": "hbm", "kernel": ["k_sirt_fwd (CSR residual SpMV)",
+                                                    "k_sirt_bwd (CSC transpose SpMV + update)"][dom],
+                         "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(ach / peak, 4), "traffic": traffic,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks
+                         else "fallback 6650 GB/s (of fallback)",
+                         "algorithmic_bytes_per_launch": fb if dom == 0 else bb,
+                         "avg_launch_ms": round(avg[dom], 5),
+                         "kernels": {"fwd": {"launches": kl[0], "ms": round(kms[0], 3),
+                                             "avg_ms": round(avg[0], 5), "bytes": fb,
+                                             "GBps": round(fb / (avg[0] / 1e3) / 1e9, 1)},
+                                     "bwd": {"launches": kl[1], "ms": round(kms[1], 3),
+                                             "avg_ms": round(avg[1], 5), "bytes": bb,
+                                             "GBps": round(bb / (avg[1] / 1e3) / 1e9, 1)}},
+                         "profiled_ms_per_step": round(ms_prof / a.steps, 4)},
+            "clocks": ck,
+            "gpu_launches": launches_per_step * a.steps,
+            "problem": {"m": m, "n": n, "nnz": nnz, "matrix_build_s": round(t_build, 3),
+                        "rho": rho.value, "rho_s": round(t_rho, 4)},
+        }
+        if not a.no_cpu and world == 1:
+            M, D = A.weights(a.method)
+            line["cpu_baseline"] = cpu_leg(A.to_scipy(), b, M, D, lam, 2 if not a.small else 10,
+                                           m, n, nnz)
+        print(json.dumps(line), flush=True)
+        del x_gpu
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_arm(a, wl, cfg, metric):
+    """The reference's CPU path: the FP64 C restatement of sirt.m (OpenMP,
+    all host threads) on the same problem, each step a bounded sample."""
+    from oracle import airt_oracle as O
+    from oracle import cbind
+    theta = np.arange(wl["nA"]) * wl["step"]
+    th, p, d, ct, st, off = O.parallel_geometry(wl["N"], theta, wl["p"])
+    t0 = time.perf_counter()
+    rows, cols, vals = cbind.trace_coo(wl["N"], list(O.parallel_rays(wl["N"], ct, st, off)), True)
+    A = O.coo_to_csc(rows, cols, vals, len(th) * p, wl["N"] ** 2)
+    t_build = time.perf_counter() - t0
+    del rows, cols, vals
+    m, n = A.shape
+    nnz = A.nnz
+    from airtoolsii_b200.testprobs import add_noise, random_ellipses  # data generator only
+    x = random_ellipses(wl["N"], wl["ellipses"], seed=100)
+    b, _ = add_noise(A @ x, wl["eta"], seed=200)
+    M, D, _, _ = O.get_mfun_dfun(a.method, A)
+    lam = 1.0
+    sample = 1 if not a.small else 5
+    Acsr = A.tocsr()
+    for _ in range(max(a.warmup, 3) if a.small else 1):
+        cbind.sirt_csr(Acsr, b, M, D, lam, 0.0, 1.0, None, sample)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        cbind.sirt_csr(Acsr, b, M, D, lam, 0.0, 1.0, None, sample)
+    dt = time.perf_counter() - t0
+    v = model_bytes(nnz, m, n) * sample * a.steps / dt / 1e9
+    line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "GB/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": max(a.warmup, 3),
+            "ms_per_step": round(dt / a.steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded random-ellipse phantom, Gaussian noise)", "config": cfg,
+            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": cbind.num_threads(),
+                             "kind": "port",
+                             "sample": f"{sample} cimmino iteration(s) per step of the same "
+                                       "problem, FP64 CSR+CSC C restatement (OpenMP); the "
+                                       "MATLAB reference cannot run here (no MATLAB/Octave)"},
+            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "problem": {"m": m, "n": n, "nnz": nnz, "matrix_build_s": round(t_build, 2)}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+/*
+ * airt.h -- C-ABI of libairt, the B200 (sm_100a) engine behind the AIR Tools II
+ * solver and operator API.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (AIRT_OK = 0) and leaves a message for airt_last_error() on failure.  Host
+ * buffers are caller-owned, MATLAB column-major doubles; the library copies in,
+ * keeps FP32 CSR/CSC matrices and FP64 vectors in HBM, and owns device memory
+ * until airt_destroy().  Functions ending in _device take device pointers and
+ * run on the problem's CUDA stream (airt_problem_stream) without host copies.
+ *
+ * Reference interfaces replaced (AIR Tools II V1.0, paths inside its tree):
+ *   airt_problem_from_csc  -> auxil/check_inputs.m:67-71 (matrix wrapped as afun)
+ *   airt_problem_parallel  -> testprobs/paralleltomo.m:112-301
+ *   airt_problem_fan       -> testprobs/fanlineartomo.m:141-358
+ *   airt_apply             -> auxil/afun_matrix.m:44-53 and the isMatrix=0 handles
+ *                             testprobs/paralleltomo.m:146-177,280-288
+ *   airt_weights           -> auxil/get_mfun_dfun.m:43-250
+ *   airt_rho               -> auxil/calc_relaxpar.m:91-103 (eigs of D*A'*M*A)
+ *   airt_sirt              -> sirt/sirt.m:147-261 with auxil/check_stoprules.m:54-94,153-161
+ *   airt_art               -> art/art.m:138-309
+ */
+#ifndef AIRT_H
+#define AIRT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define AIRT_OK 0
+#define AIRT_ERR_ARG 1     /* invalid argument (size, pointer, option)      */
+#define AIRT_ERR_OOM 2     /* device allocation failed                       */
+#define AIRT_ERR_CUDA 3    /* CUDA runtime error                             */
+#define AIRT_ERR_TIMEOUT 4 /* a bounded device wait gave up                  */
+#define AIRT_ERR_UNSUPPORTED 5
+
+/* ---- SIRT methods (sirt/sirt.m:17-26) ---------------------------------- */
+#define AIRT_LANDWEBER 0
+#define AIRT_CIMMINO 1
+#define AIRT_CAV 2
+#define AIRT_DROP 3
+#define AIRT_SART 4
+#define AIRT_CUSTOM 5 /* diagonal M and/or D given by the caller */
+
+/* ---- stopping rules (auxil/check_stoprules.m) --------------------------- */
+#define AIRT_STOP_NONE 0
+#define AIRT_STOP_DP 1
+#define AIRT_STOP_ME 2
+
+/* ---- relaxation strategy (auxil/calc_relaxpar.m: casel) ----------------- */
+#define AIRT_RELAX_CONST 1 /* relaxpar constant                     */
+#define AIRT_RELAX_LINE 2  /* line search, sirt/sirt.m:219-222      */
+#define AIRT_RELAX_TABLE 3 /* per-iteration table (psi1/psi2 rules) */
+
+/* ---- bound kinds --------------------------------------------------------- */
+#define AIRT_BOUND_NONE 0
+#define AIRT_BOUND_SCALAR 1
+#define AIRT_BOUND_VECTOR 2
+
+typedef struct airt_problem airt_problem;
+
+typedef struct {
+    int method;               /* AIRT_LANDWEBER..AIRT_CUSTOM                    */
+    const double *M;          /* AIRT_CUSTOM: m-vector diagonal of M, or NULL=I  */
+    const double *D;          /* AIRT_CUSTOM: n-vector diagonal of D, or NULL=I  */
+    int relax_kind;           /* AIRT_RELAX_*                                    */
+    double relaxpar;          /* AIRT_RELAX_CONST                                */
+    const double *relax_table;/* AIRT_RELAX_TABLE: kmax entries                  */
+    int stoprule;             /* AIRT_STOP_*                                     */
+    double taudelta;          /* DP / ME threshold                               */
+    int lb_kind, ub_kind;     /* AIRT_BOUND_*                                    */
+    double lb, ub;            /* scalar bounds                                   */
+    const double *lbv, *ubv;  /* vector bounds (n entries)                       */
+    int64_t kmax;             /* maximum number of iterations (K(end))           */
+} airt_sirt_opts;
+
+typedef struct {
+    int order_kind;           /* 0 kaczmarz, 1 symkaczmarz, 2 caller row list  */
+    const int64_t *rows;      /* order_kind 2: 0-based rows, nrows per sweep;
+                                 rows_per_sweep_stride>0 gives a new list per
+                                 sweep (randkaczmarz index stream)             */
+    int64_t nrows;
+    int64_t rows_stride;      /* 0 = same list every sweep                      */
+    double relaxpar;          /* constant relaxpar (default 1)                  */
+    const double *relax_table;/* optional relaxpar per row step: kmax blocks of
+                                 one entry per step of a sweep (the values of
+                                 the art.m:273-275 handle), or NULL           */
+    double damp;              /* art.m:206                                      */
+    int stoprule;             /* AIRT_STOP_NONE or AIRT_STOP_DP                 */
+    double taudelta;
+    int lb_kind, ub_kind;
+    double lb, ub;
+    const double *lbv, *ubv;
+    int64_t kmax;             /* sweeps (already halved for symkaczmarz)        */
+} airt_art_opts;
+
+typedef struct {
+    int stoprule;       /* 0 max iterations, 2 DP, 3 ME (check_stoprules.m:27-31) */
+    int64_t finaliter;  /* iterations performed                                 */
+    double relaxpar;    /* relaxpar of the final iteration                      */
+    int64_t nsaved;     /* columns written to X                                 */
+    double gpu_ms;      /* device time of the call (CUDA events)                */
+} airt_info;
+
+/* ---- errors and version -------------------------------------------------- */
+const char *airt_last_error(void);
+int airt_version(void);
+
+/* ---- problem construction ------------------------------------------------- */
+/* MATLAB sparse layout (mxGetJc / mxGetIr / mxGetPr): jc n+1 column starts,
+ * ir nnz row indices, pr nnz values.  Replaces the matrix branch of
+ * auxil/check_inputs.m:67-71 and auxil/afun_matrix.m:44-53. */
+int airt_problem_from_csc(int64_t m, int64_t n, const uint64_t *jc, const uint64_t *ir,
+                          const double *pr, airt_problem **out);
+
+/* paralleltomo geometry (testprobs/paralleltomo.m:112-301): nA angles given
+ * as cosd/sind tables, p ray offsets (linspace(-d/2,d/2,p)).  matrix_free=0
+ * builds the system matrix on the GPU (bit-exact sparsity with the FP64 ray
+ * trace); matrix_free=1 keeps only the geometry and recomputes rays. */
+int airt_problem_parallel(int N, int nA, const double *cos_t, const double *sin_t, int p,
+                          const double *offsets, int matrix_free, airt_problem **out);
+
+/* fanlineartomo geometry (testprobs/fanlineartomo.m:141-358): source
+ * distance R (absolute), per-angle cosd/sind of theta, per-detector cosd/sind
+ * of the ray angle omega. */
+int airt_problem_fan(int N, int nA, const double *cos_t, const double *sin_t, int p,
+                     const double *cos_w, const double *sin_w, double R, int matrix_free,
+                     airt_problem **out);
+
+int airt_problem_size(const airt_problem *h, int64_t *m, int64_t *n, int64_t *nnz);
+int airt_problem_stream(const airt_problem *h, void **cuda_stream);
+
+/* Copy the stored matrix back as MATLAB CSC (jc n+1, ir nnz, pr nnz). */
+int airt_problem_export_csc(airt_problem *h, uint64_t *jc, uint64_t *ir, double *pr);
+
+int airt_destroy(airt_problem *h);
+
+/* ---- operator (afun) ------------------------------------------------------ */
+/* y = A*x (transp=0) or y = A'*x (transp=1); host doubles. */
+int airt_apply(airt_problem *h, const double *in, double *out, int transp);
+int airt_apply_device(airt_problem *h, const double *d_in, double *d_out, int transp);
+
+/* ---- weights and spectral radius ----------------------------------------- */
+/* Diagonals of M (m) and D (n) of a built-in method (get_mfun_dfun.m). */
+int airt_weights(airt_problem *h, int method, double *M, double *D);
+
+/* rho = largest eigenvalue of D*A'*M*A (power iteration in FP64 to the given
+ * relative tolerance; maxit bounds the operator applications). */
+int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *Dcustom,
+             double tol, int maxit, double *rho);
+
+/* ---- solvers ---------------------------------------------------------------- */
+/* SIRT loop.  K: nK strictly increasing 1-based iteration numbers (K(end) =
+ * opts->kmax).  X: n x nK column-major output; the first info->nsaved columns
+ * are written (sirt.m:246-250,270).  resnorms (optional): kmax+1 entries,
+ * ||b - A x_k|| for k = 0..finaliter. */
+int airt_sirt(airt_problem *h, const airt_sirt_opts *opts, const double *b, const double *x0,
+              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
+int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *d_b,
+                     const double *d_x0, const int64_t *K, int64_t nK, double *d_X,
+                     double *resnorms, airt_info *info);
+
+/* ART (Kaczmarz) sweeps, art.m:138-309.  Same K / X / info conventions. */
+int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const double *x0,
+             const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
+
+/* ---- instrumentation ------------------------------------------------------- */
+/* When on, each SIRT kernel launch is bracketed by CUDA events on the problem
+ * stream; airt_profile_read returns launches and summed device milliseconds
+ * of kernel `which` (0 forward residual SpMV, 1 transpose SpMV + update). */
+int airt_profile_enable(airt_problem *h, int on);
+int airt_profile_read(airt_problem *h, int which, int64_t *launches, double *total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AIRT_H */

@@ -1,0 +1,341 @@
+"""GPU parity tests: libairt through its C-ABI against the FP64 oracle.
+
+Tolerances: the generated system matrix is bit-exact (pattern, and values
+equal to the FP64 trace rounded to FP32); SIRT/ART iterates agree with the
+FP64 oracle to a relative error <= 1e-5 after K iterations (rho passed
+explicitly so that the eigs tolerance is not part of the comparison).
+"""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import airtoolsii_b200 as airt
+from oracle import airt_oracle as O
+from oracle import cbind
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+RTOL = 1e-5
+
+
+def relerr(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def same_matrix(A_gpu, A_ref):
+    E = A_gpu.to_scipy()
+    R = sp.csc_matrix(A_ref)
+    assert E.shape == R.shape
+    assert np.array_equal(E.indptr, R.indptr)
+    assert np.array_equal(E.indices, R.indices)
+    assert np.array_equal(E.data, R.data.astype(np.float32).astype(np.float64))
+
+
+# ------------------------------------------------------------ matrix generation
+def test_golden_parallel_matrix():
+    g = np.load(os.path.join(GOLD, "paralleltomo_N16_30ang.npz"))
+    A, b, x, *_ = airt.paralleltomo(16, g["theta"])
+    R = sp.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=tuple(g["shape"]))
+    same_matrix(A, R)
+    np.testing.assert_allclose(b, R @ g["x"], rtol=1e-6)
+
+
+def test_golden_fan_matrix():
+    g = np.load(os.path.join(GOLD, "fanlineartomo_N12_30ang.npz"))
+    A, *_ = airt.fanlineartomo(12, np.arange(0.0, 360.0, 12.0), 17)
+    same_matrix(A, sp.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=tuple(g["shape"])))
+
+
+def test_c1_matrix_bit_exact():
+    """N=64, 180 angles, p=91 (the CPU-runnable configuration)."""
+    A, *_ = airt.paralleltomo(64)
+    assert A.shape == (16380, 4096) and A.nnz == 938572
+    same_matrix(A, O.paralleltomo_matrix(64))
+
+
+@pytest.mark.parametrize("N,theta,p,d", [
+    (15, np.arange(0.0, 180.0, 7.5), 21, 18.5),
+    (12, np.array([0, 45, 90, 135, 180, 225, 270, 315.0]), 17, None),
+    (1, np.array([0.0, 30.0]), 3, None),
+])
+def test_parallel_edge_geometries(N, theta, p, d):
+    A, *_ = airt.paralleltomo(N, theta, p, d)
+    same_matrix(A, O.paralleltomo_matrix(N, theta, p, d))
+
+
+def test_fan_matrix_vs_c_oracle():
+    N = 40
+    th, p, R, _, _, ct, st, cw, sw = O.fan_geometry(N, np.arange(0.0, 360.0, 4.0))
+    rows, cols, vals = cbind.trace_coo(N, list(O.fan_rays(N, R, ct, st, cw, sw)), False)
+    Rm = O.coo_to_csc(rows, cols, vals, len(th) * p, N * N)
+    A, *_ = airt.fanlineartomo(N, np.arange(0.0, 360.0, 4.0))
+    same_matrix(A, Rm)
+
+
+def test_c2_matrix_bit_exact_sampled_angles():
+    """N=512, p=724 on 24 of the 360 half-degree angles (full-size rays)."""
+    theta = (np.arange(360) * 0.5)[::15]
+    th, p, d, ct, st, off = O.parallel_geometry(512, theta, 724)
+    rows, cols, vals = cbind.trace_coo(512, list(O.parallel_rays(512, ct, st, off)), True)
+    Rm = O.coo_to_csc(rows, cols, vals, len(th) * p, 512 * 512)
+    A, *_ = airt.paralleltomo(512, theta, 724)
+    same_matrix(A, Rm)
+
+
+def test_csc_upload_roundtrip_and_apply():
+    rng = np.random.default_rng(0)
+    R = sp.random(300, 200, density=0.05, random_state=1, format="csc")
+    R.data = rng.standard_normal(R.nnz)
+    op = airt.afun_matrix(R)
+    same_matrix(op, R)
+    x = rng.standard_normal(200)
+    y = rng.standard_normal(300)
+    R32 = R.copy()
+    R32.data = R32.data.astype(np.float32).astype(np.float64)
+    np.testing.assert_allclose(op(x, "notransp"), R32 @ x, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(op(y, "transp"), R32.T @ y, rtol=1e-12, atol=1e-12)
+    assert list(op(None, "size")) == [300, 200]
+
+
+def test_empty_and_degenerate_matrices():
+    op = airt.afun_matrix(sp.csc_matrix((5, 4)))
+    assert op.nnz == 0
+    np.testing.assert_array_equal(op(np.ones(4), "notransp"), np.zeros(5))
+    np.testing.assert_array_equal(op(np.ones(5), "transp"), np.zeros(4))
+
+
+# ------------------------------------------------------------ matrix-free
+@pytest.mark.parametrize("geo", ["parallel", "fan"])
+def test_matrix_free_equals_stored(geo):
+    rng = np.random.default_rng(3)
+    if geo == "parallel":
+        As, *_ = airt.paralleltomo(48, np.arange(0.0, 180.0, 2.0), None, None, 0, 1)
+        Am, *_ = airt.paralleltomo(48, np.arange(0.0, 180.0, 2.0), None, None, 0, 0)
+    else:
+        As, *_ = airt.fanlineartomo(40, np.arange(0.0, 360.0, 5.0), None, None, None, None, 0, 1)
+        Am, *_ = airt.fanlineartomo(40, np.arange(0.0, 360.0, 5.0), None, None, None, None, 0, 0)
+    assert Am.matrix_free
+    x = rng.random(As.n)
+    y = rng.random(As.m)
+    np.testing.assert_allclose(Am(x, "notransp"), As(x, "notransp"), rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(Am(y, "transp"), As(y, "transp"), rtol=1e-12, atol=1e-11)
+    for meth in ("cimmino", "cav", "drop", "sart"):
+        Ms, Ds = As.weights(meth)
+        Mm, Dm = Am.weights(meth)
+        np.testing.assert_allclose(Mm, Ms, rtol=1e-12)
+        np.testing.assert_allclose(Dm, Ds, rtol=1e-12)
+
+
+def test_matrix_free_sart_equals_stored_sart():
+    """demos/demo_matrixfree.m: SART on the matrix and on the matrix-free
+    operator give the same iterates."""
+    As, b, *_ = airt.paralleltomo(40, np.arange(0.0, 180.0, 3.0))
+    Am, *_ = airt.paralleltomo(40, np.arange(0.0, 180.0, 3.0), None, None, 0, 0)
+    Xs, _ = airt.sart(As, b, 30)
+    Xm, _ = airt.sart(Am, b, 30)
+    assert relerr(Xm, Xs) <= 1e-6
+
+
+# ------------------------------------------------------------ SIRT
+@pytest.fixture(scope="module")
+def c1():
+    A_ref = O.paralleltomo_matrix(64)
+    A, *_ = airt.paralleltomo(64)
+    x = airt.random_ellipses(64, 10, seed=11)
+    b, enorm = airt.add_noise(A_ref @ x, 0.01, seed=12)
+    return A, A_ref, b, enorm, x
+
+
+@pytest.mark.parametrize("method", ["landweber", "cimmino", "cav", "drop", "sart"])
+def test_sirt_methods_c1(c1, method):
+    """C1: 50 iterations, default relaxpar, nonneg=true."""
+    A, A_ref, b, _, _ = c1
+    Xo, io, _ = O.sirt(method, A_ref, b, [10, 50], options={"lbound": 0.0})
+    X, info = airt.sirt(method, A, b, [10, 50], None, {"lbound": 0.0, "rho": io["rho"]})
+    assert X.shape == Xo.shape and info["finaliter"] == 50
+    assert relerr(X[:, 0], Xo[:, 0]) <= RTOL
+    assert relerr(X[:, 1], Xo[:, 1]) <= RTOL
+    assert list(info["itersaved"]) == [10, 50]
+    assert abs(info["relaxpar"] - io["relaxpar"]) <= 1e-12 * abs(io["relaxpar"])
+
+
+@pytest.mark.parametrize("method", ["landweber", "cimmino", "cav", "drop"])
+def test_rho_power_iteration_vs_eigs(c1, method):
+    A, A_ref, b, _, _ = c1
+    _, io, _ = O.sirt(method, A_ref, b, [1])
+    _, info = airt.sirt(method, A, b, [1])
+    assert abs(info["rho"] - io["rho"]) <= 1e-4 * io["rho"]
+
+
+def test_sirt_weights_vs_oracle(c1):
+    A, A_ref, *_ = c1
+    for meth in ("landweber", "cimmino", "cav", "drop", "sart"):
+        M, D = A.weights(meth)
+        Mo, Do, _, _ = O.get_mfun_dfun(meth, A_ref)
+        np.testing.assert_allclose(M, Mo, rtol=1e-6)
+        np.testing.assert_allclose(D, Do, rtol=1e-6)
+
+
+def test_sirt_box_vector_bounds_x0(c1):
+    A, A_ref, b, _, x = c1
+    n = A.n
+    lb = np.zeros(n)
+    ub = np.full(n, 0.8)
+    ub[::7] = 0.3
+    x0 = 0.5 * x
+    opts = {"lbound": lb, "ubound": ub, "rho": 1.0}
+    Xo, _, _ = O.sirt("sart", A_ref, b, [3, 7, 20], x0, opts)
+    X, _ = airt.sart(A, b, [3, 7, 20], x0, opts)
+    assert relerr(X, Xo) <= RTOL
+    assert X.min() >= 0 and np.all(X <= ub[:, None] + 0)
+
+
+@pytest.mark.parametrize("rule", ["line", "psi1", "psi1mod", "psi2", "psi2mod"])
+def test_sirt_relaxation_strategies(c1, rule):
+    A, A_ref, b, _, _ = c1
+    _, io, _ = O.sirt("cimmino", A_ref, b, [1])
+    opts = {"relaxpar": rule, "rho": io["rho"], "lbound": 0.0}
+    Xo, io2, _ = O.sirt("cimmino", A_ref, b, [5, 25], options=opts)
+    X, info = airt.cimmino(A, b, [5, 25], None, opts)
+    assert relerr(X, Xo) <= RTOL
+    assert abs(info["relaxpar"] - io2["relaxpar"]) <= 1e-6 * abs(io2["relaxpar"])
+
+
+def test_sirt_dp_stop(c1):
+    A, A_ref, b, enorm, _ = c1
+    _, io, _ = O.sirt("cimmino", A_ref, b, [1])
+    opts = {"stoprule": {"type": "DP", "taudelta": 1.02 * enorm}, "rho": io["rho"]}
+    Xo, io2, _ = O.sirt("cimmino", A_ref, b, [5, 1000], options=opts)
+    X, info = airt.cimmino(A, b, [5, 1000], None, opts)
+    assert io2["stoprule"] == 2
+    assert info["stoprule"] == 2 and info["finaliter"] == io2["finaliter"]
+    assert relerr(X, Xo) <= RTOL
+    np.testing.assert_allclose(info["resnorms"][1:], io2["resnorms"], rtol=1e-5)
+    assert abs(info["resnorms"][0] - np.linalg.norm(b)) <= 1e-6 * np.linalg.norm(b)
+
+
+def test_sirt_me_stop(c1):
+    A, A_ref, b, enorm, _ = c1
+    opts = {"stoprule": {"type": "ME", "taudelta": 1.02 * enorm}, "rho": 1.0}
+    Xo, io, _ = O.sirt("sart", A_ref, b, [500], options=opts)
+    X, info = airt.sart(A, b, [500], None, opts)
+    assert info["stoprule"] == io["stoprule"] == 3
+    assert info["finaliter"] == io["finaliter"]
+    assert relerr(X, Xo) <= RTOL
+
+
+def test_sirt_dp_at_k0_returns_empty(c1):
+    A, _, b, _, _ = c1
+    X, info = airt.cimmino(A, b, [10], None, {"stoprule": {"type": "DP", "taudelta": 1e12}})
+    assert X.shape == (A.n, 0) and info["finaliter"] == 0 and list(info["itersaved"]) == [0]
+
+
+def test_sirt_custom_weights(c1):
+    A, A_ref, b, _, _ = c1
+    rn = np.asarray(A_ref.multiply(A_ref).sum(axis=1)).ravel()
+    Mc = np.where(rn > 0, 1.0 / np.where(rn > 0, rn, 1), 0.0)
+    Dc = np.linspace(0.5, 1.5, A.n)
+    meth = {"M": sp.diags(Mc), "D": Dc}
+    Xo, io, _ = O.sirt(meth, A_ref, b, [20], options={"rho": 0.9})
+    X, info = airt.sirt(meth, A, b, [20], None, {"rho": 0.9})
+    assert relerr(X, Xo) <= RTOL
+    Xe, _ = airt.sirt({}, A, b, [20], None, {"rho": 20000.0})
+    Xl, _ = airt.landweber(A, b, [20], None, {"rho": 20000.0})
+    np.testing.assert_array_equal(Xe, Xl)
+
+
+def test_sirt_matrix_free_vs_oracle():
+    N = 32
+    theta = np.arange(0.0, 180.0, 4.0)
+    A_ref = O.paralleltomo_matrix(N, theta)
+    Am, *_ = airt.paralleltomo(N, theta, None, None, 0, 0)
+    b, _ = airt.add_noise(A_ref @ O.shepplogan(N), 0.02, seed=4)
+    for meth in ("cimmino", "drop"):
+        Xo, io, _ = O.sirt(meth, A_ref, b, [15], options={"lbound": 0.0})
+        X, _ = airt.sirt(meth, Am, b, [15], None, {"lbound": 0.0, "rho": io["rho"]})
+        assert relerr(X, Xo) <= RTOL
+
+
+def test_sirt_input_errors(c1):
+    A, _, b, _, _ = c1
+    with pytest.raises(ValueError, match="size of A and b"):
+        airt.cimmino(A, b[:-1], 5)
+    with pytest.raises(ValueError, match="strictly increasing"):
+        airt.cimmino(A, b, [5, 5])
+    with pytest.raises(ValueError, match="taudelta"):
+        airt.cimmino(A, b, 5, None, {"stoprule": {"type": "DP"}})
+    with pytest.raises(ValueError, match="only available for SIRT"):
+        airt.kaczmarz(A, b, 2, None, {"stoprule": {"type": "ME", "taudelta": 1.0}})
+    with pytest.raises(ValueError, match="SIRT method not defined"):
+        airt.sirt("nosuch", A, b, 5)
+
+
+# ------------------------------------------------------------ ART
+@pytest.fixture(scope="module")
+def small():
+    g = np.load(os.path.join(GOLD, "paralleltomo_N16_30ang.npz"))
+    A_ref = sp.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=tuple(g["shape"]))
+    return airt.afun_matrix(A_ref), A_ref, g["b"]
+
+
+def test_golden_sirt_and_kaczmarz(small):
+    A, A_ref, b = small
+    s = np.load(os.path.join(GOLD, "solvers_N16_30ang.npz"))
+    for meth in ("landweber", "cimmino", "cav", "drop", "sart"):
+        X, _ = airt.sirt(meth, A, b, [5, 20], None,
+                         {"lbound": 0.0, "ubound": 1.0, "rho": float(s[meth + "_rho"])})
+        assert relerr(X, s[meth + "_X"]) <= RTOL
+    X, info = airt.kaczmarz(A, b, [2, 5], None, {"lbound": 0.0})
+    assert relerr(X, s["kaczmarz_X"]) <= RTOL
+    X, info = airt.symkaczmarz(A, b, [4])
+    assert relerr(X, s["symkaczmarz_X"]) <= RTOL and info["finaliter"] == 4
+
+
+@pytest.mark.parametrize("method", ["kaczmarz", "symkaczmarz"])
+def test_art_vs_oracle_with_options(small, method):
+    A, A_ref, b = small
+    opts = {"lbound": 0.0, "ubound": 0.6, "damp": 0.05, "relaxpar": 0.8}
+    K = [2, 4, 6]
+    Xo, io = O.art(method, A_ref, b, K, 0.3 * np.ones(A.n), opts)
+    X, info = airt.art(method, A, b, K, 0.3 * np.ones(A.n), opts)
+    assert relerr(X, Xo) <= RTOL
+    assert info["finaliter"] == io["finaliter"] and list(info["itersaved"]) == list(io["itersaved"])
+
+
+def test_art_custom_order_and_lambda_handle(small):
+    A, A_ref, b = small
+    order = np.arange(A.m)[::-1]
+    lam = lambda j: 1.0 / np.sqrt(j) + 0.5  # noqa: E731
+    Xo, io = O.art(order, A_ref, b, [3], options={"relaxpar": lam})
+    X, info = airt.art(order, A, b, [3], None, {"relaxpar": lam})
+    assert relerr(X, Xo) <= RTOL
+    assert abs(info["relaxpar"] - lam(2 * A.m + int(order[-1]) + 1)) <= 1e-15
+
+
+def test_randkaczmarz_stream(small):
+    A, A_ref, b = small
+    rn = np.asarray(A_ref.multiply(A_ref).sum(axis=1)).ravel()
+    stream = O.RandStream(21)
+    I = np.flatnonzero(rn > 0)
+    rows = np.stack([O.art_sweep_rows(I, rn, True, stream, A.m)[0] for _ in range(4)])
+    Xo = np.zeros(A.n)
+    for k in range(4):
+        Xo, _ = O.art(rows[k], A_ref, b, [1], Xo)
+        Xo = Xo[:, 0]
+    X, info = airt.randkaczmarz(A, b, [4], None, {"row_stream": rows})
+    assert relerr(X[:, 0], Xo) <= RTOL
+
+
+def test_art_dp_stop_c3_sized():
+    """kaczmarz on N=64 with the DP rule, compared sweep by sweep."""
+    A_ref = O.paralleltomo_matrix(64, np.arange(0.0, 180.0, 2.0))
+    A = airt.afun_matrix(A_ref)
+    b, enorm = airt.add_noise(A_ref @ O.shepplogan(64), 0.02, seed=2)
+    opts = {"stoprule": {"type": "DP", "taudelta": 1.5 * enorm}}
+    Xo, io = O.art("kaczmarz", A_ref, b, list(range(1, 11)), None, opts)
+    X, info = airt.kaczmarz(A, b, list(range(1, 11)), None, opts)
+    assert info["finaliter"] == io["finaliter"] and info["stoprule"] == io["stoprule"]
+    for k in range(X.shape[1]):
+        assert relerr(X[:, k], Xo[:, k]) <= RTOL

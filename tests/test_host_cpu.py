@@ -1,0 +1,113 @@
+"""CPU tests of the host side: the C-ABI library loads and exports every
+symbol include/airt.h declares, argument errors come back as status codes,
+and the host tables/relaxation rules agree with the oracle."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import airtoolsii_b200 as airt
+from airtoolsii_b200 import _lib, solvers, testprobs
+from oracle import airt_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "airt.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(airt_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = _declared()
+    assert len(names) >= 18
+    L = C.CDLL(_lib.LIB_PATH)
+    for nm in names:
+        assert hasattr(L, nm), nm
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+    assert _lib.lib().airt_version() >= 10000
+
+
+def test_bad_csc_is_rejected_without_a_device():
+    L = _lib.lib()
+    h = C.c_void_p()
+    jc = np.array([0, 2, 1], np.uint64)          # decreasing column starts
+    ir = np.array([0, 1], np.uint64)
+    pr = np.array([1.0, 2.0])
+    st = L.airt_problem_from_csc(2, 2, _lib.u64ptr(jc), _lib.u64ptr(ir), _lib.dptr(pr), C.byref(h))
+    assert st == _lib.AIRT_ERR_ARG
+    assert b"nondecreasing" in L.airt_last_error()
+    jc = np.array([1, 2, 2], np.uint64)
+    assert L.airt_problem_from_csc(2, 2, _lib.u64ptr(jc), _lib.u64ptr(ir), _lib.dptr(pr),
+                                   C.byref(h)) == _lib.AIRT_ERR_ARG
+    assert L.airt_problem_from_csc(2, 2, None, None, None, C.byref(h)) == _lib.AIRT_ERR_ARG
+
+
+def test_null_handle_calls_fail_cleanly():
+    L = _lib.lib()
+    x = np.zeros(3)
+    assert L.airt_apply(None, _lib.dptr(x), _lib.dptr(x), 0) == _lib.AIRT_ERR_ARG
+    assert L.airt_problem_size(None, None, None, None) == _lib.AIRT_ERR_ARG
+    assert L.airt_profile_read(None, 0, None, None) == _lib.AIRT_ERR_ARG
+
+
+def test_parallel_tables_match_oracle():
+    for N, theta, p, d in [(64, None, None, None), (512, np.arange(360) * 0.5, 724, None),
+                           (15, np.arange(0.0, 180.0, 7.5), 21, 18.5)]:
+        a = testprobs.parallel_tables(N, theta, p, d)
+        b = O.parallel_geometry(N, theta, p, d)
+        for u, v in zip(a, b):
+            np.testing.assert_array_equal(np.asarray(u), np.asarray(v))
+
+
+def test_fan_tables_match_oracle():
+    for N, theta, p in [(32, None, None), (1024, np.arange(720) * 0.5, 1448), (20, None, 27)]:
+        a = testprobs.fan_tables(N, theta, p)
+        b = O.fan_geometry(N, theta, p)
+        for u, v in zip(a, b):
+            np.testing.assert_array_equal(np.asarray(u), np.asarray(v))
+
+
+def test_shepplogan_matches_oracle():
+    for N in (16, 33, 64):
+        np.testing.assert_array_equal(testprobs.phantomgallery("shepplogan", N).ravel(order="F"),
+                                      O.shepplogan(N))
+
+
+def test_random_ellipses_range_and_determinism():
+    x1 = testprobs.random_ellipses(48, 10, seed=5)
+    x2 = testprobs.random_ellipses(48, 10, seed=5)
+    assert np.array_equal(x1, x2) and x1.min() >= 0 and x1.max() <= 1 and x1.max() > 0
+
+
+@pytest.mark.parametrize("rule", ["psi1", "psi1mod", "psi2", "psi2mod"])
+def test_relaxation_tables_match_oracle(rule):
+    kind, _, tab = solvers._relax_sirt(rule, 0.7, 40)
+    ref, casel, _, _ = O.calc_relaxpar_sirt(rule, 0.7, 40, None, 10)
+    assert kind == casel == 3
+    np.testing.assert_array_equal(tab, ref)
+
+
+def test_default_and_user_relaxpar():
+    kind, lam, _ = solvers._relax_sirt(None, 2.0, 10)
+    assert kind == 1 and lam == 1.9 / 2.0
+    with pytest.warns(UserWarning):
+        solvers._relax_sirt(2.5, 1.0, 10)
+    with pytest.raises(ValueError):
+        solvers._relax_sirt("bogus", 1.0, 10)
+
+
+def test_randk_stream_matches_oracle_stream():
+    rng = np.random.default_rng(1)
+    normAi = rng.random(50) ** 4
+    normAi[[3, 7]] = 0
+    rows, lam_rows = solvers._randk_stream(normAi, 0.0, 3, seed=9)
+    st = O.RandStream(9)
+    I = np.flatnonzero(normAi > 0)
+    for k in range(3):
+        ri, ii = O.art_sweep_rows(I, normAi, True, st, normAi.size)
+        np.testing.assert_array_equal(rows[k], ri)
+        np.testing.assert_array_equal(lam_rows[k], ii)
