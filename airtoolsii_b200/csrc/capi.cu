@@ -1,6 +1,7 @@
 // extern "C" entry points of libairt (declared in include/airt.h).  Each one
 // converts C++ exceptions into a status code plus a thread-local message.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -63,6 +64,8 @@ void prof_collect(Problem &P) {
 
 static Problem *new_problem() {
   Problem *P = new Problem();
+  const char *kind = getenv("AIRT_SPMV");
+  P->spmv_kind = (kind && strcmp(kind, "stream") == 0) ? 1 : 0;
   cudaError_t e = cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete P;
@@ -127,6 +130,7 @@ int airt_problem_from_csc(int64_t m, int64_t n, const uint64_t *jc, const uint64
     P->n = n;
     P->nnz = nnz;
     build_csr_from_host_csc(*P, jc, ir, pr);
+    finalize_matrix(*P);
   } catch (...) {
     free_problem(P);
     throw;

@@ -129,6 +129,18 @@ struct Problem {
   DevBuf<int> ci, ri;
   DevBuf<float> rv, cv;
 
+  // SIRT SpMV kernel family: 0 vectorised gathers (spmv.cuh), 1 bulk-async
+  // streamed tiles (stream.cuh); chosen from AIRT_SPMV=stream at creation
+  int spmv_kind = 0;
+  // tile tables of the streamed kernels (stream.cuh)
+  bool stream_ok = false;
+  DevBuf<int> rtiles, ctiles;
+  int nrtiles = 0, nctiles = 0;
+  DevBuf<int> err;  // device error flag (bounded waits)
+
+  // reusable scratch of the weight and rho computations
+  DevBuf<double> w1, w2;
+
   cudaStream_t stream = nullptr;
 
   // solver work vectors
@@ -189,6 +201,7 @@ void prof_collect(Problem &P);
 // Kernel drivers implemented in the .cu files.
 void build_csc_from_csr(Problem &P);
 void build_csr_from_host_csc(Problem &P, const uint64_t *jc, const uint64_t *ir, const double *pr);
+void finalize_matrix(Problem &P);
 void generate_matrix(Problem &P);
 void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
 void compute_weights(Problem &P, int method, double *dM, double *dD);

@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "spmv.cuh"
+#include "stream.cuh"
 #include "trace.cuh"
 
 namespace airt {
@@ -82,12 +83,25 @@ __device__ __forceinline__ bool stopped(const SirtState *st) {
 }
 
 template <int LANES, bool ME>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     k_sirt_fwd(int64_t m, const int64_t *__restrict__ rp, const int *__restrict__ ci,
                const float *__restrict__ rv, const float *__restrict__ x32, FwdOut o) {
   if (stopped(o.st)) return;
   Acc4 a;
-  for_each_segment<LANES>(m, rp, ci, rv, x32, [&](int64_t i, double s, bool lead) {
+  for_each_segment_v<LANES>(m, rp, ci, rv, x32, [&](int64_t i, double s, bool lead) {
+    if (lead) resid_row<ME>(i, s, o, a);
+  });
+  flush<ME>(o.st, a);
+}
+
+// Streamed variants (stream.cuh): same epilogues, tiles of the CSR / CSC
+// brought into shared memory by bulk-async copies.
+template <bool ME>
+__global__ void __launch_bounds__(kStreamThreads, kStreamCtasPerSm)
+    k_sirt_fwd_stream(StreamArgs sa, FwdOut o) {
+  if (stopped(o.st)) return;
+  Acc4 a;
+  stream_segments(sa, [&](int64_t i, double s, bool lead) {
     if (lead) resid_row<ME>(i, s, o, a);
   });
   flush<ME>(o.st, a);
@@ -151,7 +165,7 @@ __device__ __forceinline__ void update_x(int64_t j, double g, double lam, const 
 // MODE 0: fused update with st->lam_cur.  MODE 1: line-search pass that
 // stores g and accumulates sum(D.*g.^2) (sirt.m:219-222).
 template <int LANES, int MODE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     k_sirt_bwd(int64_t n, const int64_t *__restrict__ cp, const int *__restrict__ ri,
                const float *__restrict__ cv, const float *__restrict__ mr32, UpdArgs u) {
   if (stopped(u.st)) return;
@@ -159,7 +173,7 @@ __global__ void __launch_bounds__(kThreads)
   const int slot = u.save_slot[it];
   const double lam = u.st->lam_cur;
   double a4 = 0;
-  for_each_segment<LANES>(n, cp, ri, cv, mr32, [&](int64_t j, double g, bool lead) {
+  for_each_segment_v<LANES>(n, cp, ri, cv, mr32, [&](int64_t j, double g, bool lead) {
     if (!lead) return;
     if (MODE == 0) {
       update_x(j, g, lam, u, slot);
@@ -170,6 +184,29 @@ __global__ void __launch_bounds__(kThreads)
   });
   if (MODE == 1) {
     a4 = block_sum<kThreads>(a4);
+    if (threadIdx.x == 0) atomicAdd(&u.st->acc[4], a4);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kStreamThreads, kStreamCtasPerSm)
+    k_sirt_bwd_stream(StreamArgs sa, UpdArgs u) {
+  if (stopped(u.st)) return;
+  const int it = u.st->iter;
+  const int slot = u.save_slot[it];
+  const double lam = u.st->lam_cur;
+  double a4 = 0;
+  stream_segments(sa, [&](int64_t j, double g, bool lead) {
+    if (!lead) return;
+    if (MODE == 0) {
+      update_x(j, g, lam, u, slot);
+    } else {
+      u.g64[j] = g;
+      a4 += u.D[j] * (g * g);
+    }
+  });
+  if (MODE == 1) {
+    a4 = block_sum<kStreamThreads>(a4);
     if (threadIdx.x == 0) atomicAdd(&u.st->acc[4], a4);
   }
 }
@@ -266,22 +303,56 @@ __global__ void k_copy(int64_t n, const double *__restrict__ a, double *__restri
 }
 
 // ---------------------------------------------------------------- launchers
+StreamArgs stream_args(Problem &P, bool rows, const float *gvec) {
+  StreamArgs a;
+  a.nseg = rows ? P.m : P.n;
+  a.ptr = rows ? P.rp.p : P.cp.p;
+  a.idx = rows ? P.ci.p : P.ri.p;
+  a.val = rows ? P.rv.p : P.cv.p;
+  a.gvec = gvec;
+  a.tile_seg = rows ? P.rtiles.p : P.ctiles.p;
+  a.ntiles = rows ? P.nrtiles : P.nctiles;
+  a.err = P.err.p;
+  return a;
+}
+
+template <class K>
+unsigned stream_grid(K kernel, int ntiles) {
+  static bool attr = false;
+  (void)attr;
+  AIRT_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)stream_smem_bytes()));
+  int g = kStreamCtasPerSm * num_sms();
+  return (unsigned)(ntiles < g ? ntiles : g);
+}
+
+#define AIRT_STREAM_LAUNCH(KERNEL, NT, ...)                                              \
+  do {                                                                                  \
+    auto kfn = KERNEL;                                                                  \
+    const unsigned g_ = stream_grid(kfn, NT);                                           \
+    kfn<<<g_, kStreamThreads, stream_smem_bytes(), s>>>(__VA_ARGS__);                   \
+  } while (0)
+
 template <bool ME>
 void launch_fwd_t(Problem &P, const FwdOut &o) {
   cudaStream_t s = P.stream;
+  if (P.spmv_kind == 1 && P.stream_ok && !P.matrix_free) {
+    const StreamArgs sa = stream_args(P, true, P.x32.p);
+    AIRT_STREAM_LAUNCH((k_sirt_fwd_stream<ME>), sa.ntiles, sa, o);
+    return;
+  }
   if (P.matrix_free) {
     k_sirt_fwd_mf<ME><<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m,
                                                               P.geo_kind == GEO_PARALLEL,
                                                               P.x32.p, o);
     return;
   }
-  const int L = lanes_for(P.nnz, P.m);
-  const unsigned g = grid_for(P.m * L, kThreads);
+  const int L = vec_lanes_for(P.nnz, P.m);
+  const unsigned g = grid_for(P.m * L, kThreads, 4);
   switch (L) {
-    case 32: k_sirt_fwd<32, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
-    case 16: k_sirt_fwd<16, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
     case 8: k_sirt_fwd<8, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
-    default: k_sirt_fwd<4, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    case 4: k_sirt_fwd<4, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    default: k_sirt_fwd<2, ME><<<g, kThreads, 0, s>>>(P.m, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
   }
 }
 
@@ -297,13 +368,17 @@ void launch_fwd(Problem &P, const FwdOut &o, bool me) {
 template <int MODE>
 void launch_bwd_t(Problem &P, const UpdArgs &u) {
   cudaStream_t s = P.stream;
-  const int L = lanes_for(P.nnz, P.n);
-  const unsigned g = grid_for(P.n * L, kThreads);
+  if (P.spmv_kind == 1 && P.stream_ok) {
+    const StreamArgs sa = stream_args(P, false, P.mr32.p);
+    AIRT_STREAM_LAUNCH((k_sirt_bwd_stream<MODE>), sa.ntiles, sa, u);
+    return;
+  }
+  const int L = vec_lanes_for(P.nnz, P.n);
+  const unsigned g = grid_for(P.n * L, kThreads, 4);
   switch (L) {
-    case 32: k_sirt_bwd<32, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
-    case 16: k_sirt_bwd<16, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
     case 8: k_sirt_bwd<8, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
-    default: k_sirt_bwd<4, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    case 4: k_sirt_bwd<4, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    default: k_sirt_bwd<2, MODE><<<g, kThreads, 0, s>>>(P.n, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
   }
 }
 
@@ -356,6 +431,9 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   AIRT_CHECK_CUDA(cudaEventCreate(&t0));
   AIRT_CHECK_CUDA(cudaEventCreate(&t1));
   AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
+
+  P.err.ensure(1);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.err.p, 0, sizeof(int), s));
 
   // weights (get_mfun_dfun.m)
   P.M.ensure(m);
@@ -444,11 +522,16 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
 
   // main loop, enqueued in chunks; the flag of chunk c is read after chunk
   // c+1 has been queued so the device never idles on the poll
-  if (!P.h_state) AIRT_CHECK_CUDA(cudaMallocHost(&P.h_state, 2 * sizeof(SirtState)));
-  cudaEvent_t ev[2];
-  AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  if (!P.h_state) AIRT_CHECK_CUDA(cudaMallocHost(&P.h_state, 3 * sizeof(SirtState)));
+  cudaEvent_t ev[3];
+  for (int q = 0; q < 3; ++q)
+    AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming));
+  // Without a data-dependent stopping rule every iteration runs: enqueue
+  // them all.  Otherwise poll the flag of chunk c once chunk c+2 is queued,
+  // so host-side stalls never drain the device queue.
+  const bool poll = o.stoprule != AIRT_STOP_NONE;
   const int64_t chunk = 16;
+  const int lag = 2;
   int64_t c = 0;
   for (int64_t it = 1; it <= kmax; ++c) {
     const int64_t cnt = (kmax - it + 1 < chunk) ? (kmax - it + 1) : chunk;
@@ -459,19 +542,25 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
     }
     AIRT_LAUNCH_CHECK();
     it += cnt;
-    AIRT_CHECK_CUDA(cudaMemcpyAsync(P.h_state + (c & 1), P.state.p, sizeof(SirtState),
+    if (!poll) continue;
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(P.h_state + (c % 3), P.state.p, sizeof(SirtState),
                                     cudaMemcpyDeviceToHost, s));
-    AIRT_CHECK_CUDA(cudaEventRecord(ev[c & 1], s));
-    if (c >= 1) {
-      AIRT_CHECK_CUDA(cudaEventSynchronize(ev[(c - 1) & 1]));
-      if (P.h_state[(c - 1) & 1].stop) break;
+    AIRT_CHECK_CUDA(cudaEventRecord(ev[c % 3], s));
+    if (c >= lag) {
+      AIRT_CHECK_CUDA(cudaEventSynchronize(ev[(c - lag) % 3]));
+      if (P.h_state[(c - lag) % 3].stop) break;
     }
   }
   AIRT_CHECK_CUDA(cudaMemcpyAsync(P.h_state, P.state.p, sizeof(SirtState), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
+  for (int q = 0; q < 3; ++q) cudaEventDestroy(ev[q]);
   const SirtState st = P.h_state[0];
+  int herr = 0;
+  AIRT_CHECK_CUDA(cudaMemcpy(&herr, P.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (herr) {
+    set_error("a bounded device wait gave up (bulk copy did not complete)");
+    throw Status{AIRT_ERR_TIMEOUT};
+  }
   AIRT_REQUIRE(st.stop, "internal: SIRT loop ended without a stop");
 
   // X keeps the iterates in K below finaliter plus the final one (sirt.m:270)

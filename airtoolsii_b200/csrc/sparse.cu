@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "spmv.cuh"
+#include "stream.cuh"
 
 namespace airt {
 
@@ -81,9 +82,12 @@ __global__ void k_u64_to_i64(int64_t n, const uint64_t *__restrict__ a, int64_t 
 void transpose(int64_t nmaj, int64_t nmin, int64_t nnz, const int64_t *ptr_in, const int *minor_in,
                const float *val_in, DevBuf<int64_t> &ptr_out, DevBuf<int> &minor_out,
                DevBuf<float> &val_out, cudaStream_t s) {
-  ptr_out.ensure(nmin + 1);
-  minor_out.ensure(nnz);
-  val_out.ensure(nnz);
+  ptr_out.ensure(nmin + 1 + kPtrPad);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(ptr_out.p + nmin + 1, 0, kPtrPad * sizeof(int64_t), s));
+  minor_out.ensure(nnz + kPad);
+  val_out.ensure(nnz + kPad);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(minor_out.p + nnz, 0, kPad * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(val_out.p + nnz, 0, kPad * sizeof(float), s));
   if (nnz == 0) {
     AIRT_CHECK_CUDA(cudaMemsetAsync(ptr_out.p, 0, (nmin + 1) * sizeof(int64_t), s));
     return;
@@ -121,6 +125,42 @@ void transpose(int64_t nmaj, int64_t nmin, int64_t nnz, const int64_t *ptr_in, c
 
 }  // namespace
 
+// Greedy tiles of whole segments: a tile closes before the segment that
+// would push it past kTileNnz nonzeros or kTileSeg segments.
+bool build_tiles(Problem &P, const int64_t *d_ptr, int64_t nseg, DevBuf<int> &tiles, int &ntiles) {
+  ntiles = 0;
+  if (nseg <= 0 || nseg >= INT32_MAX) return false;
+  std::vector<int64_t> h(nseg + 1);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(h.data(), d_ptr, (nseg + 1) * sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, P.stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  std::vector<int> ts;
+  ts.push_back(0);
+  int64_t tile_e0 = h[0];
+  int tile_nseg = 0;
+  for (int64_t i = 0; i < nseg; ++i) {
+    const int64_t len = h[i + 1] - h[i];
+    if (len > kTileNnz) return false;
+    if (tile_nseg == kTileSeg || h[i + 1] - tile_e0 > kTileNnz) {
+      ts.push_back((int)i);
+      tile_e0 = h[i];
+      tile_nseg = 0;
+    }
+    ++tile_nseg;
+  }
+  ts.push_back((int)nseg);
+  if (ts.size() >= (size_t)INT32_MAX) return false;
+  ntiles = (int)ts.size() - 1;
+  tiles.upload(ts.data(), ts.size(), P.stream);
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  return true;
+}
+
+void finalize_matrix(Problem &P) {
+  P.stream_ok = build_tiles(P, P.rp.p, P.m, P.rtiles, P.nrtiles) &&
+                build_tiles(P, P.cp.p, P.n, P.ctiles, P.nctiles);
+}
+
 void build_csc_from_csr(Problem &P) {
   transpose(P.m, P.n, P.nnz, P.rp.p, P.ci.p, P.rv.p, P.cp, P.ri, P.cv, P.stream);
 }
@@ -132,9 +172,12 @@ void build_csr_from_host_csc(Problem &P, const uint64_t *jc, const uint64_t *ir,
   djc.upload(jc, P.n + 1, s);
   dir.upload(ir, P.nnz, s);
   dpr.upload(pr, P.nnz, s);
-  P.cp.ensure(P.n + 1);
-  P.ri.ensure(P.nnz);
-  P.cv.ensure(P.nnz);
+  P.cp.ensure(P.n + 1 + kPtrPad);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.cp.p + P.n + 1, 0, kPtrPad * sizeof(int64_t), s));
+  P.ri.ensure(P.nnz + kPad);
+  P.cv.ensure(P.nnz + kPad);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.ri.p + P.nnz, 0, kPad * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.cv.p + P.nnz, 0, kPad * sizeof(float), s));
   DevBuf<int> bad;
   bad.ensure(1);
   AIRT_CHECK_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
@@ -274,7 +317,7 @@ void row_col_stats_mf(Problem &P, double *s2, double *s1, double *colcnt, double
 void compute_weights(Problem &P, int method, double *dM, double *dD) {
   cudaStream_t s = P.stream;
   const int64_t m = P.m, n = P.n;
-  DevBuf<double> t1, t2;
+  DevBuf<double> &t1 = P.w1, &t2 = P.w2;
   t1.ensure(m > n ? m : n);
   t2.ensure(n);
   auto rows = [&](double *s2, double *s1, const double *colw, double *s2w) {
@@ -325,7 +368,6 @@ void compute_weights(Problem &P, int method, double *dM, double *dD) {
       AIRT_REQUIRE(false, "SIRT method not defined.");
   }
   AIRT_LAUNCH_CHECK();
-  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
 }
 
 // ------------------------------------------------------------------ apply

@@ -45,13 +45,68 @@ __device__ __forceinline__ void for_each_segment(int64_t nseg, const int64_t *__
   }
 }
 
+// Vectorised variant: the 4-aligned body of each segment is read with 16-byte
+// loads (float4 values, int4 indices; the arrays are padded and 16-byte
+// aligned), one vector per lane per round, and a warp carries 32/LANES
+// segments at once so that many independent loads and gathers are in flight
+// per SM (narrow groups measured best on B200: 8 lanes per ~460-entry ray).
+// The unaligned head and tail (< 4 elements each) are read element-wise.
+template <int LANES, typename TX, class Epi>
+__device__ __forceinline__ void for_each_segment_v(int64_t nseg, const int64_t *__restrict__ ptr,
+                                                   const int *__restrict__ idx,
+                                                   const float *__restrict__ val,
+                                                   const TX *__restrict__ x, Epi &&epi) {
+  const int lane = threadIdx.x % LANES;
+  const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / LANES;
+  const int64_t ng = (int64_t)gridDim.x * blockDim.x / LANES;
+  const int64_t trips = (nseg + ng - 1) / ng;
+  const float4 *__restrict__ V4 = reinterpret_cast<const float4 *>(val);
+  const int4 *__restrict__ I4 = reinterpret_cast<const int4 *>(idx);
+  for (int64_t t = 0; t < trips; ++t) {
+    const int64_t i = gid + t * ng;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (i < nseg) {
+      const int64_t q0 = __ldg(ptr + i), q1 = __ldg(ptr + i + 1);
+      int64_t qa = (q0 + 3) & ~(int64_t)3;
+      if (qa > q1) qa = q1;
+      int64_t qb = q1 & ~(int64_t)3;
+      if (qb < qa) qb = qa;
+      for (int64_t q = q0 + lane; q < qa; q += LANES)
+        a0 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a0);
+      for (int64_t q = qb + lane; q < q1; q += LANES)
+        a1 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a1);
+      const int64_t ve = qb >> 2;
+      for (int64_t v = (qa >> 2) + lane; v < ve; v += LANES) {
+        const float4 f = __ldg(V4 + v);
+        const int4 c = __ldg(I4 + v);
+        const TX g0 = __ldg(x + c.x), g1 = __ldg(x + c.y), g2 = __ldg(x + c.z), g3 = __ldg(x + c.w);
+        a0 = fma((double)f.x, (double)g0, a0);
+        a1 = fma((double)f.y, (double)g1, a1);
+        a2 = fma((double)f.z, (double)g2, a2);
+        a3 = fma((double)f.w, (double)g3, a3);
+      }
+    }
+    double acc = (a0 + a1) + (a2 + a3);
+    acc = group_sum<LANES>(acc);
+    epi(i, acc, lane == 0 && i < nseg);
+  }
+}
+
+// Lanes per segment of the vectorised kernels from the mean segment length.
+inline int vec_lanes_for(int64_t nnz, int64_t nseg) {
+  const double avg = nseg ? (double)nnz / (double)nseg : 0.0;
+  if (avg > 128) return 8;
+  if (avg > 16) return 4;
+  return 2;
+}
+
 template <int LANES>
-__global__ void __launch_bounds__(256) k_spmv_plain(int64_t nseg, const int64_t *__restrict__ ptr,
-                                                    const int *__restrict__ idx,
-                                                    const float *__restrict__ val,
-                                                    const double *__restrict__ x,
-                                                    double *__restrict__ y) {
-  for_each_segment<LANES>(nseg, ptr, idx, val, x, [&](int64_t i, double s, bool lead) {
+__global__ void __launch_bounds__(256, 4) k_spmv_plain(int64_t nseg, const int64_t *__restrict__ ptr,
+                                                       const int *__restrict__ idx,
+                                                       const float *__restrict__ val,
+                                                       const double *__restrict__ x,
+                                                       double *__restrict__ y) {
+  for_each_segment_v<LANES>(nseg, ptr, idx, val, x, [&](int64_t i, double s, bool lead) {
     if (lead) y[i] = s;
   });
 }
@@ -70,13 +125,12 @@ inline void spmv_plain(int64_t nseg, const int64_t *ptr, const int *idx, const f
   int64_t nnz = 0;
   AIRT_CHECK_CUDA(cudaMemcpyAsync(&nnz, ptr + nseg, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-  const int L = lanes_for(nnz, nseg);
-  const unsigned g = grid_for(nseg * L, 256);
+  const int L = vec_lanes_for(nnz, nseg);
+  const unsigned g = grid_for(nseg * L, 256, 4);
   switch (L) {
-    case 32: k_spmv_plain<32><<<g, 256, 0, s>>>(nseg, ptr, idx, val, x, y); break;
-    case 16: k_spmv_plain<16><<<g, 256, 0, s>>>(nseg, ptr, idx, val, x, y); break;
     case 8: k_spmv_plain<8><<<g, 256, 0, s>>>(nseg, ptr, idx, val, x, y); break;
-    default: k_spmv_plain<4><<<g, 256, 0, s>>>(nseg, ptr, idx, val, x, y); break;
+    case 4: k_spmv_plain<4><<<g, 256, 0, s>>>(nseg, ptr, idx, val, x, y); break;
+    default: k_spmv_plain<2><<<g, 256, 0, s>>>(nseg, ptr, idx, val, x, y); break;
   }
   AIRT_LAUNCH_CHECK();
 }

@@ -14,6 +14,7 @@
 //    up to summation order.
 #include "common.cuh"
 #include "spmv.cuh"
+#include "stream.cuh"
 #include "trace.cuh"
 
 namespace airt {
@@ -123,18 +124,22 @@ void generate_matrix(Problem &P) {
   const unsigned grid = grid_for(nrays, 128, 16);
   k_trace_count<<<grid, 128, 0, s>>>(g, nrays, excl_of(P), counts.p, bad.p);
   AIRT_LAUNCH_CHECK();
-  P.rp.ensure(nrays + 1);
+  P.rp.ensure(nrays + 1 + kPtrPad);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.rp.p + nrays + 1, 0, kPtrPad * sizeof(int64_t), s));
   exclusive_scan_i64(counts.p, P.rp.p, nrays, s);
   int hbad = 0;
   AIRT_CHECK_CUDA(cudaMemcpyAsync(&P.nnz, P.rp.p + nrays, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   AIRT_REQUIRE(!hbad, "ray trace produced a pixel index outside the image");
-  P.ci.ensure(P.nnz);
-  P.rv.ensure(P.nnz);
+  P.ci.ensure(P.nnz + kPad);
+  P.rv.ensure(P.nnz + kPad);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.ci.p + P.nnz, 0, kPad * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.rv.p + P.nnz, 0, kPad * sizeof(float), s));
   k_trace_fill<<<grid, 128, 0, s>>>(g, nrays, excl_of(P), P.rp.p, P.ci.p, P.rv.p);
   AIRT_LAUNCH_CHECK();
   build_csc_from_csr(P);
+  finalize_matrix(P);
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
 }
 

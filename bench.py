@@ -12,7 +12,7 @@ divided by the step's device time.  Inputs exceed L2 (A is ~1.9 GB), so no
 extra L2 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl airt|reference]
-                  [--small]  (N=128 case for ncu captures)
+                  [--small]  (N=256 case for ncu captures; A ~0.25 GB > L2)
 """
 from __future__ import annotations
 
@@ -39,14 +39,14 @@ def parse():
     ap.add_argument("--impl", default="airt", choices=["airt", "reference"])
     ap.add_argument("--method", default="cimmino")
     ap.add_argument("--iters", type=int, default=200)
-    ap.add_argument("--small", action="store_true", help="N=128 problem (profiling captures)")
+    ap.add_argument("--small", action="store_true", help="N=256 problem (profiling captures)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     return ap.parse_args()
 
 
 def workload(small: bool):
     if small:
-        return dict(N=128, nA=180, p=181, step=1.0, ellipses=30, eta=0.005)
+        return dict(N=256, nA=360, p=362, step=0.5, ellipses=30, eta=0.005)
     return dict(N=512, nA=360, p=724, step=0.5, ellipses=30, eta=0.005)
 
 
@@ -107,10 +107,13 @@ class Clocks:
 
 
 def cpu_leg(A_csc, b, M, D, lam, iters, m, n, nnz):
-    """FP64 C restatement (OpenMP, all host threads) on a bounded sample."""
+    """FP64 C restatement (OpenMP, all host threads) on a bounded sample;
+    only the iterations are timed."""
     from oracle import cbind
+    prep = cbind.PreparedSirt(A_csc, b, M, D)
+    prep.run(lam, 0.0, 1.0, 1)
     t0 = time.perf_counter()
-    x, k, _ = cbind.sirt_csr(A_csc.tocsr(), b, M, D, lam, 0.0, 1.0, None, iters)
+    prep.run(lam, 0.0, 1.0, iters)
     dt = time.perf_counter() - t0
     return {"value": model_bytes(nnz, m, n) * iters / dt / 1e9, "unit": "GB/s",
             "cores": cbind.num_threads(), "kind": "port",
@@ -129,7 +132,7 @@ def main():
            "N": wl["N"], "angles": wl["nA"], "rays": wl["p"], "method": a.method,
            "iterations": a.iters, "phantom": f"{wl['ellipses']} random ellipses",
            "noise": wl["eta"], "l2": "inputs larger than L2 (A ~1.9 GB)" if not a.small else
-           "N=128 case", "parallelism": f"replicas x{a.gpus}"}
+           "inputs larger than L2 (A ~0.25 GB)", "parallelism": f"replicas x{a.gpus}"}
     metric = "SIRT SpMV HBM GB/s (CSR+CSC byte model, plain GPU SIRT)"
 
     if a.impl == "reference":
@@ -216,10 +219,10 @@ def main():
             ms = float(t.item())
         return ms
 
+    clocks = Clocks(local)
+    clocks.start()                    # sampler runs from before warm-up to the end
     for _ in range(max(a.warmup, 3)):
         step_device()
-    clocks = Clocks(local)
-    clocks.start()
     ms_dev = timed(step_device, a.steps)
     ck = clocks.stop()
     for _ in range(2):
@@ -292,7 +295,7 @@ def main():
         }
         if not a.no_cpu and world == 1:
             M, D = A.weights(a.method)
-            line["cpu_baseline"] = cpu_leg(A.to_scipy(), b, M, D, lam, 2 if not a.small else 10,
+            line["cpu_baseline"] = cpu_leg(A.to_scipy(), b, M, D, lam, 5 if not a.small else 20,
                                            m, n, nnz)
         print(json.dumps(line), flush=True)
         del x_gpu
@@ -320,13 +323,13 @@ def reference_arm(a, wl, cfg, metric):
     b, _ = add_noise(A @ x, wl["eta"], seed=200)
     M, D, _, _ = O.get_mfun_dfun(a.method, A)
     lam = 1.0
-    sample = 1 if not a.small else 5
-    Acsr = A.tocsr()
-    for _ in range(max(a.warmup, 3) if a.small else 1):
-        cbind.sirt_csr(Acsr, b, M, D, lam, 0.0, 1.0, None, sample)
+    sample = 2 if not a.small else 10
+    prep = cbind.PreparedSirt(A, b, M, D)
+    for _ in range(max(a.warmup, 3)):
+        prep.run(lam, 0.0, 1.0, 1)
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        cbind.sirt_csr(Acsr, b, M, D, lam, 0.0, 1.0, None, sample)
+        prep.run(lam, 0.0, 1.0, sample)
     dt = time.perf_counter() - t0
     v = model_bytes(nnz, m, n) * sample * a.steps / dt / 1e9
     line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "GB/s",

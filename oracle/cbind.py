@@ -66,6 +66,35 @@ def trace_coo(N, rays, exclude):
     return rows, cols, vals
 
 
+class PreparedSirt:
+    """FP64 CSR + CSC arrays of A prepared once, so that timing covers only
+    the C iterations (oracle_sirt_csr)."""
+
+    def __init__(self, A, b, M, D):
+        A = sp.csr_matrix(A, dtype=np.float64)
+        Ac = A.tocsc()
+        self.m, self.n = A.shape
+        self.rp = A.indptr.astype(np.int64)
+        self.ci = A.indices.astype(np.int64)
+        self.rv = np.ascontiguousarray(A.data)
+        self.cp = Ac.indptr.astype(np.int64)
+        self.ri = Ac.indices.astype(np.int64)
+        self.cv = np.ascontiguousarray(Ac.data)
+        self.b = np.ascontiguousarray(b, np.float64)
+        self.M = np.ascontiguousarray(M, np.float64)
+        self.D = np.ascontiguousarray(D, np.float64)
+
+    def run(self, lam, lb, ub, kmax, taudelta=None):
+        x = np.zeros(self.n)
+        resn = np.zeros(kmax + 1)
+        k = lib().oracle_sirt_csr(self.m, self.n, self.rp, self.ci, self.rv, self.cp, self.ri,
+                                  self.cv, self.b, self.M, self.D, float(lam),
+                                  float("nan") if lb is None else float(lb),
+                                  float("nan") if ub is None else float(ub),
+                                  -1.0 if taudelta is None else float(taudelta), int(kmax), x, resn)
+        return x, k, resn[:k + 1]
+
+
 def sirt_csr(A, b, M, D, lam, lb, ub, taudelta, kmax, x0=None):
     """FP64 SIRT with constant relaxpar (see oracle_sirt_csr).  Returns
     (x, finaliter, resnorms)."""

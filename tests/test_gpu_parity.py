@@ -238,9 +238,11 @@ def test_sirt_custom_weights(c1):
     Mc = np.where(rn > 0, 1.0 / np.where(rn > 0, rn, 1), 0.0)
     Dc = np.linspace(0.5, 1.5, A.n)
     meth = {"M": sp.diags(Mc), "D": Dc}
-    Xo, io, _ = O.sirt(meth, A_ref, b, [20], options={"rho": 0.9})
-    X, info = airt.sirt(meth, A, b, [20], None, {"rho": 0.9})
+    Xo, io, _ = O.sirt(meth, A_ref, b, [20])
+    X, info = airt.sirt(meth, A, b, [20], None, {"rho": io["rho"]})
     assert relerr(X, Xo) <= RTOL
+    _, info2 = airt.sirt(meth, A, b, [1])
+    assert abs(info2["rho"] - io["rho"]) <= 1e-4 * io["rho"]
     Xe, _ = airt.sirt({}, A, b, [20], None, {"rho": 20000.0})
     Xl, _ = airt.landweber(A, b, [20], None, {"rho": 20000.0})
     np.testing.assert_array_equal(Xe, Xl)
@@ -311,7 +313,9 @@ def test_art_custom_order_and_lambda_handle(small):
     Xo, io = O.art(order, A_ref, b, [3], options={"relaxpar": lam})
     X, info = airt.art(order, A, b, [3], None, {"relaxpar": lam})
     assert relerr(X, Xo) <= RTOL
-    assert abs(info["relaxpar"] - lam(2 * A.m + int(order[-1]) + 1)) <= 1e-15
+    rn = np.asarray(A_ref.multiply(A_ref).sum(axis=1)).ravel()
+    last = order[rn[order] > 0][-1]
+    assert abs(info["relaxpar"] - lam(2 * A.m + int(last) + 1)) <= 1e-15
 
 
 def test_randkaczmarz_stream(small):
