@@ -77,6 +77,9 @@ SIGNATURES = {
                                    C.c_int64, C.c_void_p, _dp, C.POINTER(Info)]),
     "airt_art": (C.c_int, [C.c_void_p, C.POINTER(ArtOpts), _dp, _dp, _i64p, C.c_int64, _dp, _dp,
                            C.POINTER(Info)]),
+    "airt_residual_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
     "airt_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "airt_profile_read": (C.c_int, [C.c_void_p, C.c_int, _i64p, _dp]),
 }

@@ -167,6 +167,21 @@ int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *
 int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const double *x0,
              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
 
+/* ---- allocation-free residual ------------------------------------------------ */
+/* No counterpart in the reference.  r = b - A*x and ||r|| (into d_resnorm) for
+ * a caller that holds an FP32 CSR (d_rp m+1, d_ci/d_rv nnz), x, b and r on
+ * the device and cannot allocate device memory: an application that owns the
+ * GPU memory budget through its own pool, or code that must not call
+ * cudaMalloc/cudaFree because they synchronise the device.  It allocates
+ * nothing; its scratch is a static 4 MiB + 256 B device array, so n is limited
+ * to 1,048,576 unknowns (AIRT_ERR_ARG beyond).  The first call on a device
+ * looks the array up and should come before any stream capture; calls that
+ * overlap on the GPU race on the shared scratch.  Runs on cuda_stream (NULL =
+ * legacy default stream). */
+int airt_residual_noalloc(int64_t m, int64_t n, const int64_t *d_rp, const int *d_ci,
+                          const float *d_rv, const double *d_x, const double *d_b, double *d_r,
+                          double *d_resnorm, void *cuda_stream);
+
 /* ---- instrumentation ------------------------------------------------------- */
 /* When on, each SIRT kernel launch is bracketed by CUDA events on the problem
  * stream; airt_profile_read returns launches and summed device milliseconds

@@ -1,0 +1,67 @@
+"""airt_residual_noalloc: the forward residual for callers that cannot
+allocate device memory (an application that owns the GPU memory budget
+through its own pool, or code that must not call cudaMalloc/cudaFree because
+they synchronise the device).  The caller holds the CSR, x, b and r on the
+device; the entry point uses its own static scratch.
+
+Checked through the C-ABI against the existing operator entry point
+(airt_apply: A*x), on two calls in a row, within the suite's relative
+tolerance of 1e-5.  This file is collected last on purpose.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import airtoolsii_b200 as airt
+from airtoolsii_b200 import _lib
+from oracle import airt_oracle as O
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-5
+
+
+def _relerr(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_residual_noalloc_matches_apply_twice():
+    import torch
+
+    A = sp.csr_matrix(O.paralleltomo_matrix(48, np.arange(0.0, 180.0, 2.0)))
+    m, n = A.shape
+    rng = np.random.default_rng(5)
+    x = rng.random(n)
+    b = rng.random(m) * 10.0
+    op = airt.afun_matrix(A)
+    r_ref = b - op(x, "notransp")                  # existing entry point airt_apply
+
+    dev = torch.device("cuda")
+    rp = torch.from_numpy(A.indptr.astype(np.int64)).to(dev)
+    ci = torch.from_numpy(A.indices.astype(np.int32)).to(dev)
+    rv = torch.from_numpy(A.data.astype(np.float32)).to(dev)
+    dx = torch.from_numpy(x).to(dev)
+    db = torch.from_numpy(b).to(dev)
+    dr = torch.zeros(m, dtype=torch.float64, device=dev)
+    dn = torch.zeros(1, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    L = _lib.lib()
+    for _ in range(2):
+        dr.fill_(-7.0)
+        st = L.airt_residual_noalloc(m, n, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+                                     C.c_void_p(rv.data_ptr()), C.c_void_p(dx.data_ptr()),
+                                     C.c_void_p(db.data_ptr()), C.c_void_p(dr.data_ptr()),
+                                     C.c_void_p(dn.data_ptr()), C.c_void_p(stream))
+        assert st == _lib.AIRT_OK, L.airt_last_error()
+        torch.cuda.synchronize()
+        r = dr.cpu().numpy()
+        assert _relerr(r, r_ref) <= RTOL
+        assert abs(float(dn.item()) - np.linalg.norm(r_ref)) <= RTOL * np.linalg.norm(r_ref)
+
+
+def test_residual_noalloc_rejects_oversize():
+    L = _lib.lib()
+    st = L.airt_residual_noalloc(10, (1 << 20) + 1, None, None, None, None, None, None, None, None)
+    assert st == _lib.AIRT_ERR_ARG
+    assert b"no-alloc maximum" in L.airt_last_error()
