@@ -77,6 +77,20 @@ SIGNATURES = {
                                    C.c_int64, C.c_void_p, _dp, C.POINTER(Info)]),
     "airt_art": (C.c_int, [C.c_void_p, C.POINTER(ArtOpts), _dp, _dp, _i64p, C.c_int64, _dp, _dp,
                            C.POINTER(Info)]),
+    "airt_batch_parallel": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int), _dp, _dp, _dp, C.POINTER(C.c_void_p)]),
+    "airt_batch_layout": (C.c_int, [C.c_void_p, _i64p, _i64p, _i64p]),
+    "airt_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "airt_batch_rho": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, _dp]),
+    "airt_batch_sirt": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int64, C.c_int,
+                                  C.c_double, C.c_int, C.c_double, _dp, _dp, _i64p,
+                                  C.POINTER(C.c_int), _dp]),
+    "airt_batch_sirt_device": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_void_p, _dp, C.c_int64,
+                                         C.c_int, C.c_double, C.c_int, C.c_double, C.c_void_p,
+                                         C.c_void_p, _i64p, C.POINTER(C.c_int), _dp]),
+    "airt_batch_kaczmarz": (C.c_int, [C.c_void_p, _dp, C.c_int64, C.c_double, C.c_int,
+                                      C.c_double, C.c_int, C.c_double, _dp, _dp]),
+    "airt_batch_destroy": (C.c_int, [C.c_void_p]),
     "airt_residual_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),

@@ -1,0 +1,725 @@
+// Batched independent SIRT / Kaczmarz problems (no counterpart in the
+// reference, which solves one problem per sirt/art call).
+//
+// The batch is one block-diagonal system: instance k owns rows
+// [row_off[k], row_off[k+1]) and columns [col_off[k], col_off[k+1]); all
+// matrices are generated on the GPU in one pass over every ray of every
+// instance and stored as one FP32 CSR + CSC.  An iteration is therefore a
+// handful of full-bandwidth launches over all instances:
+//   bwd (per size bucket)  x += lambda_k * D.*A'(M.*r), box clamp
+//   fwd (per size bucket)  r = b - A*x, M.*r, r.^2 per row
+//   reduce                 ||r_k||^2 per instance (one block per instance)
+//   ctrl                   per-instance DP / max-iteration rule
+// Per-instance scalars (lambda, tau*delta, stop flag, iteration count) are
+// read through the row->instance and column->instance maps; stopped
+// instances skip their rows and columns entirely.  Instances of equal N are
+// contiguous "size buckets"; an autotuner times the candidate lane widths of
+// the segment kernels on every bucket once and launches each bucket with its
+// fastest width.  Kaczmarz runs one CTA per instance.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "spmv.cuh"
+#include "trace.cuh"
+
+namespace airt {
+
+struct InstGeom {
+  int N, nA, p;
+  int ang0;      // first entry of the instance in the angle tables
+  int off0;      // first entry in the offset table
+  int64_t ray0;  // first global row
+  int64_t col0;  // first global column
+};
+
+struct Bucket {
+  int k0, k1;          // instances
+  int64_t r0, r1;      // rows
+  int64_t c0, c1;      // columns
+  int lanes_fwd = 8, lanes_bwd = 8;
+};
+
+struct Batch {
+  Problem P;                 // block-diagonal CSR/CSC and work vectors
+  int ninst = 0;
+  std::vector<InstGeom> hg;
+  std::vector<int64_t> row_off, col_off;
+  std::vector<Bucket> buckets;
+  DevBuf<InstGeom> g;
+  DevBuf<int64_t> d_row_off, d_col_off;
+  DevBuf<int> inst_row, inst_col, stop, iters, rule;
+  DevBuf<double> rsq, nrm2, lam, taud, resn_last;
+  bool tuned = false;
+};
+
+namespace {
+
+__device__ __forceinline__ int find_inst(const int64_t *off, int ninst, int64_t r) {
+  int lo = 0, hi = ninst;  // off[lo] <= r < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= r) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ Ray batch_ray(const InstGeom &gk, const double *cos_t, const double *sin_t,
+                                         const double *offs, int64_t local) {
+  RayGeom g;
+  g.kind = GEO_PARALLEL;
+  g.N = gk.N;
+  g.nA = gk.nA;
+  g.p = gk.p;
+  g.R = 0;
+  g.cos_t = cos_t + gk.ang0;
+  g.sin_t = sin_t + gk.ang0;
+  g.offsets = offs + gk.off0;
+  g.cos_w = g.sin_w = nullptr;
+  return ray_of(g, local);
+}
+
+__global__ void k_batch_count(int ninst, const InstGeom *__restrict__ G, const int64_t *__restrict__ roff,
+                              const double *cos_t, const double *sin_t, const double *offs,
+                              int64_t nrays, int64_t *__restrict__ counts, int *__restrict__ bad) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int k = find_inst(roff, ninst, r);
+    const InstGeom gk = G[k];
+    const Ray q = batch_ray(gk, cos_t, sin_t, offs, r - gk.ray0);
+    const int64_t nn = (int64_t)gk.N * gk.N;
+    int64_t c = 0;
+    trace_entries(gk.N, q, true, [&](int col, double) {
+      if (col < 0 || col >= nn) atomicExch(bad, 1);
+      else ++c;
+    });
+    counts[r] = c;
+  }
+}
+
+__global__ void k_batch_fill(int ninst, const InstGeom *__restrict__ G, const int64_t *__restrict__ roff,
+                             const double *cos_t, const double *sin_t, const double *offs,
+                             int64_t nrays, const int64_t *__restrict__ rp, int *__restrict__ ci,
+                             float *__restrict__ rv) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int k = find_inst(roff, ninst, r);
+    const InstGeom gk = G[k];
+    const Ray q = batch_ray(gk, cos_t, sin_t, offs, r - gk.ray0);
+    const int64_t nn = (int64_t)gk.N * gk.N;
+    int64_t pos = rp[r];
+    const int64_t end = rp[r + 1];
+    trace_entries(gk.N, q, true, [&](int col, double v) {
+      if (col >= 0 && col < nn && pos < end) {
+        ci[pos] = (int)(gk.col0 + col);
+        rv[pos] = (float)v;
+        ++pos;
+      }
+    });
+  }
+}
+
+__global__ void k_fill_inst(int ninst, const int64_t *__restrict__ off, int64_t total,
+                            int *__restrict__ inst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x)
+    inst[i] = find_inst(off, ninst, i);
+}
+
+// cimmino: M_i = 1/m_k * (1./||a_i||^2) with m_k the rows of i's instance.
+__global__ void k_cimmino_batch(int64_t m, const double *__restrict__ s2, const int *__restrict__ inst_row,
+                                const int64_t *__restrict__ roff, double *__restrict__ M) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int k = inst_row[i];
+    const double mk = (double)(roff[k + 1] - roff[k]);
+    const double v = (1.0 / mk) * (1.0 / s2[i]);
+    M[i] = isinf(v) ? 0.0 : v;
+  }
+}
+
+struct BFwd {
+  const double *b, *M;
+  float *mr32;
+  double *rsq;
+  const int *inst_row, *stop;
+  int64_t r0;
+};
+
+template <int L>
+__global__ void __launch_bounds__(256, 4)
+    k_batch_fwd(int64_t nseg, const int64_t *__restrict__ rp, const int *__restrict__ ci,
+                const float *__restrict__ rv, const float *__restrict__ x32, BFwd o) {
+  for_each_segment_vp<L>(
+      nseg, rp + o.r0, ci, rv, x32, [&](int64_t i) { return o.stop[o.inst_row[o.r0 + i]] == 0; },
+      [&](int64_t i, double s, bool lead) {
+        if (!lead) return;
+        const int64_t r = o.r0 + i;
+        const double ri = o.b[r] - s;
+        o.mr32[r] = (float)(o.M[r] * ri);
+        o.rsq[r] = ri * ri;
+      });
+}
+
+struct BUpd {
+  const double *D, *lam;
+  double *x64;
+  float *x32;
+  const int *inst_col, *stop;
+  int lbk, ubk;
+  double lb, ub;
+  int64_t c0;
+};
+
+template <int L>
+__global__ void __launch_bounds__(256, 4)
+    k_batch_bwd(int64_t nseg, const int64_t *__restrict__ cp, const int *__restrict__ ri,
+                const float *__restrict__ cv, const float *__restrict__ mr32, BUpd u) {
+  for_each_segment_vp<L>(
+      nseg, cp + u.c0, ri, cv, mr32, [&](int64_t j) { return u.stop[u.inst_col[u.c0 + j]] == 0; },
+      [&](int64_t j, double g, bool lead) {
+        if (!lead) return;
+        const int64_t c = u.c0 + j;
+        double x = u.x64[c] + u.lam[u.inst_col[c]] * (u.D[c] * g);
+        if (u.lbk) x = fmax(x, u.lb);
+        if (u.ubk) x = fmin(x, u.ub);
+        u.x64[c] = x;
+        u.x32[c] = (float)x;
+      });
+}
+
+// ||r_k||^2 per active instance: one block per instance, fixed order.
+__global__ void __launch_bounds__(256) k_batch_reduce(const int64_t *__restrict__ roff,
+                                                      const double *__restrict__ rsq,
+                                                      const int *__restrict__ stop,
+                                                      double *__restrict__ nrm2) {
+  const int k = blockIdx.x;
+  if (stop[k]) return;
+  double a = 0;
+  for (int64_t i = roff[k] + threadIdx.x; i < roff[k + 1]; i += blockDim.x) a += rsq[i];
+  a = block_sum<256>(a);
+  if (threadIdx.x == 0) nrm2[k] = a;
+}
+
+// Per-instance rule of check_stoprules.m:56-72 (DP) / 153-161 (NONE).
+__global__ void k_batch_ctrl(int ninst, int initial, int64_t kmax, const double *__restrict__ taud,
+                             const double *__restrict__ nrm2, int *__restrict__ stop,
+                             int *__restrict__ iters, int *__restrict__ rule,
+                             double *__restrict__ resn) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ninst; k += gridDim.x * blockDim.x) {
+    if (stop[k]) continue;
+    const int it = iters[k] + (initial ? 0 : 1);
+    iters[k] = it;
+    const double nrk = sqrt(nrm2[k]);
+    resn[k] = nrk;
+    const bool dp = taud != nullptr;
+    if ((dp && nrk <= taud[k]) || it >= kmax) {
+      stop[k] = 1;
+      rule[k] = (dp && it != kmax) ? 2 : 0;
+    }
+  }
+}
+
+__global__ void k_copy_f32(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// Per-instance power-iteration pieces on column ranges.
+__global__ void __launch_bounds__(256) k_inst_dot2(const int64_t *__restrict__ coff,
+                                                   const double *__restrict__ u,
+                                                   const double *__restrict__ w,
+                                                   double *__restrict__ uw, double *__restrict__ ww) {
+  const int k = blockIdx.x;
+  double a = 0, b2 = 0;
+  for (int64_t j = coff[k] + threadIdx.x; j < coff[k + 1]; j += blockDim.x) {
+    a += u[j] * w[j];
+    b2 += w[j] * w[j];
+  }
+  a = block_sum<256>(a);
+  b2 = block_sum<256>(b2);
+  if (threadIdx.x == 0) {
+    uw[k] = a;
+    ww[k] = b2;
+  }
+}
+
+__global__ void k_inst_normalize(int64_t n, const int *__restrict__ inst_col, const double *__restrict__ w,
+                                 const double *__restrict__ ww, double *__restrict__ u) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const double s = ww[inst_col[j]];
+    u[j] = s > 0 ? w[j] / sqrt(s) : 0.0;
+  }
+}
+
+__global__ void k_inst_init(int64_t n, const int *__restrict__ inst_col, const int64_t *__restrict__ coff,
+                            double *__restrict__ u) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int k = inst_col[j];
+    u[j] = 1.0 / sqrt((double)(coff[k + 1] - coff[k]));
+  }
+}
+
+__global__ void k_vmul(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
+                       double *__restrict__ c) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    c[i] = a[i] * b[i];
+}
+
+__global__ void k_vsqrt(int64_t n, const double *__restrict__ a, double *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = sqrt(a[i] > 0 ? a[i] : 0.0);
+}
+
+// ---------------------------------------------------------------- launchers
+template <class F>
+float time_launch(cudaStream_t s, F &&f, int reps = 3) {
+  cudaEvent_t e0, e1;
+  AIRT_CHECK_CUDA(cudaEventCreate(&e0));
+  AIRT_CHECK_CUDA(cudaEventCreate(&e1));
+  f();
+  AIRT_CHECK_CUDA(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) f();
+  AIRT_CHECK_CUDA(cudaEventRecord(e1, s));
+  AIRT_CHECK_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / reps;
+}
+
+void launch_bfwd(Batch &B, const Bucket &bk, int L, const BFwd &o) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  const int64_t ns = bk.r1 - bk.r0;
+  if (ns <= 0) return;
+  const unsigned g = grid_for(ns * L, 256, 4);
+  switch (L) {
+    case 16: k_batch_fwd<16><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    case 8: k_batch_fwd<8><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    case 4: k_batch_fwd<4><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+    default: k_batch_fwd<2><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+  }
+}
+
+void launch_bbwd(Batch &B, const Bucket &bk, int L, const BUpd &u) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  const int64_t ns = bk.c1 - bk.c0;
+  if (ns <= 0) return;
+  const unsigned g = grid_for(ns * L, 256, 4);
+  switch (L) {
+    case 16: k_batch_bwd<16><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    case 8: k_batch_bwd<8><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    case 4: k_batch_bwd<4><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+    default: k_batch_bwd<2><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- building
+Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const double *cos_t,
+                   const double *sin_t, const double *offsets) {
+  Batch *B = new Batch();
+  try {
+    AIRT_CHECK_CUDA(cudaStreamCreateWithFlags(&B->P.stream, cudaStreamNonBlocking));
+    Problem &P = B->P;
+    cudaStream_t s = P.stream;
+    B->ninst = ninst;
+    B->hg.resize(ninst);
+    B->row_off.assign(ninst + 1, 0);
+    B->col_off.assign(ninst + 1, 0);
+    int64_t angs = 0, offs = 0;
+    for (int k = 0; k < ninst; ++k) {
+      AIRT_REQUIRE(N[k] >= 1 && N[k] <= 46340 && nA[k] >= 0 && p[k] >= 0, "instance %d: bad size", k);
+      InstGeom &gk = B->hg[k];
+      gk.N = N[k];
+      gk.nA = nA[k];
+      gk.p = p[k];
+      gk.ang0 = (int)angs;
+      gk.off0 = (int)offs;
+      gk.ray0 = B->row_off[k];
+      gk.col0 = B->col_off[k];
+      angs += nA[k];
+      offs += p[k];
+      B->row_off[k + 1] = B->row_off[k] + (int64_t)nA[k] * p[k];
+      B->col_off[k + 1] = B->col_off[k] + (int64_t)N[k] * N[k];
+    }
+    P.m = B->row_off[ninst];
+    P.n = B->col_off[ninst];
+    AIRT_REQUIRE(P.m < INT32_MAX && P.n < INT32_MAX, "batch too large (rows or columns >= 2^31)");
+    P.geo_kind = GEO_PARALLEL;
+    P.cos_t.upload(cos_t, angs, s);
+    P.sin_t.upload(sin_t, angs, s);
+    P.offsets.upload(offsets, offs, s);
+    B->g.upload(B->hg.data(), ninst, s);
+    B->d_row_off.upload(B->row_off.data(), ninst + 1, s);
+    B->d_col_off.upload(B->col_off.data(), ninst + 1, s);
+    // size buckets: maximal runs of equal N
+    for (int k = 0; k < ninst;) {
+      int e = k + 1;
+      while (e < ninst && N[e] == N[k]) ++e;
+      Bucket bk;
+      bk.k0 = k;
+      bk.k1 = e;
+      bk.r0 = B->row_off[k];
+      bk.r1 = B->row_off[e];
+      bk.c0 = B->col_off[k];
+      bk.c1 = B->col_off[e];
+      B->buckets.push_back(bk);
+      k = e;
+    }
+    // generation: count, scan, fill, transpose (as generate_matrix)
+    DevBuf<int64_t> counts;
+    DevBuf<int> bad;
+    counts.ensure(P.m);
+    bad.ensure(1);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    const unsigned grid = grid_for(P.m, 128, 16);
+    k_batch_count<<<grid, 128, 0, s>>>(ninst, B->g.p, B->d_row_off.p, P.cos_t.p, P.sin_t.p,
+                                       P.offsets.p, P.m, counts.p, bad.p);
+    AIRT_LAUNCH_CHECK();
+    P.rp.ensure(P.m + 1 + 4);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(P.rp.p + P.m + 1, 0, 4 * sizeof(int64_t), s));
+    exclusive_scan_i64(counts.p, P.rp.p, P.m, s);
+    int hbad = 0;
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(&P.nnz, P.rp.p + P.m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    AIRT_REQUIRE(!hbad, "ray trace produced a pixel index outside the image");
+    P.ci.ensure(P.nnz + 8);
+    P.rv.ensure(P.nnz + 8);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(P.ci.p + P.nnz, 0, 8 * sizeof(int), s));
+    AIRT_CHECK_CUDA(cudaMemsetAsync(P.rv.p + P.nnz, 0, 8 * sizeof(float), s));
+    k_batch_fill<<<grid, 128, 0, s>>>(ninst, B->g.p, B->d_row_off.p, P.cos_t.p, P.sin_t.p,
+                                      P.offsets.p, P.m, P.rp.p, P.ci.p, P.rv.p);
+    AIRT_LAUNCH_CHECK();
+    counts.release();
+    build_csc_from_csr(P);
+    B->inst_row.ensure(P.m);
+    B->inst_col.ensure(P.n);
+    k_fill_inst<<<grid_for(P.m, 256), 256, 0, s>>>(ninst, B->d_row_off.p, P.m, B->inst_row.p);
+    k_fill_inst<<<grid_for(P.n, 256), 256, 0, s>>>(ninst, B->d_col_off.p, P.n, B->inst_col.p);
+    AIRT_LAUNCH_CHECK();
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    if (B->P.stream) cudaStreamSynchronize(B->P.stream);
+    cudaStream_t st = B->P.stream;
+    delete B;
+    if (st) cudaStreamDestroy(st);
+    throw;
+  }
+  return B;
+}
+
+Problem &batch_problem(Batch &B) { return B.P; }
+int batch_ninst(const Batch &B) { return B.ninst; }
+const int64_t *batch_row_off(const Batch &B) { return B.row_off.data(); }
+const int64_t *batch_col_off(const Batch &B) { return B.col_off.data(); }
+
+void batch_destroy(Batch *B) {
+  if (!B) return;
+  cudaStream_t s = B->P.stream;
+  if (s) cudaStreamSynchronize(s);
+  if (B->P.h_state) cudaFreeHost(B->P.h_state);
+  B->P.h_state = nullptr;
+  delete B;
+  if (s) cudaStreamDestroy(s);
+}
+
+namespace {
+__global__ void k_fill1(int64_t n, double *__restrict__ a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = 1.0;
+}
+}  // namespace
+
+// Weights of get_mfun_dfun.m per instance: only cimmino's 1/m factor depends on
+// the instance; every other weight is a per-row or per-column quantity.
+void batch_weights(Batch &B, int method) {
+  Problem &P = B.P;
+  P.M.ensure(P.m);
+  P.D.ensure(P.n);
+  if (method != AIRT_CIMMINO) {
+    compute_weights(P, method, P.M.p, P.D.p);
+    return;
+  }
+  P.w2.ensure(P.m > P.n ? P.m : P.n);
+  row_sums_sq(P, P.w2.p);
+  k_cimmino_batch<<<grid_for(P.m, 256), 256, 0, P.stream>>>(P.m, P.w2.p, B.inst_row.p,
+                                                            B.d_row_off.p, P.M.p);
+  k_fill1<<<grid_for(P.n, 256), 256, 0, P.stream>>>(P.n, P.D.p);
+  AIRT_LAUNCH_CHECK();
+}
+
+void batch_rho(Batch &B, int method, double tol, int maxit, double *rho_host) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  batch_weights(B, method);
+  const int K = B.ninst;
+  DevBuf<double> sd, u, t, y, w, uw, ww;
+  sd.ensure(P.n);
+  u.ensure(P.n);
+  t.ensure(P.n);
+  y.ensure(P.m);
+  w.ensure(P.n);
+  uw.ensure(K);
+  ww.ensure(K);
+  const unsigned gn = grid_for(P.n, 256), gm = grid_for(P.m, 256);
+  k_vsqrt<<<gn, 256, 0, s>>>(P.n, P.D.p, sd.p);
+  k_inst_init<<<gn, 256, 0, s>>>(P.n, B.inst_col.p, B.d_col_off.p, u.p);
+  std::vector<double> lam(K, 0.0), prev(K, 0.0);
+  for (int it = 0; it < maxit; ++it) {
+    k_vmul<<<gn, 256, 0, s>>>(P.n, sd.p, u.p, t.p);
+    apply_operator(P, t.p, y.p, 0);
+    k_vmul<<<gm, 256, 0, s>>>(P.m, P.M.p, y.p, y.p);
+    apply_operator(P, y.p, t.p, 1);
+    k_vmul<<<gn, 256, 0, s>>>(P.n, sd.p, t.p, w.p);
+    k_inst_dot2<<<K, 256, 0, s>>>(B.d_col_off.p, u.p, w.p, uw.p, ww.p);
+    k_inst_normalize<<<gn, 256, 0, s>>>(P.n, B.inst_col.p, w.p, ww.p, u.p);
+    AIRT_LAUNCH_CHECK();
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(lam.data(), uw.p, K * sizeof(double), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    bool done = it > 0;
+    for (int k = 0; k < K && done; ++k)
+      if (std::fabs(lam[k] - prev[k]) > tol * std::fabs(lam[k])) done = false;
+    prev = lam;
+    if (done) break;
+  }
+  for (int k = 0; k < K; ++k) rho_host[k] = lam[k];
+}
+
+// Times the candidate lane widths per bucket once (the autotuner).
+void batch_tune(Batch &B) {
+  if (B.tuned) return;
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  DevBuf<double> yr, yc;
+  DevBuf<float> xr, xc;
+  yr.ensure(P.m);
+  yc.ensure(P.n);
+  xr.ensure(P.m);
+  xc.ensure(P.n);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(xr.p, 0, P.m * sizeof(float), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(xc.p, 0, P.n * sizeof(float), s));
+  DevBuf<int> nostop;
+  nostop.ensure(B.ninst);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(nostop.p, 0, B.ninst * sizeof(int), s));
+  DevBuf<double> zero;
+  zero.ensure(P.m > P.n ? P.m : P.n);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(zero.p, 0, zero.n * sizeof(double), s));
+  DevBuf<double> xtmp;
+  xtmp.ensure(P.n);
+  DevBuf<float> mtmp, x32tmp;
+  mtmp.ensure(P.m);
+  x32tmp.ensure(P.n);
+  const int cands[4] = {2, 4, 8, 16};
+  for (Bucket &bk : B.buckets) {
+    float best_f = 1e30f, best_b = 1e30f;
+    for (int L : cands) {
+      BFwd o{zero.p, zero.p, mtmp.p, yr.p, B.inst_row.p, nostop.p, bk.r0};
+      const float tf = time_launch(s, [&] {
+        const int64_t ns = bk.r1 - bk.r0;
+        const unsigned g = grid_for(ns * L, 256, 4);
+        switch (L) {
+          case 16: k_batch_fwd<16><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
+          case 8: k_batch_fwd<8><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
+          case 4: k_batch_fwd<4><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
+          default: k_batch_fwd<2><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
+        }
+      });
+      BUpd u{zero.p, zero.p, xtmp.p, x32tmp.p, B.inst_col.p, nostop.p, 0, 0, 0.0, 0.0, bk.c0};
+      const float tb = time_launch(s, [&] {
+        const int64_t ns = bk.c1 - bk.c0;
+        const unsigned g = grid_for(ns * L, 256, 4);
+        switch (L) {
+          case 16: k_batch_bwd<16><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
+          case 8: k_batch_bwd<8><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
+          case 4: k_batch_bwd<4><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
+          default: k_batch_bwd<2><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
+        }
+      });
+      AIRT_LAUNCH_CHECK();
+      if (tf < best_f) {
+        best_f = tf;
+        bk.lanes_fwd = L;
+      }
+      if (tb < best_b) {
+        best_b = tb;
+        bk.lanes_bwd = L;
+      }
+    }
+  }
+  B.tuned = true;
+}
+
+// SIRT over the whole batch with per-instance relaxpar and DP thresholds.
+void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b, const double *taud_host,
+                int64_t kmax, int lbk, double lb, int ubk, double ub, const double *d_x0, double *d_x,
+                int64_t *finaliter, int *stoprule, double *gpu_ms) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  const int K = B.ninst;
+  AIRT_REQUIRE(kmax >= 0 && kmax < INT32_MAX, "kmax out of range");
+  cudaEvent_t t0, t1;
+  AIRT_CHECK_CUDA(cudaEventCreate(&t0));
+  AIRT_CHECK_CUDA(cudaEventCreate(&t1));
+  batch_tune(B);
+  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
+  batch_weights(B, method);
+  P.x64.ensure(P.n);
+  P.x32.ensure(P.n);
+  P.mr32.ensure(P.m);
+  B.rsq.ensure(P.m);
+  B.nrm2.ensure(K);
+  B.stop.ensure(K);
+  B.iters.ensure(K);
+  B.rule.ensure(K);
+  B.resn_last.ensure(K);
+  B.lam.upload(lam_host, K, s);
+  if (taud_host) B.taud.upload(taud_host, K, s);
+  if (d_x0)
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(P.x64.p, d_x0, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  else
+    AIRT_CHECK_CUDA(cudaMemsetAsync(P.x64.p, 0, P.n * sizeof(double), s));
+  k_copy_f32<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, P.x64.p, P.x32.p);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(B.stop.p, 0, K * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(B.iters.p, 0, K * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(B.rule.p, 0, K * sizeof(int), s));
+  BFwd fo{d_b, P.M.p, P.mr32.p, B.rsq.p, B.inst_row.p, B.stop.p, 0};
+  BUpd uo{P.D.p, B.lam.p, P.x64.p, P.x32.p, B.inst_col.p, B.stop.p, lbk, ubk, lb, ub, 0};
+  const double *taud = taud_host ? B.taud.p : nullptr;
+  auto fwd_all = [&]() {
+    for (const Bucket &bk : B.buckets) {
+      BFwd o = fo;
+      o.r0 = bk.r0;
+      launch_bfwd(B, bk, bk.lanes_fwd, o);
+    }
+    k_batch_reduce<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, B.stop.p, B.nrm2.p);
+  };
+  auto bwd_all = [&]() {
+    for (const Bucket &bk : B.buckets) {
+      BUpd u = uo;
+      u.c0 = bk.c0;
+      launch_bbwd(B, bk, bk.lanes_bwd, u);
+    }
+  };
+  const unsigned gk = (unsigned)((K + 127) / 128);
+  fwd_all();
+  k_batch_ctrl<<<gk, 128, 0, s>>>(K, 1, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
+                                  B.resn_last.p);
+  AIRT_LAUNCH_CHECK();
+  std::vector<int> hstop(K);
+  const int64_t chunk = 8;
+  for (int64_t it = 1; it <= kmax;) {
+    const int64_t cnt = std::min<int64_t>(chunk, kmax - it + 1);
+    for (int64_t j = 0; j < cnt; ++j) {
+      bwd_all();
+      fwd_all();
+      k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
+                                      B.resn_last.p);
+    }
+    AIRT_LAUNCH_CHECK();
+    it += cnt;
+    if (!taud) continue;
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hstop.data(), B.stop.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    bool all = true;
+    for (int k = 0; k < K && all; ++k) all = hstop[k] != 0;
+    if (all) break;
+  }
+  AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(d_x, P.x64.p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  std::vector<int> hit(K), hrule(K);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(hit.data(), B.iters.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(hrule.data(), B.rule.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  for (int k = 0; k < K; ++k) {
+    if (finaliter) finaliter[k] = hit[k];
+    if (stoprule) stoprule[k] = hrule[k];
+  }
+  if (gpu_ms) *gpu_ms = ms;
+}
+
+// ---------------------------------------------------------------- Kaczmarz
+namespace {
+// One CTA per instance: the instance's rows with nonzero norm in order,
+// sequentially (art.m:248-285 with kaczmarz order), all threads on one row.
+__global__ void __launch_bounds__(256)
+    k_batch_kacz(const int64_t *__restrict__ roff, const int64_t *__restrict__ rp,
+                 const int *__restrict__ ci, const float *__restrict__ rv, const double *__restrict__ b,
+                 const double *__restrict__ nrm, double lam, int lbk, double lb, int ubk, double ub,
+                 int sweeps, double *__restrict__ x) {
+  const int k = blockIdx.x;
+  __shared__ double sh[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int sw = 0; sw < sweeps; ++sw) {
+    for (int64_t i = roff[k]; i < roff[k + 1]; ++i) {
+      const double ni = nrm[i];
+      if (!(ni > 0)) continue;
+      const int64_t s0 = rp[i], s1 = rp[i + 1];
+      double a = 0;
+      for (int64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) a = fma((double)rv[e], x[ci[e]], a);
+      a = warp_sum(a);
+      if (lane == 0) sh[w] = a;
+      __syncthreads();
+      double dot = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dot += sh[q];
+      const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(b[i], dot)), ni);
+      for (int64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) {
+        const int j = ci[e];
+        double v = __dadd_rn(x[j], __dmul_rn(c, (double)rv[e]));
+        if (lbk) v = fmax(v, lb);
+        if (ubk) v = fmin(v, ub);
+        x[j] = v;
+      }
+      __syncthreads();
+    }
+  }
+}
+}  // namespace
+
+void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int lbk, double lb,
+                    int ubk, double ub, double *d_x, double *gpu_ms) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  AIRT_REQUIRE(sweeps >= 0 && sweeps < INT32_MAX, "sweeps out of range");
+  cudaEvent_t t0, t1;
+  AIRT_CHECK_CUDA(cudaEventCreate(&t0));
+  AIRT_CHECK_CUDA(cudaEventCreate(&t1));
+  P.w1.ensure(P.m > P.n ? P.m : P.n);
+  row_sums_sq(P, P.w1.p);
+  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
+  // x0 = 0 is feasible for lb <= 0 <= ub, so the whole-vector clamp after the
+  // first row step (art.m:279-284) only matters on each row's support.
+  AIRT_REQUIRE((lbk == 0 || lb <= 0) && (ubk == 0 || ub >= 0),
+               "batched Kaczmarz starts from x0 = 0 and needs lbound <= 0 <= ubound");
+  AIRT_CHECK_CUDA(cudaMemsetAsync(d_x, 0, P.n * sizeof(double), s));
+  k_batch_kacz<<<B.ninst, 256, 0, s>>>(B.d_row_off.p, P.rp.p, P.ci.p, P.rv.p, d_b, P.w1.p, lam, lbk,
+                                       lb, ubk, ub, (int)sweeps, d_x);
+  AIRT_LAUNCH_CHECK();
+  AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
+  AIRT_CHECK_CUDA(cudaEventSynchronize(t1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (gpu_ms) *gpu_ms = ms;
+}
+
+}  // namespace airt

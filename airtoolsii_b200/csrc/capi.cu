@@ -1,5 +1,6 @@
 // extern "C" entry points of libairt (declared in include/airt.h).  Each one
 // converts C++ exceptions into a status code plus a thread-local message.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -331,6 +332,100 @@ int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const 
                                     cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   if (info) *info = inf;
+  AIRT_API_END
+}
+
+// ---------------------------------------------------------------- batches
+int airt_batch_parallel(int ninst, const int *N, const int *nA, const int *p, const double *cos_t,
+                        const double *sin_t, const double *offsets, airt_batch **out) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(out && N && nA && p && cos_t && sin_t && offsets && ninst >= 1,
+               "null pointer argument or empty batch");
+  *out = reinterpret_cast<airt_batch *>(batch_build(ninst, N, nA, p, cos_t, sin_t, offsets));
+  AIRT_API_END
+}
+
+int airt_batch_layout(const airt_batch *h, int64_t *row_off, int64_t *col_off, int64_t *nnz) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h, "null batch handle");
+  Batch &B = *reinterpret_cast<Batch *>(const_cast<airt_batch *>(h));
+  const int K = batch_ninst(B);
+  if (row_off) std::copy(batch_row_off(B), batch_row_off(B) + K + 1, row_off);
+  if (col_off) std::copy(batch_col_off(B), batch_col_off(B) + K + 1, col_off);
+  if (nnz) *nnz = batch_problem(B).nnz;
+  AIRT_API_END
+}
+
+int airt_batch_stream(const airt_batch *h, void **cuda_stream) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && cuda_stream, "null pointer argument");
+  Batch &B = *reinterpret_cast<Batch *>(const_cast<airt_batch *>(h));
+  *cuda_stream = (void *)batch_problem(B).stream;
+  AIRT_API_END
+}
+
+int airt_batch_rho(airt_batch *h, int method, double tol, int maxit, double *rho) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && rho && maxit > 0, "invalid argument");
+  AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+  batch_rho(*reinterpret_cast<Batch *>(h), method, tol, maxit, rho);
+  AIRT_API_END
+}
+
+int airt_batch_sirt_device(airt_batch *h, int method, const double *relaxpar, const double *d_b,
+                           const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
+                           double ub, const double *d_x0, double *d_x, int64_t *finaliter,
+                           int *stoprule, double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && relaxpar && d_b && d_x, "null pointer argument");
+  AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+  AIRT_REQUIRE(lb_kind != AIRT_BOUND_VECTOR && ub_kind != AIRT_BOUND_VECTOR,
+               "batched SIRT takes scalar bounds");
+  batch_sirt(*reinterpret_cast<Batch *>(h), method, relaxpar, d_b, taudelta, kmax, lb_kind, lb,
+             ub_kind, ub, d_x0, d_x, finaliter, stoprule, gpu_ms);
+  AIRT_API_END
+}
+
+int airt_batch_sirt(airt_batch *h, int method, const double *relaxpar, const double *b,
+                    const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
+                    double ub, const double *x0, double *x, int64_t *finaliter, int *stoprule,
+                    double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && relaxpar && b && x, "null pointer argument");
+  Batch &B = *reinterpret_cast<Batch *>(h);
+  Problem &P = batch_problem(B);
+  P.b64.upload(b, P.m, P.stream);
+  if (x0) P.vin.upload(x0, P.n, P.stream);
+  P.Xd.ensure(P.n);
+  AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+  AIRT_REQUIRE(lb_kind != AIRT_BOUND_VECTOR && ub_kind != AIRT_BOUND_VECTOR,
+               "batched SIRT takes scalar bounds");
+  batch_sirt(B, method, relaxpar, P.b64.p, taudelta, kmax, lb_kind, lb, ub_kind, ub,
+             x0 ? P.vin.p : nullptr, P.Xd.p, finaliter, stoprule, gpu_ms);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P.Xd.p, P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  AIRT_API_END
+}
+
+int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double relaxpar,
+                        int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && b && x, "null pointer argument");
+  AIRT_REQUIRE(lb_kind != AIRT_BOUND_VECTOR && ub_kind != AIRT_BOUND_VECTOR,
+               "batched Kaczmarz takes scalar bounds");
+  Batch &B = *reinterpret_cast<Batch *>(h);
+  Problem &P = batch_problem(B);
+  P.b64.upload(b, P.m, P.stream);
+  P.Xd.ensure(P.n);
+  batch_kaczmarz(B, P.b64.p, sweeps, relaxpar, lb_kind, lb, ub_kind, ub, P.Xd.p, gpu_ms);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P.Xd.p, P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  AIRT_API_END
+}
+
+int airt_batch_destroy(airt_batch *h) {
+  AIRT_API_BEGIN
+  batch_destroy(reinterpret_cast<Batch *>(h));
   AIRT_API_END
 }
 

@@ -211,6 +211,23 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
              const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
 double estimate_rho(Problem &P, const double *dM, const double *dD, double tol, int maxit);
 void export_csc(Problem &P, uint64_t *jc, uint64_t *ir, double *pr);
+void row_sums_sq(Problem &P, double *out);
+
+// Batched independent problems (batch.cu).
+struct Batch;
+Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const double *cos_t,
+                   const double *sin_t, const double *offsets);
+void batch_destroy(Batch *B);
+Problem &batch_problem(Batch &B);
+int batch_ninst(const Batch &B);
+const int64_t *batch_row_off(const Batch &B);
+const int64_t *batch_col_off(const Batch &B);
+void batch_rho(Batch &B, int method, double tol, int maxit, double *rho_host);
+void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b, const double *taud_host,
+                int64_t kmax, int lbk, double lb, int ubk, double ub, const double *d_x0, double *d_x,
+                int64_t *finaliter, int *stoprule, double *gpu_ms);
+void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int lbk, double lb,
+                    int ubk, double ub, double *d_x, double *gpu_ms);
 
 // Exclusive scan of counts[0..n) into offs[0..n] (offs[n] = total), device.
 void exclusive_scan_i64(const int64_t *counts, int64_t *offs, int64_t n, cudaStream_t s);

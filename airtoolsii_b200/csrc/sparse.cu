@@ -313,6 +313,13 @@ __global__ void k_fill(int64_t n, double v, double *__restrict__ w) {
 void row_col_stats_mf(Problem &P, double *s2, double *s1, double *colcnt, double *cols1,
                       const double *colw, double *s2w);
 
+// Squared row norms of the stored matrix (FP64 sums of the FP32 entries).
+void row_sums_sq(Problem &P, double *out) {
+  k_row_stats<32><<<grid_for(P.m * 32, 256), 256, 0, P.stream>>>(P.m, P.rp.p, P.ci.p, P.rv.p,
+                                                                  nullptr, out, nullptr, nullptr);
+  AIRT_LAUNCH_CHECK();
+}
+
 // dM (m) and dD (n) receive the diagonals; landweber gives ones.
 void compute_weights(Problem &P, int method, double *dM, double *dD) {
   cudaStream_t s = P.stream;

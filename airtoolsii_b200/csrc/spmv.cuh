@@ -92,6 +92,52 @@ __device__ __forceinline__ void for_each_segment_v(int64_t nseg, const int64_t *
   }
 }
 
+// for_each_segment_v with a per-segment predicate: segments for which
+// active(i) is false are skipped without touching their nonzeros (all lanes
+// of a group evaluate it, so the group stays converged).
+template <int LANES, typename TX, class Act, class Epi>
+__device__ __forceinline__ void for_each_segment_vp(int64_t nseg, const int64_t *__restrict__ ptr,
+                                                    const int *__restrict__ idx,
+                                                    const float *__restrict__ val,
+                                                    const TX *__restrict__ x, Act &&active,
+                                                    Epi &&epi) {
+  const int lane = threadIdx.x % LANES;
+  const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / LANES;
+  const int64_t ng = (int64_t)gridDim.x * blockDim.x / LANES;
+  const int64_t trips = (nseg + ng - 1) / ng;
+  const float4 *__restrict__ V4 = reinterpret_cast<const float4 *>(val);
+  const int4 *__restrict__ I4 = reinterpret_cast<const int4 *>(idx);
+  for (int64_t t = 0; t < trips; ++t) {
+    const int64_t i = gid + t * ng;
+    const bool on = i < nseg && active(i);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (on) {
+      const int64_t q0 = __ldg(ptr + i), q1 = __ldg(ptr + i + 1);
+      int64_t qa = (q0 + 3) & ~(int64_t)3;
+      if (qa > q1) qa = q1;
+      int64_t qb = q1 & ~(int64_t)3;
+      if (qb < qa) qb = qa;
+      for (int64_t q = q0 + lane; q < qa; q += LANES)
+        a0 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a0);
+      for (int64_t q = qb + lane; q < q1; q += LANES)
+        a1 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a1);
+      const int64_t ve = qb >> 2;
+      for (int64_t v = (qa >> 2) + lane; v < ve; v += LANES) {
+        const float4 f = __ldg(V4 + v);
+        const int4 c = __ldg(I4 + v);
+        const TX g0 = __ldg(x + c.x), g1 = __ldg(x + c.y), g2 = __ldg(x + c.z), g3 = __ldg(x + c.w);
+        a0 = fma((double)f.x, (double)g0, a0);
+        a1 = fma((double)f.y, (double)g1, a1);
+        a2 = fma((double)f.z, (double)g2, a2);
+        a3 = fma((double)f.w, (double)g3, a3);
+      }
+    }
+    double acc = (a0 + a1) + (a2 + a3);
+    acc = group_sum<LANES>(acc);
+    epi(i, acc, lane == 0 && on);
+  }
+}
+
 // Lanes per segment of the vectorised kernels from the mean segment length.
 inline int vec_lanes_for(int64_t nnz, int64_t nseg) {
   const double avg = nseg ? (double)nnz / (double)nseg : 0.0;

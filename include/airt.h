@@ -167,6 +167,36 @@ int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *
 int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const double *x0,
              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
 
+/* ---- batches of independent problems --------------------------------------- */
+/* No counterpart in the reference (one problem per sirt/art call, sirt/sirt.m:1).
+ * ninst paralleltomo instances (N[k], nA[k] angles, p[k] rays); cos_t/sin_t
+ * concatenate the per-instance angle tables, offsets the ray offsets.  The
+ * batch is stored as one block-diagonal FP32 CSR + CSC generated on the GPU;
+ * vectors are the instances' vectors concatenated in order (row_off/col_off
+ * from airt_batch_layout, ninst+1 entries each). */
+typedef struct airt_batch airt_batch;
+int airt_batch_parallel(int ninst, const int *N, const int *nA, const int *p, const double *cos_t,
+                        const double *sin_t, const double *offsets, airt_batch **out);
+int airt_batch_layout(const airt_batch *h, int64_t *row_off, int64_t *col_off, int64_t *nnz);
+int airt_batch_stream(const airt_batch *h, void **cuda_stream);
+/* Per-instance rho of D*A_k'*M*A_k (power iteration, as airt_rho). */
+int airt_batch_rho(airt_batch *h, int method, double tol, int maxit, double *rho);
+/* SIRT on every instance at once: relaxpar[k], optional taudelta[k] (DP rule
+ * per instance; NULL = run kmax iterations), scalar bounds; x receives the
+ * final iterates, finaliter/stoprule one entry per instance. */
+int airt_batch_sirt(airt_batch *h, int method, const double *relaxpar, const double *b,
+                    const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
+                    double ub, const double *x0, double *x, int64_t *finaliter, int *stoprule,
+                    double *gpu_ms);
+int airt_batch_sirt_device(airt_batch *h, int method, const double *relaxpar, const double *d_b,
+                           const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
+                           double ub, const double *d_x0, double *d_x, int64_t *finaliter,
+                           int *stoprule, double *gpu_ms);
+/* Kaczmarz sweeps in the kaczmarz row order, one CTA per instance, x0 = 0. */
+int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double relaxpar,
+                        int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms);
+int airt_batch_destroy(airt_batch *h);
+
 /* ---- allocation-free residual ------------------------------------------------ */
 /* No counterpart in the reference.  r = b - A*x and ||r|| (into d_resnorm) for
  * a caller that holds an FP32 CSR (d_rp m+1, d_ci/d_rv nnz), x, b and r on

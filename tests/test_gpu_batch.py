@@ -1,0 +1,85 @@
+"""GPU tests of the batched solvers: every instance of an uneven batch
+against the FP64 oracle run on that instance alone (relative iterate error
+<= 1e-5, identical DP stopping iteration)."""
+import numpy as np
+import pytest
+
+import airtoolsii_b200 as airt
+from oracle import airt_oracle as O
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-5
+
+
+def relerr(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def batch():
+    rng = np.random.default_rng(17)
+    Ns = [16, 16, 24, 32, 32, 48]
+    thetas = [np.sort(rng.choice(np.arange(0.0, 180.0, 1.0), size=int(rng.integers(12, 40)),
+                                 replace=False)) for _ in Ns]
+    B = airt.ParallelBatch(Ns, thetas)
+    mats, bs, tds, xs = [], [], [], []
+    for k, N in enumerate(Ns):
+        A = O.paralleltomo_matrix(N, thetas[k])
+        x = airt.random_ellipses(N, 6, seed=30 + k)
+        eta = [0.005, 0.01, 0.02, 0.03, 0.01, 0.02][k]
+        b, en = airt.add_noise(A @ x, eta, seed=60 + k)
+        mats.append(A)
+        bs.append(b)
+        tds.append(1.02 * en)
+        xs.append(x)
+    return B, mats, bs, np.array(tds), xs
+
+
+def test_batch_layout(batch):
+    B, mats, *_ = batch
+    assert B.K == len(mats)
+    for k, A in enumerate(mats):
+        assert B.row_off[k + 1] - B.row_off[k] == A.shape[0]
+        assert B.col_off[k + 1] - B.col_off[k] == A.shape[1]
+    assert B.nnz == sum(A.nnz for A in mats)
+
+
+@pytest.mark.parametrize("method", ["cimmino", "drop"])
+def test_batch_rho(batch, method):
+    B, mats, bs, _, _ = batch
+    rho = B.rho(method)
+    for k, A in enumerate(mats):
+        _, io, _ = O.sirt(method, A, bs[k], [1])
+        assert abs(rho[k] - io["rho"]) <= 1e-4 * io["rho"]
+
+
+@pytest.mark.parametrize("method", ["cimmino", "drop", "sart"])
+def test_batch_sirt_dp_per_instance(batch, method):
+    B, mats, bs, tds, _ = batch
+    rho = np.ones(B.K) if method == "sart" else B.rho(method)
+    xs, info = B.sirt(method, bs, 400, taudelta=tds, rho=rho, lbound=0.0)
+    for k, A in enumerate(mats):
+        Xo, io, _ = O.sirt(method, A, bs[k], [400], options={
+            "stoprule": {"type": "DP", "taudelta": tds[k]}, "rho": float(rho[k]), "lbound": 0.0})
+        assert info["finaliter"][k] == io["finaliter"], (k, info["finaliter"][k], io["finaliter"])
+        assert info["stoprule"][k] == io["stoprule"]
+        assert relerr(xs[k], Xo[:, -1]) <= RTOL
+
+
+def test_batch_sirt_fixed_iterations_box(batch):
+    B, mats, bs, _, _ = batch
+    rho = B.rho("cimmino")
+    xs, info = B.sirt("cimmino", bs, 25, rho=rho, lbound=0.0, ubound=0.7)
+    assert np.all(info["finaliter"] == 25)
+    for k, A in enumerate(mats):
+        Xo, _, _ = O.sirt("cimmino", A, bs[k], [25], options={"rho": float(rho[k]),
+                                                               "lbound": 0.0, "ubound": 0.7})
+        assert relerr(xs[k], Xo[:, -1]) <= RTOL
+
+
+def test_batch_kaczmarz(batch):
+    B, mats, bs, _, _ = batch
+    xs, _ = B.kaczmarz(bs, 3, 1.0, lbound=0.0)
+    for k, A in enumerate(mats):
+        Xo, _ = O.art("kaczmarz", A, bs[k], [3], options={"lbound": 0.0})
+        assert relerr(xs[k], Xo[:, -1]) <= RTOL
