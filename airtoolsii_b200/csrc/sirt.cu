@@ -533,12 +533,36 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   const int64_t chunk = 16;
   const int lag = 2;
   int64_t c = 0;
-  for (int64_t it = 1; it <= kmax; ++c) {
-    const int64_t cnt = (kmax - it + 1 < chunk) ? (kmax - it + 1) : chunk;
-    for (int64_t j = 0; j < cnt; ++j) {
+  // A full chunk is captured once as a CUDA graph and replayed: the kernel
+  // arguments never change between iterations (all loop state lives in
+  // device memory), so one graph serves the whole solve.  With per-launch
+  // profiling on, kernels are launched one by one so each gets its events.
+  cudaGraphExec_t chunk_graph = nullptr;
+  if (!P.profiling && kmax >= chunk) {
+    cudaGraph_t g = nullptr;
+    AIRT_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int64_t j = 0; j < chunk; ++j) {
       launch_bwd(P, ua, o.relax_kind);
       launch_fwd(P, fo, me);
       k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
+    }
+    const cudaError_t ec = cudaStreamEndCapture(s, &g);
+    if (ec == cudaSuccess && g) {
+      if (cudaGraphInstantiate(&chunk_graph, g, 0) != cudaSuccess) chunk_graph = nullptr;
+      cudaGraphDestroy(g);
+    }
+    cudaGetLastError();
+  }
+  for (int64_t it = 1; it <= kmax; ++c) {
+    const int64_t cnt = (kmax - it + 1 < chunk) ? (kmax - it + 1) : chunk;
+    if (cnt == chunk && chunk_graph) {
+      AIRT_CHECK_CUDA(cudaGraphLaunch(chunk_graph, s));
+    } else {
+      for (int64_t j = 0; j < cnt; ++j) {
+        launch_bwd(P, ua, o.relax_kind);
+        launch_fwd(P, fo, me);
+        k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
+      }
     }
     AIRT_LAUNCH_CHECK();
     it += cnt;
@@ -553,6 +577,7 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   }
   AIRT_CHECK_CUDA(cudaMemcpyAsync(P.h_state, P.state.p, sizeof(SirtState), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (chunk_graph) cudaGraphExecDestroy(chunk_graph);
   for (int q = 0; q < 3; ++q) cudaEventDestroy(ev[q]);
   const SirtState st = P.h_state[0];
   int herr = 0;
