@@ -8,6 +8,7 @@ sm_100a); the package raises on import if the library is missing.
 from ._lib import AirtError, lib as _load_lib
 from .afun import AirtOperator, afun_matrix, as_operator
 from .batch import ParallelBatch
+from .unet import UNet
 from .solvers import (art, calczeta, cav, cimmino, drop, kaczmarz, landweber, randkaczmarz,
                       sart, sirt, symkaczmarz)
 from .testprobs import (add_noise, cosd, fanlineartomo, paralleltomo, phantomgallery,
@@ -15,7 +16,7 @@ from .testprobs import (add_noise, cosd, fanlineartomo, paralleltomo, phantomgal
 
 _load_lib()
 
-__all__ = ["AirtError", "AirtOperator", "ParallelBatch", "afun_matrix", "as_operator", "art", "calczeta", "cav",
+__all__ = ["AirtError", "AirtOperator", "ParallelBatch", "UNet", "afun_matrix", "as_operator", "art", "calczeta", "cav",
            "cimmino", "drop", "kaczmarz", "landweber", "randkaczmarz", "sart", "sirt",
            "symkaczmarz", "add_noise", "cosd", "fanlineartomo", "paralleltomo",
            "phantomgallery", "random_ellipses", "sind"]

@@ -91,6 +91,19 @@ SIGNATURES = {
     "airt_batch_kaczmarz": (C.c_int, [C.c_void_p, _dp, C.c_int64, C.c_double, C.c_int,
                                       C.c_double, C.c_int, C.c_double, _dp, _dp]),
     "airt_batch_destroy": (C.c_int, [C.c_void_p]),
+    "airt_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                   C.POINTER(C.c_void_p)]),
+    "airt_unet_destroy": (C.c_int, [C.c_void_p]),
+    "airt_unet_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "airt_unet_num_params": (C.c_int, [C.c_void_p, _i64p]),
+    "airt_unet_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "airt_unet_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "airt_unet_get_grads": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "airt_unet_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "airt_unet_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.POINTER(C.c_float)]),
+    "airt_unet_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                       C.POINTER(C.c_float)]),
     "airt_residual_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),

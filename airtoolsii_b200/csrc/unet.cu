@@ -1,0 +1,750 @@
+// Learned warm start: a U-Net (levels x {conv3x3+ReLU, conv3x3+ReLU},
+// 2x2 max-pool down, nearest 2x up + skip concatenation, 1x1 head) trained
+// and evaluated with this project's own kernels.  No counterpart in the
+// reference: its output only enters the solvers as x0 (sirt/sirt.m:5).
+//
+// Layout: activations NHWC BF16 ([pixel][channel], pixel = (b*H + h)*W + w),
+// gradients FP32, weights FP32 masters [Cout][Kp] with a BF16 copy for the
+// tensor cores (Kp = 9*Cin rounded up to 64, zero padded; K index
+// (kh*3 + kw)*Cin + ci).  Every 3x3 convolution is an im2col followed by the
+// tcgen05 GEMM of umma.cuh:
+//   forward  Y[P][Co]  = relu(col(X)[P][Kp] * W[Co][Kp]^T + b)   (K/K-major)
+//   dW^T     [Kp][Co] += col(X)^T * dYm   (both MN-major, split-K atomics
+//                        written transposed straight into W's layout)
+//   dcol     [P][Kp]   = dYm[P][Co] * W   (W as MN-major B), then col2im.
+// The image (x(:), column-major N x N) maps to NHWC with h = column-major row.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "common.cuh"
+#include "umma.cuh"
+
+namespace airt {
+
+namespace {
+
+constexpr int kT = 256;
+
+__global__ void k_im2col(int B, int H, int W, int C, int Kp, const __nv_bfloat16 *__restrict__ X,
+                         __nv_bfloat16 *__restrict__ col) {
+  const int64_t total = (int64_t)B * H * W * Kp;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int kk = (int)(t % Kp);
+    const int64_t p = t / Kp;
+    __nv_bfloat16 v = __float2bfloat16(0.f);
+    if (kk < 9 * C) {
+      const int ci = kk % C, tap = kk / C;
+      const int kh = tap / 3, kw = tap % 3;
+      const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
+      const int hh = h + kh - 1, ww = w + kw - 1;
+      if (hh >= 0 && hh < H && ww >= 0 && ww < W) v = X[(((int64_t)b * H + hh) * W + ww) * C + ci];
+    }
+    col[t] = v;
+  }
+}
+
+__global__ void k_col2im(int B, int H, int W, int C, int Kp, const float *__restrict__ dcol,
+                         float *__restrict__ dX) {
+  const int64_t total = (int64_t)B * H * W * C;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int ci = (int)(t % C);
+    const int64_t p = t / C;
+    const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
+    float acc = 0.f;
+#pragma unroll
+    for (int kh = 0; kh < 3; ++kh)
+#pragma unroll
+      for (int kw = 0; kw < 3; ++kw) {
+        const int hs = h - kh + 1, ws = w - kw + 1;
+        if (hs >= 0 && hs < H && ws >= 0 && ws < W)
+          acc += dcol[(((int64_t)b * H + hs) * W + ws) * Kp + (kh * 3 + kw) * C + ci];
+      }
+    dX[t] += acc;
+  }
+}
+
+// dYm = bf16(dY * (Y > 0)) and db += column sums (one block per 256 columns-slab)
+__global__ void k_relu_mask(int64_t n, const float *__restrict__ dY, const __nv_bfloat16 *__restrict__ Y,
+                            __nv_bfloat16 *__restrict__ dYm) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dYm[i] = __float2bfloat16(__bfloat162float(Y[i]) > 0.f ? dY[i] : 0.f);
+}
+
+__global__ void k_colsum(int64_t P, int C, const __nv_bfloat16 *__restrict__ M, float *__restrict__ out) {
+  // grid.x over channels, each block reduces one channel
+  const int c = blockIdx.x;
+  float a = 0.f;
+  for (int64_t p = threadIdx.x; p < P; p += blockDim.x) a += __bfloat162float(M[p * C + c]);
+  __shared__ float sh[kT / 32];
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float t = threadIdx.x < kT / 32 ? sh[threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) out[c] += t;
+  }
+}
+
+__global__ void k_pool(int B, int H, int W, int C, const __nv_bfloat16 *__restrict__ X,
+                       __nv_bfloat16 *__restrict__ Y) {
+  const int Ho = H / 2, Wo = W / 2;
+  const int64_t total = (int64_t)B * Ho * Wo * C;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C);
+    const int64_t q = t / C;
+    const int w = (int)(q % Wo), h = (int)((q / Wo) % Ho), b = (int)(q / ((int64_t)Wo * Ho));
+    float m = -INFINITY;
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j)
+        m = fmaxf(m, __bfloat162float(X[(((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + c]));
+    Y[t] = __float2bfloat16(m);
+  }
+}
+
+// gradient of the max pool goes to the first maximal element of each window
+__global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__restrict__ X,
+                            const float *__restrict__ dY, float *__restrict__ dX) {
+  const int Ho = H / 2, Wo = W / 2;
+  const int64_t total = (int64_t)B * Ho * Wo * C;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C);
+    const int64_t q = t / C;
+    const int w = (int)(q % Wo), h = (int)((q / Wo) % Ho), b = (int)(q / ((int64_t)Wo * Ho));
+    float m = -INFINITY;
+    int bi = 0, bj = 0;
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j) {
+        const float v = __bfloat162float(X[(((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + c]);
+        if (v > m) {
+          m = v;
+          bi = i;
+          bj = j;
+        }
+      }
+    dX[(((int64_t)b * H + 2 * h + bi) * W + 2 * w + bj) * C + c] += dY[t];
+  }
+}
+
+// cat[..., 0:C1] = up2(prev) (prev at H/2 x W/2), cat[..., C1:C1+C2] = skip
+__global__ void k_up_concat(int B, int H, int W, int C1, int C2, const __nv_bfloat16 *__restrict__ prev,
+                            const __nv_bfloat16 *__restrict__ skip, __nv_bfloat16 *__restrict__ cat) {
+  const int C = C1 + C2;
+  const int64_t total = (int64_t)B * H * W * C;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C);
+    const int64_t p = t / C;
+    if (c < C1) {
+      const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
+      cat[t] = prev[(((int64_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * C1 + c];
+    } else {
+      cat[t] = skip[p * C2 + (c - C1)];
+    }
+  }
+}
+
+__global__ void k_up_concat_back(int B, int H, int W, int C1, int C2, const float *__restrict__ dcat,
+                                 float *__restrict__ dprev, float *__restrict__ dskip) {
+  const int C = C1 + C2;
+  // dskip: direct
+  const int64_t totS = (int64_t)B * H * W * C2;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < totS;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C2);
+    const int64_t p = t / C2;
+    dskip[t] += dcat[p * C + C1 + c];
+  }
+  // dprev: sum of the 4 children
+  const int Hh = H / 2, Wh = W / 2;
+  const int64_t totP = (int64_t)B * Hh * Wh * C1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < totP;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C1);
+    const int64_t q = t / C1;
+    const int w = (int)(q % Wh), h = (int)((q / Wh) % Hh), b = (int)(q / ((int64_t)Wh * Hh));
+    float a = 0.f;
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j) a += dcat[(((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + c];
+    dprev[t] += a;
+  }
+}
+
+// head: out[p] = sum_c w[c]*Y[p][c] + b ; column-major image <-> NHWC
+__global__ void k_head(int64_t P, int C, const __nv_bfloat16 *__restrict__ Y, const float *__restrict__ w,
+                       const float *__restrict__ b, float *__restrict__ out) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    float a = b[0];
+    for (int c = 0; c < C; ++c) a += w[c] * __bfloat162float(Y[p * C + c]);
+    out[p] = a;
+  }
+}
+
+// loss = mean((out - t)^2); dout = 2 (out - t) / P; dY = dout * w; gw, gb
+__global__ void k_head_back(int64_t P, int C, const __nv_bfloat16 *__restrict__ Y, const float *__restrict__ w,
+                            const float *__restrict__ out, const float *__restrict__ tgt,
+                            float *__restrict__ dY, float *__restrict__ gw, float *__restrict__ gb,
+                            float *__restrict__ loss) {
+  float lsum = 0.f, bsum = 0.f;
+  float wsum[64];
+  for (int c = 0; c < C && c < 64; ++c) wsum[c] = 0.f;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const float d = out[p] - tgt[p];
+    lsum += d * d;
+    const float g = 2.f * d / (float)P;
+    bsum += g;
+    for (int c = 0; c < C; ++c) {
+      dY[p * C + c] = g * w[c];
+      if (c < 64) wsum[c] += g * __bfloat162float(Y[p * C + c]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(loss, lsum / (float)P);
+    atomicAdd(gb, bsum);
+  }
+  for (int c = 0; c < C && c < 64; ++c) {
+    float v = wsum[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(gw + c, v);
+  }
+}
+
+__global__ void k_to_bf16(int64_t n, const float *__restrict__ a, __nv_bfloat16 *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16(a[i]);
+}
+
+__global__ void k_adam(int64_t n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
+                       float *__restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float v = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = v;
+    w[i] -= lr * (a / c1) / (sqrtf(v / c2) + eps);
+  }
+}
+
+inline unsigned gsz(int64_t n) { return grid_for(n, kT, 8); }
+
+}  // namespace
+
+struct Tensor {
+  int C = 0, H = 0, W = 0;
+  DevBuf<__nv_bfloat16> y;  // [B*H*W][C]
+  DevBuf<float> g;          // gradient
+};
+
+struct Conv {
+  int cin, cout, kp, H, W;
+  Tensor *in, *out;
+  DevBuf<float> w, gw, mw, vw, b, gb, mb, vb;
+  DevBuf<__nv_bfloat16> w16;
+};
+
+struct UNet {
+  int H, W, base, levels, maxB;
+  cudaStream_t s = nullptr;
+  std::vector<Tensor *> tensors;
+  Tensor *xin;
+  std::vector<Tensor *> ea, eb, pool, cat, da, db;
+  std::vector<Conv> convs;  // forward order
+  DevBuf<float> hw, hgw, hmw, hvw, hb, hgb, hmb, hvb;  // head (1x1, base -> 1)
+  DevBuf<float> out, loss;
+  DevBuf<__nv_bfloat16> col, dym;
+  DevBuf<float> dcol;
+  DevBuf<int> err;
+  int64_t adam_t = 0;
+  Tensor *T(int C, int H, int W) {
+    Tensor *t = new Tensor();
+    t->C = C;
+    t->H = H;
+    t->W = W;
+    tensors.push_back(t);
+    return t;
+  }
+  ~UNet() {
+    for (Tensor *t : tensors) delete t;
+  }
+};
+
+namespace {
+
+int kp_of(int cin) { return ((9 * cin + 63) / 64) * 64; }
+
+void conv_alloc(UNet &U, Conv &c, std::mt19937_64 &rng) {
+  c.kp = kp_of(c.cin);
+  const size_t nw = (size_t)c.cout * c.kp;
+  std::vector<float> hw(nw, 0.f), hb(c.cout, 0.f);
+  std::normal_distribution<float> nd(0.f, std::sqrt(2.f / (9.f * c.cin)));
+  for (int o = 0; o < c.cout; ++o)
+    for (int k = 0; k < 9 * c.cin; ++k) hw[(size_t)o * c.kp + k] = nd(rng);
+  c.w.upload(hw.data(), nw, U.s);
+  c.b.upload(hb.data(), c.cout, U.s);
+  for (DevBuf<float> *d : {&c.gw, &c.mw, &c.vw}) {
+    d->ensure(nw);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(d->p, 0, nw * 4, U.s));
+  }
+  for (DevBuf<float> *d : {&c.gb, &c.mb, &c.vb}) {
+    d->ensure(c.cout);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(d->p, 0, c.cout * 4, U.s));
+  }
+  c.w16.ensure(nw);
+  k_to_bf16<<<gsz(nw), kT, 0, U.s>>>(nw, c.w.p, c.w16.p);
+}
+
+void ensure_act(UNet &U, Tensor *t, int B) {
+  const size_t n = (size_t)B * t->H * t->W * t->C;
+  t->y.ensure(n);
+  t->g.ensure(n);
+}
+
+int bn_for(int n) { return n >= 256 ? 256 : n >= 128 ? 128 : n >= 64 ? 64 : 32; }
+
+void conv_forward(UNet &U, Conv &c, int B) {
+  const int64_t P = (int64_t)B * c.H * c.W;
+  k_im2col<<<gsz(P * c.kp), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, c.in->y.p, U.col.p);
+  AIRT_LAUNCH_CHECK();
+  GemmArgs g{};
+  g.M = (int)P;
+  g.N = c.cout;
+  g.K = c.kp;
+  g.A = U.col.p;
+  g.lda = c.kp;
+  g.B = c.w16.p;
+  g.ldb = c.kp;
+  g.D = c.out->y.p;
+  g.ldd = c.cout;
+  g.bias = c.b.p;
+  g.ksplit = 0;
+  g.err = U.err.p;
+  gemm_bf16(g, bn_for(c.cout), false, false, EPI_BIAS_RELU_BF16, U.s);
+}
+
+void conv_backward(UNet &U, Conv &c, int B, bool need_dx) {
+  const int64_t P = (int64_t)B * c.H * c.W;
+  const int64_t ny = P * c.cout;
+  k_relu_mask<<<gsz(ny), kT, 0, U.s>>>(ny, c.out->g.p, c.out->y.p, U.dym.p);
+  k_colsum<<<c.cout, kT, 0, U.s>>>(P, c.cout, U.dym.p, c.gb.p);
+  k_im2col<<<gsz(P * c.kp), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, c.in->y.p, U.col.p);
+  AIRT_LAUNCH_CHECK();
+  // dW^T[Kp][Co] += col^T * dYm, stored transposed into gw[Co][Kp]
+  GemmArgs gw{};
+  gw.M = c.kp;
+  gw.N = c.cout;
+  gw.K = (int)P;
+  gw.A = U.col.p;
+  gw.lda = c.kp;
+  gw.B = U.dym.p;
+  gw.ldb = c.cout;
+  gw.D = c.gw.p;
+  gw.ldd = c.kp;
+  gw.ksplit = (int)std::max<int64_t>(64, ((P / 64 + 63) / 64) * 64);  // ~64 K-splits
+  gw.err = U.err.p;
+  gemm_bf16(gw, bn_for(c.cout), true, true, EPI_ATOMIC_F32_T, U.s);
+  if (!need_dx) return;
+  // dcol[P][Kp] = dYm[P][Co] * W[Co][Kp]
+  GemmArgs gd{};
+  gd.M = (int)P;
+  gd.N = c.kp;
+  gd.K = c.cout;
+  gd.A = U.dym.p;
+  gd.lda = c.cout;
+  gd.B = c.w16.p;
+  gd.ldb = c.kp;
+  gd.D = U.dcol.p;
+  gd.ldd = c.kp;
+  gd.ksplit = 0;
+  gd.err = U.err.p;
+  gemm_bf16(gd, bn_for(c.kp), false, true, EPI_STORE_F32, U.s);
+  k_col2im<<<gsz(P * c.cin), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, U.dcol.p, c.in->g.p);
+  AIRT_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+UNet *unet_create(int H, int W, int base, int levels, int maxB, uint64_t seed) {
+  AIRT_REQUIRE(levels >= 2 && levels <= 6, "levels must be 2..6");
+  AIRT_REQUIRE(base % 8 == 0 && base >= 8, "base width must be a multiple of 8");
+  AIRT_REQUIRE(H % (1 << (levels - 1)) == 0 && W % (1 << (levels - 1)) == 0,
+               "image size must be divisible by 2^(levels-1)");
+  AIRT_REQUIRE(maxB >= 1, "batch must be positive");
+  AIRT_REQUIRE(base <= 64, "head supports at most 64 channels");
+  UNet *U = new UNet();
+  try {
+    U->H = H;
+    U->W = W;
+    U->base = base;
+    U->levels = levels;
+    U->maxB = maxB;
+    AIRT_CHECK_CUDA(cudaStreamCreateWithFlags(&U->s, cudaStreamNonBlocking));
+    std::mt19937_64 rng(seed);
+    U->xin = U->T(1, H, W);
+    U->ea.resize(levels);
+    U->eb.resize(levels);
+    U->pool.assign(levels, nullptr);
+    U->cat.resize(levels - 1);
+    U->da.resize(levels - 1);
+    U->db.resize(levels - 1);
+    for (int l = 0; l < levels; ++l) {
+      const int h = H >> l, w = W >> l, c = base << l;
+      if (l > 0) U->pool[l] = U->T(base << (l - 1), h, w);
+      U->ea[l] = U->T(c, h, w);
+      U->eb[l] = U->T(c, h, w);
+    }
+    for (int l = levels - 2; l >= 0; --l) {
+      const int h = H >> l, w = W >> l, c = base << l;
+      U->cat[l] = U->T((base << (l + 1)) + c, h, w);
+      U->da[l] = U->T(c, h, w);
+      U->db[l] = U->T(c, h, w);
+    }
+    auto add = [&](Tensor *in, Tensor *out) {
+      Conv c;
+      c.cin = in->C;
+      c.cout = out->C;
+      c.H = out->H;
+      c.W = out->W;
+      c.in = in;
+      c.out = out;
+      U->convs.push_back(std::move(c));
+    };
+    U->convs.reserve(4 * levels);
+    for (int l = 0; l < levels; ++l) {
+      add(l == 0 ? U->xin : U->pool[l], U->ea[l]);
+      add(U->ea[l], U->eb[l]);
+    }
+    for (int l = levels - 2; l >= 0; --l) {
+      add(U->cat[l], U->da[l]);
+      add(U->da[l], U->db[l]);
+    }
+    for (Conv &c : U->convs) conv_alloc(*U, c, rng);
+    std::normal_distribution<float> nd(0.f, std::sqrt(1.f / base));
+    std::vector<float> hw(base);
+    for (float &v : hw) v = nd(rng);
+    float zero = 0.f;
+    U->hw.upload(hw.data(), base, U->s);
+    U->hb.upload(&zero, 1, U->s);
+    for (DevBuf<float> *d : {&U->hgw, &U->hmw, &U->hvw}) {
+      d->ensure(base);
+      AIRT_CHECK_CUDA(cudaMemsetAsync(d->p, 0, base * 4, U->s));
+    }
+    for (DevBuf<float> *d : {&U->hgb, &U->hmb, &U->hvb}) {
+      d->ensure(1);
+      AIRT_CHECK_CUDA(cudaMemsetAsync(d->p, 0, 4, U->s));
+    }
+    for (Tensor *t : U->tensors) ensure_act(*U, t, maxB);
+    size_t colmax = 0;
+    int64_t dymax = 0;
+    for (const Conv &c : U->convs) {
+      colmax = std::max(colmax, (size_t)maxB * c.H * c.W * c.kp);
+      dymax = std::max<int64_t>(dymax, (int64_t)maxB * c.H * c.W * c.cout);
+    }
+    U->col.ensure(colmax);
+    U->dcol.ensure(colmax);
+    U->dym.ensure(dymax);
+    U->out.ensure((size_t)maxB * H * W);
+    U->loss.ensure(1);
+    U->err.ensure(1);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(U->err.p, 0, sizeof(int), U->s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(U->s));
+  } catch (...) {
+    if (U->s) cudaStreamSynchronize(U->s);
+    cudaStream_t s = U->s;
+    delete U;
+    if (s) cudaStreamDestroy(s);
+    throw;
+  }
+  return U;
+}
+
+void unet_destroy(UNet *U) {
+  if (!U) return;
+  cudaStream_t s = U->s;
+  if (s) cudaStreamSynchronize(s);
+  delete U;
+  if (s) cudaStreamDestroy(s);
+}
+
+cudaStream_t unet_stream(UNet &U) { return U.s; }
+
+// in: [B][H*W] FP32 images in the x(:) (column-major) order of the solvers;
+// with NHWC pixel (b, h, w) = in[b][w*H + h] ... the map is a transpose, so
+// images are copied with h = row index of the column-major image.
+namespace {
+__global__ void k_img_in(int B, int H, int W, const float *__restrict__ in, __nv_bfloat16 *__restrict__ x) {
+  const int64_t total = (int64_t)B * H * W;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
+    x[t] = __float2bfloat16(in[(int64_t)b * H * W + (int64_t)w * H + h]);
+  }
+}
+__global__ void k_img_out(int B, int H, int W, const float *__restrict__ o, float *__restrict__ out) {
+  const int64_t total = (int64_t)B * H * W;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
+    out[(int64_t)b * H * W + (int64_t)w * H + h] = o[t];
+  }
+}
+__global__ void k_img_tgt(int B, int H, int W, const float *__restrict__ in, float *__restrict__ o) {
+  const int64_t total = (int64_t)B * H * W;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
+    o[t] = in[(int64_t)b * H * W + (int64_t)w * H + h];
+  }
+}
+}  // namespace
+
+void unet_forward(UNet &U, const float *d_in, int B) {
+  AIRT_REQUIRE(B >= 1 && B <= U.maxB, "batch larger than the network was created for");
+  const int64_t P0 = (int64_t)B * U.H * U.W;
+  k_img_in<<<gsz(P0), kT, 0, U.s>>>(B, U.H, U.W, d_in, U.xin->y.p);
+  int ci = 0;
+  for (int l = 0; l < U.levels; ++l) {
+    if (l > 0) {
+      Tensor *src = U.eb[l - 1];
+      k_pool<<<gsz((int64_t)B * U.pool[l]->H * U.pool[l]->W * src->C), kT, 0, U.s>>>(
+          B, src->H, src->W, src->C, src->y.p, U.pool[l]->y.p);
+    }
+    conv_forward(U, U.convs[ci++], B);
+    conv_forward(U, U.convs[ci++], B);
+  }
+  for (int l = U.levels - 2; l >= 0; --l) {
+    Tensor *prev = (l == U.levels - 2) ? U.eb[U.levels - 1] : U.db[l + 1];
+    Tensor *cat = U.cat[l];
+    k_up_concat<<<gsz((int64_t)B * cat->H * cat->W * cat->C), kT, 0, U.s>>>(
+        B, cat->H, cat->W, prev->C, U.eb[l]->C, prev->y.p, U.eb[l]->y.p, cat->y.p);
+    conv_forward(U, U.convs[ci++], B);
+    conv_forward(U, U.convs[ci++], B);
+  }
+  k_head<<<gsz(P0), kT, 0, U.s>>>(P0, U.base, U.db[0]->y.p, U.hw.p, U.hb.p, U.out.p);
+  AIRT_LAUNCH_CHECK();
+}
+
+void unet_output(UNet &U, float *d_out, int B) {
+  k_img_out<<<gsz((int64_t)B * U.H * U.W), kT, 0, U.s>>>(B, U.H, U.W, U.out.p, d_out);
+  AIRT_LAUNCH_CHECK();
+}
+
+// Forward + backward; gradients land in the g* buffers (zeroed here).
+// Returns the MSE loss of the batch.
+float unet_gradients(UNet &U, const float *d_in, const float *d_tgt, int B) {
+  unet_forward(U, d_in, B);
+  const int64_t P0 = (int64_t)B * U.H * U.W;
+  for (Conv &c : U.convs) {
+    AIRT_CHECK_CUDA(cudaMemsetAsync(c.gw.p, 0, (size_t)c.cout * c.kp * 4, U.s));
+    AIRT_CHECK_CUDA(cudaMemsetAsync(c.gb.p, 0, (size_t)c.cout * 4, U.s));
+  }
+  AIRT_CHECK_CUDA(cudaMemsetAsync(U.hgw.p, 0, U.base * 4, U.s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(U.hgb.p, 0, 4, U.s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(U.loss.p, 0, 4, U.s));
+  for (Tensor *t : U.tensors)
+    AIRT_CHECK_CUDA(cudaMemsetAsync(t->g.p, 0, (size_t)B * t->H * t->W * t->C * 4, U.s));
+  float *tgt = U.dcol.p;  // target in NHWC order (dcol is free until the first conv backward)
+  k_img_tgt<<<gsz(P0), kT, 0, U.s>>>(B, U.H, U.W, d_tgt, tgt);
+  k_head_back<<<gsz(P0), kT, 0, U.s>>>(P0, U.base, U.db[0]->y.p, U.hw.p, U.out.p, tgt,
+                                        U.db[0]->g.p, U.hgw.p, U.hgb.p, U.loss.p);
+  AIRT_LAUNCH_CHECK();
+  int ci = (int)U.convs.size() - 1;
+  // decoder, in reverse of the forward order (levels 0 .. L-2)
+  for (int l = 0; l <= U.levels - 2; ++l) {
+    conv_backward(U, U.convs[ci--], B, true);  // da[l] -> db[l]
+    conv_backward(U, U.convs[ci--], B, true);  // cat[l] -> da[l]
+    Tensor *prev = (l == U.levels - 2) ? U.eb[U.levels - 1] : U.db[l + 1];
+    Tensor *cat = U.cat[l];
+    k_up_concat_back<<<gsz((int64_t)B * cat->H * cat->W * cat->C), kT, 0, U.s>>>(
+        B, cat->H, cat->W, prev->C, U.eb[l]->C, cat->g.p, prev->g.p, U.eb[l]->g.p);
+    AIRT_LAUNCH_CHECK();
+  }
+  // encoder, levels L-1 .. 0; eb[l] has its skip and pool gradients by now
+  for (int l = U.levels - 1; l >= 0; --l) {
+    conv_backward(U, U.convs[ci--], B, true);    // ea[l] -> eb[l]
+    conv_backward(U, U.convs[ci--], B, l > 0);   // in -> ea[l]
+    if (l > 0) {
+      Tensor *src = U.eb[l - 1];
+      k_pool_back<<<gsz((int64_t)B * U.pool[l]->H * U.pool[l]->W * src->C), kT, 0, U.s>>>(
+          B, src->H, src->W, src->C, src->y.p, U.pool[l]->g.p, src->g.p);
+      AIRT_LAUNCH_CHECK();
+    }
+  }
+  float h = 0.f;
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(&h, U.loss.p, 4, cudaMemcpyDeviceToHost, U.s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(U.s));
+  int herr = 0;
+  AIRT_CHECK_CUDA(cudaMemcpy(&herr, U.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (herr) {
+    set_error("a bounded tensor-core wait gave up");
+    throw Status{AIRT_ERR_TIMEOUT};
+  }
+  return h;
+}
+
+void unet_adam(UNet &U, float lr) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  ++U.adam_t;
+  const float c1 = 1.f - std::pow(b1, (float)U.adam_t), c2 = 1.f - std::pow(b2, (float)U.adam_t);
+  for (Conv &c : U.convs) {
+    const int64_t nw = (int64_t)c.cout * c.kp;
+    k_adam<<<gsz(nw), kT, 0, U.s>>>(nw, c.w.p, c.gw.p, c.mw.p, c.vw.p, lr, b1, b2, eps, c1, c2);
+    k_adam<<<gsz(c.cout), kT, 0, U.s>>>(c.cout, c.b.p, c.gb.p, c.mb.p, c.vb.p, lr, b1, b2, eps, c1, c2);
+    k_to_bf16<<<gsz(nw), kT, 0, U.s>>>(nw, c.w.p, c.w16.p);
+  }
+  k_adam<<<1, kT, 0, U.s>>>(U.base, U.hw.p, U.hgw.p, U.hmw.p, U.hvw.p, lr, b1, b2, eps, c1, c2);
+  k_adam<<<1, kT, 0, U.s>>>(1, U.hb.p, U.hgb.p, U.hmb.p, U.hvb.p, lr, b1, b2, eps, c1, c2);
+  AIRT_LAUNCH_CHECK();
+}
+
+// Flattened parameters: per convolution (forward order) W[cout][9*cin]
+// (K index (kh*3+kw)*cin + ci) then b[cout]; then the head w[base], b.
+int64_t unet_num_params(const UNet &U) {
+  int64_t n = 0;
+  for (const Conv &c : U.convs) n += (int64_t)c.cout * 9 * c.cin + c.cout;
+  return n + U.base + 1;
+}
+
+void unet_params(UNet &U, float *host, bool grads, bool set) {
+  int64_t off = 0;
+  auto xfer = [&](DevBuf<float> &d, size_t n, size_t dst_stride, size_t src_stride, size_t rows) {
+    // rows x n block between host (packed, stride n) and device (stride src_stride)
+    std::vector<float> tmp(rows * src_stride);
+    if (!set) {
+      AIRT_CHECK_CUDA(cudaMemcpyAsync(tmp.data(), d.p, tmp.size() * 4, cudaMemcpyDeviceToHost, U.s));
+      AIRT_CHECK_CUDA(cudaStreamSynchronize(U.s));
+      for (size_t r = 0; r < rows; ++r)
+        for (size_t k = 0; k < n; ++k) host[off + r * dst_stride + k] = tmp[r * src_stride + k];
+    } else {
+      std::fill(tmp.begin(), tmp.end(), 0.f);
+      for (size_t r = 0; r < rows; ++r)
+        for (size_t k = 0; k < n; ++k) tmp[r * src_stride + k] = host[off + r * dst_stride + k];
+      AIRT_CHECK_CUDA(cudaMemcpyAsync(d.p, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice, U.s));
+      AIRT_CHECK_CUDA(cudaStreamSynchronize(U.s));
+    }
+    off += rows * n;
+  };
+  for (Conv &c : U.convs) {
+    xfer(grads ? c.gw : c.w, 9 * c.cin, 9 * c.cin, c.kp, c.cout);
+    xfer(grads ? c.gb : c.b, c.cout, c.cout, c.cout, 1);
+    if (set && !grads) {
+      const int64_t nw = (int64_t)c.cout * c.kp;
+      k_to_bf16<<<gsz(nw), kT, 0, U.s>>>(nw, c.w.p, c.w16.p);
+    }
+  }
+  xfer(grads ? U.hgw : U.hw, U.base, U.base, U.base, 1);
+  xfer(grads ? U.hgb : U.hb, 1, 1, 1, 1);
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(U.s));
+}
+
+}  // namespace airt
+
+using namespace airt;
+
+#define UNET_API_BEGIN try {
+#define UNET_API_END                 \
+  }                                  \
+  catch (const airt::Status &st) {   \
+    return st.code;                  \
+  }                                  \
+  catch (...) {                      \
+    set_error("unexpected internal error"); \
+    return AIRT_ERR_CUDA;            \
+  }                                  \
+  return AIRT_OK;
+
+extern "C" {
+
+int airt_unet_create(int H, int W, int base, int levels, int max_batch, uint64_t seed, airt_unet **out) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(out, "null pointer argument");
+  *out = reinterpret_cast<airt_unet *>(unet_create(H, W, base, levels, max_batch, seed));
+  UNET_API_END
+}
+
+int airt_unet_destroy(airt_unet *h) {
+  UNET_API_BEGIN
+  unet_destroy(reinterpret_cast<UNet *>(h));
+  UNET_API_END
+}
+
+int airt_unet_stream(const airt_unet *h, void **cuda_stream) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && cuda_stream, "null pointer argument");
+  *cuda_stream = (void *)reinterpret_cast<const UNet *>(h)->s;
+  UNET_API_END
+}
+
+int airt_unet_num_params(const airt_unet *h, int64_t *n) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && n, "null pointer argument");
+  *n = unet_num_params(*reinterpret_cast<const UNet *>(h));
+  UNET_API_END
+}
+
+int airt_unet_get_params(airt_unet *h, float *host) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && host, "null pointer argument");
+  unet_params(*reinterpret_cast<UNet *>(h), host, false, false);
+  UNET_API_END
+}
+
+int airt_unet_set_params(airt_unet *h, const float *host) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && host, "null pointer argument");
+  unet_params(*reinterpret_cast<UNet *>(h), const_cast<float *>(host), false, true);
+  UNET_API_END
+}
+
+int airt_unet_get_grads(airt_unet *h, float *host) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && host, "null pointer argument");
+  unet_params(*reinterpret_cast<UNet *>(h), host, true, false);
+  UNET_API_END
+}
+
+int airt_unet_forward(airt_unet *h, const float *d_in, float *d_out, int B) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && d_in && d_out, "null pointer argument");
+  UNet &U = *reinterpret_cast<UNet *>(h);
+  unet_forward(U, d_in, B);
+  unet_output(U, d_out, B);
+  UNET_API_END
+}
+
+int airt_unet_gradients(airt_unet *h, const float *d_in, const float *d_tgt, int B, float *loss) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && d_in && d_tgt, "null pointer argument");
+  const float l = unet_gradients(*reinterpret_cast<UNet *>(h), d_in, d_tgt, B);
+  if (loss) *loss = l;
+  UNET_API_END
+}
+
+int airt_unet_train_step(airt_unet *h, const float *d_in, const float *d_tgt, int B, float lr,
+                         float *loss) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && d_in && d_tgt && lr > 0, "invalid argument");
+  UNet &U = *reinterpret_cast<UNet *>(h);
+  const float l = unet_gradients(U, d_in, d_tgt, B);
+  unet_adam(U, lr);
+  if (loss) *loss = l;
+  UNET_API_END
+}
+
+}  // extern "C"

@@ -197,6 +197,31 @@ int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double r
                         int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms);
 int airt_batch_destroy(airt_batch *h);
 
+/* ---- learned warm start ---------------------------------------------------- */
+/* No counterpart in the reference; the network's output enters the solvers
+ * only as x0 (sirt/sirt.m:5).  A U-Net of `levels` levels (two 3x3
+ * conv+ReLU per level, widths base*2^l, 2x2 max-pool down, nearest 2x up with
+ * skip concatenation, 1x1 head) on H x W images, BF16 activations and tensor-
+ * core GEMMs with FP32 accumulation, FP32 master weights and Adam.  Images
+ * are FP32 device arrays of B images in the solvers' x(:) (column-major)
+ * order.  Parameters flatten per convolution (W[cout][9*cin] with K index
+ * (kh*3+kw)*cin+ci, then b[cout]) followed by the head (w[base], b). */
+typedef struct airt_unet airt_unet;
+int airt_unet_create(int H, int W, int base, int levels, int max_batch, uint64_t seed,
+                     airt_unet **out);
+int airt_unet_destroy(airt_unet *h);
+int airt_unet_stream(const airt_unet *h, void **cuda_stream);
+int airt_unet_num_params(const airt_unet *h, int64_t *n);
+int airt_unet_get_params(airt_unet *h, float *host);
+int airt_unet_set_params(airt_unet *h, const float *host);
+int airt_unet_get_grads(airt_unet *h, float *host);
+int airt_unet_forward(airt_unet *h, const float *d_in, float *d_out, int B);
+/* MSE loss mean((net(in) - target)^2) and its gradient (airt_unet_get_grads). */
+int airt_unet_gradients(airt_unet *h, const float *d_in, const float *d_tgt, int B, float *loss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on the batch; returns the loss. */
+int airt_unet_train_step(airt_unet *h, const float *d_in, const float *d_tgt, int B, float lr,
+                         float *loss);
+
 /* ---- allocation-free residual ------------------------------------------------ */
 /* No counterpart in the reference.  r = b - A*x and ||r|| (into d_resnorm) for
  * a caller that holds an FP32 CSR (d_rp m+1, d_ci/d_rv nnz), x, b and r on

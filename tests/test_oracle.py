@@ -245,3 +245,27 @@ def test_calczeta_roots():
     k = np.arange(2, 30)
     g = (2 * k - 1) * z ** (k - 1) - np.array([np.sum(zz ** np.arange(kk - 1)) for zz, kk in zip(z, k)])
     assert np.max(np.abs(g)) < 1e-10
+
+
+def test_unet_oracle_gradient_matches_finite_differences():
+    """The NumPy U-Net used as the GPU gradient checker, without BF16 rounding,
+    against central differences on random parameters."""
+    from oracle import unet_oracle as UO
+    base, levels, H, W = 8, 2, 8, 8
+    n = sum(co * 9 * ci + co for ci, co in UO.layer_shapes(base, levels)) + base + 1
+    rng = np.random.default_rng(4)
+    p = rng.standard_normal(n) * 0.3
+    x = rng.random((2, H * W))
+    t = rng.random((2, H * W))
+    UO.EXACT = True
+    try:
+        _, g, _ = UO.forward_backward(p, x, t, base, levels, H, W)
+        for i in rng.choice(n, 25, replace=False):
+            e = np.zeros(n)
+            e[i] = 1e-6
+            lp, _, _ = UO.forward_backward(p + e, x, t, base, levels, H, W)
+            lm, _, _ = UO.forward_backward(p - e, x, t, base, levels, H, W)
+            fd = (lp - lm) / 2e-6
+            assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i])), (i, fd, g[i])
+    finally:
+        UO.EXACT = False
