@@ -100,10 +100,14 @@ SIGNATURES = {
     "airt_unet_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "airt_unet_get_grads": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "airt_unet_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "airt_unet_forward_f64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.c_void_p]),
     "airt_unet_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                       C.POINTER(C.c_float)]),
     "airt_unet_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
                                        C.POINTER(C.c_float)]),
+    "airt_phantom_ellipses": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, C.c_double, C.c_double,
+                                        C.c_void_p, C.c_void_p]),
     "airt_residual_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),

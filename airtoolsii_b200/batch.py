@@ -151,6 +151,33 @@ class ParallelBatch:
                 "rho": None if rho is None else np.asarray(rho), "gpu_ms": float(ms.value)}
         return self.split_cols(x), info
 
+    def sirt_device(self, method, d_b, d_x, kmax, taudelta=None, relaxpar=None, rho=None,
+                    lbound=None, ubound=None, d_x0=None):
+        """sirt on device vectors: d_b (m doubles), d_x (n doubles), optional
+        d_x0 (n doubles) given as device addresses.  Returns info as sirt."""
+        if relaxpar is None:
+            if method == "sart":
+                rho = np.ones(self.K)
+            elif rho is None:
+                rho = self.rho(method)
+            lam = 1.9 / np.broadcast_to(np.asarray(rho, dtype=np.float64), (self.K,))
+        else:
+            lam = np.broadcast_to(np.asarray(relaxpar, dtype=np.float64), (self.K,))
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        td = None if taudelta is None else np.ascontiguousarray(
+            np.broadcast_to(np.asarray(taudelta, dtype=np.float64), (self.K,)))
+        fin = np.zeros(self.K, np.int64)
+        rule = np.zeros(self.K, np.int32)
+        ms = C.c_double()
+        lk, lv = _bounds(lbound)
+        uk, uv = _bounds(ubound)
+        check(self._L.airt_batch_sirt_device(self._h, _lib.METHODS[method], dptr(lam),
+                                             C.c_void_p(d_b), dptr(td), int(kmax), lk, lv, uk,
+                                             uv, C.c_void_p(d_x0 or None), C.c_void_p(d_x),
+                                             _lib.i64ptr(fin), rule.ctypes.data_as(_ip),
+                                             C.byref(ms)))
+        return {"finaliter": fin, "stoprule": rule, "relaxpar": lam, "gpu_ms": float(ms.value)}
+
     def kaczmarz(self, b, sweeps, relaxpar=1.0, lbound=None, ubound=None):
         """Kaczmarz sweeps (row order of art.m:188) on every instance from x0 = 0."""
         b = np.ascontiguousarray(np.concatenate(b) if isinstance(b, (list, tuple)) else b,

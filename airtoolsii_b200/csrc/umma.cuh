@@ -3,17 +3,18 @@
 //
 //   D[M x N] (+)= A[M x K] * B[N x K]^T
 //
-// One CTA computes a 128 x BN tile with 128 threads (4 warps):
-//  * all threads stage the A and B tiles of a 64-wide K slice from global
-//    memory into shared memory in the canonical no-swizzle UMMA layout
-//    (8 x 16-byte core matrices), zero-filling outside the matrix;
-//  * one thread issues four tcgen05.mma.kind::f16 (K = 16 each) per slice,
-//    and tcgen05.commit signals an mbarrier when they have read the stage;
-//  * two stages alternate, so the next slice is staged while the tensor core
-//    works on the current one;
+// One CTA computes a 128 x BN tile with 5 warps:
+//  * warps 0-3 stage the A and B tiles of 64-wide K slices from global
+//    memory into an S-stage shared-memory ring in the canonical no-swizzle
+//    UMMA layout (8 x 16-byte core matrices) with cp.async, zero-filling
+//    outside the matrix; each thread's copies complete onto the stage's
+//    `full` mbarrier (cp.async.mbarrier.arrive);
+//  * one thread of warp 4 waits for a full stage, issues four
+//    tcgen05.mma.kind::f16 (K = 16 each) and commits them to the stage's
+//    `empty` mbarrier, which releases the stage to the producers;
 //  * the accumulator lives in TMEM (128 lanes x BN FP32 columns); after the
-//    last slice each warp reads its 32 lanes with tcgen05.ld and runs the
-//    epilogue (store, bias + ReLU, or split-K atomic accumulation).
+//    last slice warps 0-3 read their 32 lanes each with tcgen05.ld and run
+//    the epilogue (store, bias + ReLU, accumulate, or split-K atomics).
 //
 // Operand "majorness": K-major means the K index is contiguous in global
 // memory (row-major [rows][K]); MN-major means the M (or N) index is
@@ -35,7 +36,8 @@ namespace umma {
 
 constexpr int BM = 128;
 constexpr int BK = 64;
-constexpr int kThreads = 128;
+constexpr int kProducers = 128;                // operand-gathering and epilogue threads
+constexpr int kGemmThreads = kProducers + 32;  // plus one MMA-issuing warp
 constexpr long long kWaitBudget = 4000000000ll;  // ~2 s of SM clocks
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -131,6 +133,7 @@ enum GemmEpi {
   EPI_BIAS_RELU_BF16 = 1, // relu(D + bias[n]) -> bf16 [M][ldd]
   EPI_BIAS_BF16 = 2,      // D + bias[n] -> bf16
   EPI_ATOMIC_F32_T = 3,   // atomicAdd(D) into fp32 stored transposed [N][ldd] (split-K)
+  EPI_ADD_F32 = 4,        // D += result, fp32 [M][ldd] (no split-K)
 };
 
 struct GemmArgs {
@@ -143,8 +146,107 @@ struct GemmArgs {
   const float *bias;
   int ksplit;              // K range per blockIdx.z
   int *err;
+  // implicit 3x3 convolution: A is gathered from an NHWC image X (conv_C
+  // channels, conv_C % 8 == 0) instead of a materialised im2col matrix;
+  // K index (kh*3 + kw)*conv_C + ci, zero outside the image and for K >= 9C.
+  const __nv_bfloat16 *convX;
+  int conv_H, conv_W, conv_C;
 };
 
+// Epilogue of a 128 x BN tile held in TMEM, run by warps 0-3 (warp w owns
+// TMEM lanes and tile rows 32w..32w+31).  have_acc = false: the tile's K
+// range was empty and the result is zero.
+template <int BN, int EPI>
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, uint32_t tmem, int m0, int n0,
+                                              bool have_acc) {
+  using namespace umma;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = m0 + warp * 32 + lane;
+  // 16-byte row stores when the 8 columns are in range and aligned
+  const bool vec_ok = (g.ldd & 7) == 0 && ((uintptr_t)g.D & 15) == 0 &&
+                      (g.bias == nullptr || ((uintptr_t)g.bias & 15) == 0);
+#pragma unroll 1
+  for (int c = 0; c < BN; c += 8) {
+    float v[8];
+    if (have_acc) {
+      tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = 0.f;
+    }
+    if (EPI != EPI_ATOMIC_F32_T && vec_ok && row < g.M && n0 + c + 8 <= g.N) {
+      const int col = n0 + c;
+      if (EPI == EPI_STORE_F32 || EPI == EPI_ADD_F32) {
+        float4 *d = reinterpret_cast<float4 *>((float *)g.D + (size_t)row * g.ldd + col);
+        float4 a = make_float4(v[0], v[1], v[2], v[3]), b = make_float4(v[4], v[5], v[6], v[7]);
+        if (EPI == EPI_ADD_F32) {
+          const float4 a0 = d[0], b0 = d[1];
+          a.x += a0.x; a.y += a0.y; a.z += a0.z; a.w += a0.w;
+          b.x += b0.x; b.y += b0.y; b.z += b0.z; b.w += b0.w;
+        }
+        d[0] = a;
+        d[1] = b;
+      } else {
+        if (g.bias) {
+          const float4 b0 = __ldg(reinterpret_cast<const float4 *>(g.bias + col));
+          const float4 b1 = __ldg(reinterpret_cast<const float4 *>(g.bias + col) + 1);
+          v[0] += b0.x; v[1] += b0.y; v[2] += b0.z; v[3] += b0.w;
+          v[4] += b1.x; v[5] += b1.y; v[6] += b1.z; v[7] += b1.w;
+        }
+        uint4 pk;
+        uint32_t *pw = reinterpret_cast<uint32_t *>(&pk);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          float lo = v[2 * i], hi = v[2 * i + 1];
+          if (EPI == EPI_BIAS_RELU_BF16) {
+            lo = fmaxf(lo, 0.f);
+            hi = fmaxf(hi, 0.f);
+          }
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
+          pw[i] = *reinterpret_cast<const uint32_t *>(&h2);
+        }
+        *reinterpret_cast<uint4 *>((__nv_bfloat16 *)g.D + (size_t)row * g.ldd + col) = pk;
+      }
+      continue;
+    }
+    if (row < g.M) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int col = n0 + c + i;
+        if (col >= g.N) continue;
+        float y = v[i];
+        if (EPI == EPI_STORE_F32) {
+          ((float *)g.D)[(size_t)row * g.ldd + col] = y;
+        } else if (EPI == EPI_BIAS_RELU_BF16 || EPI == EPI_BIAS_BF16) {
+          y += g.bias ? g.bias[col] : 0.f;
+          if (EPI == EPI_BIAS_RELU_BF16) y = fmaxf(y, 0.f);
+          ((__nv_bfloat16 *)g.D)[(size_t)row * g.ldd + col] = __float2bfloat16(y);
+        } else if (EPI == EPI_ADD_F32) {
+          ((float *)g.D)[(size_t)row * g.ldd + col] += y;
+        } else {
+          atomicAdd((float *)g.D + (size_t)col * g.ldd + row, y);
+        }
+      }
+    }
+  }
+}
+
 void gemm_bf16(const GemmArgs &g, int bn, bool a_mn, bool b_mn, int epi, cudaStream_t s);
+// Implicit-GEMM 3x3 convolution forward: D = act(conv(X) + bias), A gathered
+// from g.convX, B = weights [N][ldb] K-major.
+void conv3x3_bf16(const GemmArgs &g, int bn, int epi, cudaStream_t s);
+// Implicit-GEMM weight gradient of a 3x3 convolution: gw[N][ldd] +=
+// (col(X)^T[M][K] * dY[K][N])^T with M = padded 9*conv_C, K = pixels (split
+// by ksplit), B = dY MN-major [pixels][ldb], A^T gathered from g.convX.
+void conv3x3_wgrad_bf16(const GemmArgs &g, int bn, cudaStream_t s);
+
+// TMA-fed variants (gemm_tma.cu) for K-major operands; the *_ok predicates
+// say whether the operands' alignment and shape allow them.
+bool gemm_tma_ok(const GemmArgs &g);
+void gemm_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s);
+bool conv3x3_tma_ok(const GemmArgs &g);
+void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s);
+// Operand path: 0 = TMA where possible, 1 = always cp.async (a test switch).
+extern int g_gemm_path;
 
 }  // namespace airt

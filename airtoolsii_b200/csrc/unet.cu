@@ -6,15 +6,21 @@
 // Layout: activations NHWC BF16 ([pixel][channel], pixel = (b*H + h)*W + w),
 // gradients FP32, weights FP32 masters [Cout][Kp] with a BF16 copy for the
 // tensor cores (Kp = 9*Cin rounded up to 64, zero padded; K index
-// (kh*3 + kw)*Cin + ci).  Every 3x3 convolution is an im2col followed by the
-// tcgen05 GEMM of umma.cuh:
+// (kh*3 + kw)*Cin + ci).  Every 3x3 convolution is a tcgen05 GEMM of
+// umma.cuh whose A tiles are gathered straight from the NHWC activations
+// (implicit GEMM, col(X) is never stored):
 //   forward  Y[P][Co]  = relu(col(X)[P][Kp] * W[Co][Kp]^T + b)   (K/K-major)
 //   dW^T     [Kp][Co] += col(X)^T * dYm   (both MN-major, split-K atomics
 //                        written transposed straight into W's layout)
-//   dcol     [P][Kp]   = dYm[P][Co] * W   (W as MN-major B), then col2im.
-// The image (x(:), column-major N x N) maps to NHWC with h = column-major row.
+//   dX       [P][Ci]  += col(dYm)[P][Kq] * Wt[Ci][Kq]^T, the 3x3 convolution
+//                        of dYm with the tap-flipped, transposed weights
+//                        Wt[ci][(8-tap)*Co + co] = W[co][tap*Ci + ci].
+// The first convolution (Cin = 1, not a multiple of 8 channels) keeps an
+// explicit im2col.  The image (x(:), column-major N x N) maps to NHWC with
+// h = column-major row.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <random>
 #include <vector>
@@ -47,6 +53,18 @@ __global__ void k_im2col(int B, int H, int W, int C, int Kp, const __nv_bfloat16
   }
 }
 
+// Wt[ci][kq] = W[co][(8 - tap)*Ci + ci] for kq = tap*Co + co < 9*Co, else 0.
+__global__ void k_flip_w(int Co, int Ci, int Kp, int Kq, const __nv_bfloat16 *__restrict__ w,
+                         __nv_bfloat16 *__restrict__ wt) {
+  const int64_t total = (int64_t)Ci * Kq;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int kq = (int)(t % Kq), ci = (int)(t / Kq);
+    const int tap = kq / Co, co = kq - tap * Co;
+    wt[t] = tap < 9 ? w[(int64_t)co * Kp + (8 - tap) * Ci + ci] : __float2bfloat16(0.f);
+  }
+}
+
 __global__ void k_col2im(int B, int H, int W, int C, int Kp, const float *__restrict__ dcol,
                          float *__restrict__ dX) {
   const int64_t total = (int64_t)B * H * W * C;
@@ -69,26 +87,50 @@ __global__ void k_col2im(int B, int H, int W, int C, int Kp, const float *__rest
 }
 
 // dYm = bf16(dY * (Y > 0)) and db += column sums (one block per 256 columns-slab)
-__global__ void k_relu_mask(int64_t n, const float *__restrict__ dY, const __nv_bfloat16 *__restrict__ Y,
-                            __nv_bfloat16 *__restrict__ dYm) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    dYm[i] = __float2bfloat16(__bfloat162float(Y[i]) > 0.f ? dY[i] : 0.f);
-}
-
-__global__ void k_colsum(int64_t P, int C, const __nv_bfloat16 *__restrict__ M, float *__restrict__ out) {
-  // grid.x over channels, each block reduces one channel
-  const int c = blockIdx.x;
-  float a = 0.f;
-  for (int64_t p = threadIdx.x; p < P; p += blockDim.x) a += __bfloat162float(M[p * C + c]);
-  __shared__ float sh[kT / 32];
-  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    float t = threadIdx.x < kT / 32 ? sh[threadIdx.x] : 0.f;
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (threadIdx.x == 0) out[c] += t;
+// dYm = bf16(dY * (Y > 0)) and db[c] += sum over pixels of dYm[p][c].
+// Each block owns a contiguous range of pixel rows; with C < 256 a pass
+// covers 256 / C rows (thread t: row t / C, column t % C), with C >= 256
+// each thread walks columns t, t + 256, ...  Per-thread sums meet in shared
+// memory and leave the block as one atomicAdd per column.
+__global__ void __launch_bounds__(256) k_relu_mask_colsum(int64_t P, int C, int64_t rows_per_block,
+                                                          const float *__restrict__ dY,
+                                                          const __nv_bfloat16 *__restrict__ Y,
+                                                          __nv_bfloat16 *__restrict__ dYm,
+                                                          float *__restrict__ db) {
+  __shared__ float sh[256];
+  const int t = threadIdx.x;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(P, r0 + rows_per_block);
+  if (C < 256) {
+    const int R = 256 / C;
+    float acc = 0.f;
+    if (t < R * C) {
+      const int c = t % C;
+      for (int64_t r = r0 + t / C; r < r1; r += R) {
+        const int64_t i = r * C + c;
+        const __nv_bfloat16 m = __float2bfloat16(__bfloat162float(Y[i]) > 0.f ? dY[i] : 0.f);
+        dYm[i] = m;
+        acc += __bfloat162float(m);
+      }
+    }
+    sh[t] = acc;
+    __syncthreads();
+    if (t < C) {
+      float a = 0.f;
+      for (int k = 0; k < R; ++k) a += sh[t + k * C];
+      atomicAdd(db + t, a);
+    }
+  } else {
+    for (int c = t; c < C; c += 256) {
+      float acc = 0.f;
+      for (int64_t r = r0; r < r1; ++r) {
+        const int64_t i = r * C + c;
+        const __nv_bfloat16 m = __float2bfloat16(__bfloat162float(Y[i]) > 0.f ? dY[i] : 0.f);
+        dYm[i] = m;
+        acc += __bfloat162float(m);
+      }
+      atomicAdd(db + c, acc);
+    }
   }
 }
 
@@ -135,20 +177,24 @@ __global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__r
 }
 
 // cat[..., 0:C1] = up2(prev) (prev at H/2 x W/2), cat[..., C1:C1+C2] = skip
+// cat = [nearest-2x(prev) | skip] along channels, 8 channels (16 bytes) per
+// thread; C1 and C2 are multiples of 8.
 __global__ void k_up_concat(int B, int H, int W, int C1, int C2, const __nv_bfloat16 *__restrict__ prev,
                             const __nv_bfloat16 *__restrict__ skip, __nv_bfloat16 *__restrict__ cat) {
-  const int C = C1 + C2;
-  const int64_t total = (int64_t)B * H * W * C;
+  const int C8 = (C1 + C2) / 8, c18 = C1 / 8;
+  const int64_t total = (int64_t)B * H * W * C8;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t % C);
-    const int64_t p = t / C;
-    if (c < C1) {
+    const int c8 = (int)(t % C8);
+    const int64_t p = t / C8;
+    uint4 v;
+    if (c8 < c18) {
       const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
-      cat[t] = prev[(((int64_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * C1 + c];
+      v = reinterpret_cast<const uint4 *>(prev)[(((int64_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * c18 + c8];
     } else {
-      cat[t] = skip[p * C2 + (c - C1)];
+      v = reinterpret_cast<const uint4 *>(skip)[p * (C2 / 8) + (c8 - c18)];
     }
+    reinterpret_cast<uint4 *>(cat)[t] = v;
   }
 }
 
@@ -256,7 +302,7 @@ struct Conv {
   int cin, cout, kp, H, W;
   Tensor *in, *out;
   DevBuf<float> w, gw, mw, vw, b, gb, mb, vb;
-  DevBuf<__nv_bfloat16> w16;
+  DevBuf<__nv_bfloat16> w16, wt16;  // wt16: tap-flipped transpose for dX
 };
 
 struct UNet {
@@ -270,6 +316,7 @@ struct UNet {
   DevBuf<float> out, loss;
   DevBuf<__nv_bfloat16> col, dym;
   DevBuf<float> dcol;
+  DevBuf<float> tgt;  // training target in NHWC order, maxB*H*W
   DevBuf<int> err;
   int64_t adam_t = 0;
   Tensor *T(int C, int H, int W) {
@@ -308,6 +355,7 @@ void conv_alloc(UNet &U, Conv &c, std::mt19937_64 &rng) {
   }
   c.w16.ensure(nw);
   k_to_bf16<<<gsz(nw), kT, 0, U.s>>>(nw, c.w.p, c.w16.p);
+  if (c.cin % 8 == 0 && c.cout % 8 == 0) c.wt16.ensure((size_t)c.cin * kp_of(c.cout));
 }
 
 void ensure_act(UNet &U, Tensor *t, int B) {
@@ -320,6 +368,24 @@ int bn_for(int n) { return n >= 256 ? 256 : n >= 128 ? 128 : n >= 64 ? 64 : 32; 
 
 void conv_forward(UNet &U, Conv &c, int B) {
   const int64_t P = (int64_t)B * c.H * c.W;
+  if (c.cin % 8 == 0 && c.cout % 8 == 0) {  // implicit GEMM: taps gathered from the NHWC input
+    GemmArgs g{};
+    g.M = (int)P;
+    g.N = c.cout;
+    g.K = c.kp;
+    g.B = c.w16.p;
+    g.ldb = c.kp;
+    g.D = c.out->y.p;
+    g.ldd = c.cout;
+    g.bias = c.b.p;
+    g.err = U.err.p;
+    g.convX = c.in->y.p;
+    g.conv_H = c.H;
+    g.conv_W = c.W;
+    g.conv_C = c.cin;
+    conv3x3_bf16(g, bn_for(c.cout), EPI_BIAS_RELU_BF16, U.s);
+    return;
+  }
   k_im2col<<<gsz(P * c.kp), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, c.in->y.p, U.col.p);
   AIRT_LAUNCH_CHECK();
   GemmArgs g{};
@@ -340,9 +406,50 @@ void conv_forward(UNet &U, Conv &c, int B) {
 
 void conv_backward(UNet &U, Conv &c, int B, bool need_dx) {
   const int64_t P = (int64_t)B * c.H * c.W;
-  const int64_t ny = P * c.cout;
-  k_relu_mask<<<gsz(ny), kT, 0, U.s>>>(ny, c.out->g.p, c.out->y.p, U.dym.p);
-  k_colsum<<<c.cout, kT, 0, U.s>>>(P, c.cout, U.dym.p, c.gb.p);
+  const int64_t ksplit = std::max<int64_t>(64, ((P / 64 + 63) / 64) * 64);  // ~64 K-splits
+  {
+    const int64_t blocks = std::min<int64_t>(1184, std::max<int64_t>(1, P / 64));
+    const int64_t rpb = (P + blocks - 1) / blocks;
+    k_relu_mask_colsum<<<(unsigned)((P + rpb - 1) / rpb), 256, 0, U.s>>>(
+        P, c.cout, rpb, c.out->g.p, c.out->y.p, U.dym.p, c.gb.p);
+    AIRT_LAUNCH_CHECK();
+  }
+  if (c.cin % 8 == 0 && c.cout % 8 == 0) {
+    GemmArgs gw{};
+    gw.M = c.kp;
+    gw.N = c.cout;
+    gw.K = (int)P;
+    gw.B = U.dym.p;
+    gw.ldb = c.cout;
+    gw.D = c.gw.p;
+    gw.ldd = c.kp;
+    gw.ksplit = (int)ksplit;
+    gw.err = U.err.p;
+    gw.convX = c.in->y.p;
+    gw.conv_H = c.H;
+    gw.conv_W = c.W;
+    gw.conv_C = c.cin;
+    conv3x3_wgrad_bf16(gw, bn_for(c.cout), U.s);
+    if (!need_dx) return;
+    const int kq = kp_of(c.cout);
+    k_flip_w<<<gsz((int64_t)c.cin * kq), kT, 0, U.s>>>(c.cout, c.cin, c.kp, kq, c.w16.p, c.wt16.p);
+    AIRT_LAUNCH_CHECK();
+    GemmArgs gd{};
+    gd.M = (int)P;
+    gd.N = c.cin;
+    gd.K = kq;
+    gd.B = c.wt16.p;
+    gd.ldb = kq;
+    gd.D = c.in->g.p;
+    gd.ldd = c.cin;
+    gd.err = U.err.p;
+    gd.convX = U.dym.p;
+    gd.conv_H = c.H;
+    gd.conv_W = c.W;
+    gd.conv_C = c.cout;
+    conv3x3_bf16(gd, bn_for(c.cin), EPI_ADD_F32, U.s);
+    return;
+  }
   k_im2col<<<gsz(P * c.kp), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, c.in->y.p, U.col.p);
   AIRT_LAUNCH_CHECK();
   // dW^T[Kp][Co] += col^T * dYm, stored transposed into gw[Co][Kp]
@@ -356,7 +463,7 @@ void conv_backward(UNet &U, Conv &c, int B, bool need_dx) {
   gw.ldb = c.cout;
   gw.D = c.gw.p;
   gw.ldd = c.kp;
-  gw.ksplit = (int)std::max<int64_t>(64, ((P / 64 + 63) / 64) * 64);  // ~64 K-splits
+  gw.ksplit = (int)ksplit;
   gw.err = U.err.p;
   gemm_bf16(gw, bn_for(c.cout), true, true, EPI_ATOMIC_F32_T, U.s);
   if (!need_dx) return;
@@ -450,14 +557,22 @@ UNet *unet_create(int H, int W, int base, int levels, int maxB, uint64_t seed) {
       AIRT_CHECK_CUDA(cudaMemsetAsync(d->p, 0, 4, U->s));
     }
     for (Tensor *t : U->tensors) ensure_act(*U, t, maxB);
-    size_t colmax = 0;
+    // col / dcol only for convolutions without the implicit path (Cin = 1);
+    // the first convolution never needs dX.
+    size_t colmax = 1, dcolmax = 1;
     int64_t dymax = 0;
-    for (const Conv &c : U->convs) {
-      colmax = std::max(colmax, (size_t)maxB * c.H * c.W * c.kp);
+    for (size_t i = 0; i < U->convs.size(); ++i) {
+      const Conv &c = U->convs[i];
+      const size_t ncol = (size_t)maxB * c.H * c.W * c.kp;
+      if (c.cin % 8 != 0 || c.cout % 8 != 0) {
+        colmax = std::max(colmax, ncol);
+        if (i > 0) dcolmax = std::max(dcolmax, ncol);
+      }
       dymax = std::max<int64_t>(dymax, (int64_t)maxB * c.H * c.W * c.cout);
     }
     U->col.ensure(colmax);
-    U->dcol.ensure(colmax);
+    U->dcol.ensure(dcolmax);
+    U->tgt.ensure((size_t)maxB * H * W);
     U->dym.ensure(dymax);
     U->out.ensure((size_t)maxB * H * W);
     U->loss.ensure(1);
@@ -488,20 +603,22 @@ cudaStream_t unet_stream(UNet &U) { return U.s; }
 // with NHWC pixel (b, h, w) = in[b][w*H + h] ... the map is a transpose, so
 // images are copied with h = row index of the column-major image.
 namespace {
-__global__ void k_img_in(int B, int H, int W, const float *__restrict__ in, __nv_bfloat16 *__restrict__ x) {
+template <typename TI>
+__global__ void k_img_in(int B, int H, int W, const TI *__restrict__ in, __nv_bfloat16 *__restrict__ x) {
   const int64_t total = (int64_t)B * H * W;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
-    x[t] = __float2bfloat16(in[(int64_t)b * H * W + (int64_t)w * H + h]);
+    x[t] = __float2bfloat16((float)in[(int64_t)b * H * W + (int64_t)w * H + h]);
   }
 }
-__global__ void k_img_out(int B, int H, int W, const float *__restrict__ o, float *__restrict__ out) {
+template <typename TO>
+__global__ void k_img_out(int B, int H, int W, const float *__restrict__ o, TO *__restrict__ out) {
   const int64_t total = (int64_t)B * H * W;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
-    out[(int64_t)b * H * W + (int64_t)w * H + h] = o[t];
+    out[(int64_t)b * H * W + (int64_t)w * H + h] = (TO)o[t];
   }
 }
 __global__ void k_img_tgt(int B, int H, int W, const float *__restrict__ in, float *__restrict__ o) {
@@ -514,10 +631,20 @@ __global__ void k_img_tgt(int B, int H, int W, const float *__restrict__ in, flo
 }
 }  // namespace
 
-void unet_forward(UNet &U, const float *d_in, int B) {
+void unet_forward_body(UNet &U, int B);
+
+template <typename TI>
+void unet_forward_t(UNet &U, const TI *d_in, int B) {
   AIRT_REQUIRE(B >= 1 && B <= U.maxB, "batch larger than the network was created for");
   const int64_t P0 = (int64_t)B * U.H * U.W;
-  k_img_in<<<gsz(P0), kT, 0, U.s>>>(B, U.H, U.W, d_in, U.xin->y.p);
+  k_img_in<TI><<<gsz(P0), kT, 0, U.s>>>(B, U.H, U.W, d_in, U.xin->y.p);
+  unet_forward_body(U, B);
+}
+
+void unet_forward(UNet &U, const float *d_in, int B) { unet_forward_t<float>(U, d_in, B); }
+
+void unet_forward_body(UNet &U, int B) {
+  const int64_t P0 = (int64_t)B * U.H * U.W;
   int ci = 0;
   for (int l = 0; l < U.levels; ++l) {
     if (l > 0) {
@@ -531,7 +658,7 @@ void unet_forward(UNet &U, const float *d_in, int B) {
   for (int l = U.levels - 2; l >= 0; --l) {
     Tensor *prev = (l == U.levels - 2) ? U.eb[U.levels - 1] : U.db[l + 1];
     Tensor *cat = U.cat[l];
-    k_up_concat<<<gsz((int64_t)B * cat->H * cat->W * cat->C), kT, 0, U.s>>>(
+    k_up_concat<<<gsz((int64_t)B * cat->H * cat->W * cat->C / 8), kT, 0, U.s>>>(
         B, cat->H, cat->W, prev->C, U.eb[l]->C, prev->y.p, U.eb[l]->y.p, cat->y.p);
     conv_forward(U, U.convs[ci++], B);
     conv_forward(U, U.convs[ci++], B);
@@ -540,8 +667,9 @@ void unet_forward(UNet &U, const float *d_in, int B) {
   AIRT_LAUNCH_CHECK();
 }
 
-void unet_output(UNet &U, float *d_out, int B) {
-  k_img_out<<<gsz((int64_t)B * U.H * U.W), kT, 0, U.s>>>(B, U.H, U.W, U.out.p, d_out);
+template <typename TO>
+void unet_output(UNet &U, TO *d_out, int B) {
+  k_img_out<TO><<<gsz((int64_t)B * U.H * U.W), kT, 0, U.s>>>(B, U.H, U.W, U.out.p, d_out);
   AIRT_LAUNCH_CHECK();
 }
 
@@ -559,7 +687,7 @@ float unet_gradients(UNet &U, const float *d_in, const float *d_tgt, int B) {
   AIRT_CHECK_CUDA(cudaMemsetAsync(U.loss.p, 0, 4, U.s));
   for (Tensor *t : U.tensors)
     AIRT_CHECK_CUDA(cudaMemsetAsync(t->g.p, 0, (size_t)B * t->H * t->W * t->C * 4, U.s));
-  float *tgt = U.dcol.p;  // target in NHWC order (dcol is free until the first conv backward)
+  float *tgt = U.tgt.p;
   k_img_tgt<<<gsz(P0), kT, 0, U.s>>>(B, U.H, U.W, d_tgt, tgt);
   k_head_back<<<gsz(P0), kT, 0, U.s>>>(P0, U.base, U.db[0]->y.p, U.hw.p, U.out.p, tgt,
                                         U.db[0]->g.p, U.hgw.p, U.hgb.p, U.loss.p);
@@ -725,6 +853,31 @@ int airt_unet_forward(airt_unet *h, const float *d_in, float *d_out, int B) {
   UNet &U = *reinterpret_cast<UNet *>(h);
   unet_forward(U, d_in, B);
   unet_output(U, d_out, B);
+  UNET_API_END
+}
+
+int airt_unet_forward_f64(airt_unet *h, const double *d_in, double *d_out, int B, void *cuda_stream) {
+  UNET_API_BEGIN
+  AIRT_REQUIRE(h && d_in && d_out, "null pointer argument");
+  UNet &U = *reinterpret_cast<UNet *>(h);
+  // order the network after work already queued on the caller's stream
+  cudaEvent_t ev = nullptr;
+  if (cuda_stream) {
+    AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    AIRT_CHECK_CUDA(cudaEventRecord(ev, static_cast<cudaStream_t>(cuda_stream)));
+    AIRT_CHECK_CUDA(cudaStreamWaitEvent(U.s, ev, 0));
+  }
+  for (int b0 = 0; b0 < B; b0 += U.maxB) {
+    const int nb = std::min(U.maxB, B - b0);
+    const int64_t off = (int64_t)b0 * U.H * U.W;
+    unet_forward_t<double>(U, d_in + off, nb);
+    unet_output<double>(U, d_out + off, nb);
+  }
+  if (cuda_stream) {
+    AIRT_CHECK_CUDA(cudaEventRecord(ev, U.s));
+    AIRT_CHECK_CUDA(cudaStreamWaitEvent(static_cast<cudaStream_t>(cuda_stream), ev, 0));
+    cudaEventDestroy(ev);
+  }
   UNET_API_END
 }
 

@@ -58,6 +58,12 @@ class UNet:
         """d_in, d_out: device float32 buffers of B images (x(:) order)."""
         check(lib().airt_unet_forward(self._h, C.c_void_p(d_in), C.c_void_p(d_out), int(B)))
 
+    def forward_f64(self, d_in, d_out, B: int, stream=0) -> None:
+        """d_in, d_out: device float64 buffers of B images, any B; ordered on
+        the CUDA stream `stream` (0: the network's own stream)."""
+        check(lib().airt_unet_forward_f64(self._h, C.c_void_p(d_in), C.c_void_p(d_out), int(B),
+                                          C.c_void_p(stream or None)))
+
     def gradients(self, d_in, d_tgt, B: int) -> float:
         loss = C.c_float()
         check(lib().airt_unet_gradients(self._h, C.c_void_p(d_in), C.c_void_p(d_tgt), int(B),

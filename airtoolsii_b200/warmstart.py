@@ -1,0 +1,216 @@
+"""Learned warm start for SIRT (no counterpart in the reference; it reaches
+the solvers only through their x0 argument, sirt/sirt.m:5).
+
+For one fixed paralleltomo geometry a U-Net maps the normalised
+back-projection of the data, u = D.*A'(M.*b) with the SART weights (one SART
+step from zero with relaxpar 1), to a starting point x0; cimmino then runs
+from x0 to the discrepancy-principle stop.  Training pairs come from
+seeded random-ellipse phantoms: the input u of the noisy sinogram and, as
+target, the DP-stopped cimmino solution that the GPU SIRT computes for it.
+Plain SIRT from zero stays the fallback, and the DP residual of SIRT judges
+every warm-started answer.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, lib
+from .batch import ParallelBatch
+from .solvers import cimmino, sart
+from .testprobs import parallel_operator, parallel_tables
+from .unet import UNet
+
+
+def ellipse_params(N_seeds, count=10):
+    """Per seed `count` ellipses (amp, a, b, x0, y0, cos phi, sin phi):
+    centres U[-0.6,0.6]^2, semi-axes U[0.05,0.4], rotation U[0,pi),
+    intensity U[0.1,1]."""
+    out = np.zeros((len(N_seeds), count, 7))
+    for k, s in enumerate(N_seeds):
+        rng = np.random.default_rng(int(s))
+        for e in range(count):
+            cx, cy = rng.uniform(-0.6, 0.6, 2)
+            a, b = rng.uniform(0.05, 0.4, 2)
+            phi = rng.uniform(0.0, math.pi)
+            amp = rng.uniform(0.1, 1.0)
+            out[k, e] = (amp, a, b, cx, cy, math.cos(phi), math.sin(phi))
+    return out
+
+
+class WarmStart:
+    """Warm-start pipeline for one paralleltomo geometry (N, theta, p).
+
+    Every stage runs on the GPU with device-resident data: phantoms
+    (airt_phantom_ellipses), sinograms (airt_apply_device plus seeded
+    Gaussian noise scaled to eta*||b||), the network input (one batched SART
+    step), the training targets (batched cimmino to the per-instance DP
+    stop), training (airt_unet_train_step) and inference
+    (airt_unet_forward_f64).  Batches of `chunk` instances share one
+    block-diagonal system."""
+
+    def __init__(self, N=256, theta=None, p=None, base=32, levels=4, method="cimmino",
+                 tau=1.02, max_batch=16, seed=0, chunk=64):
+        import torch
+        self.torch = torch
+        theta = np.arange(0.0, 180.0, 3.0) if theta is None else np.asarray(theta, float)
+        th, p, d, ct, st, off = parallel_tables(N, theta, p)
+        self.N, self.theta, self.p = N, th, p
+        self.n, self.m = N * N, p * len(th)
+        self.A = parallel_operator(N, ct, st, off)
+        self.method, self.tau, self.chunk = method, tau, chunk
+        r = C.c_double()
+        check(lib().airt_rho(self.A.handle, _lib.METHODS[method], None, None, 1e-7, 200, C.byref(r)))
+        self.rho = float(r.value)
+        self.net = UNet(N, N, base, levels, max_batch, seed)
+        self.max_batch = max_batch
+        self._batches = {}
+
+    def batch(self, K) -> ParallelBatch:
+        if K not in self._batches:
+            self._batches[K] = ParallelBatch([self.N] * K, [self.theta] * K, [self.p] * K)
+        return self._batches[K]
+
+    # ------------------------------------------------------------ data
+    def phantoms(self, seeds, count=10):
+        """Device FP64 tensor (len(seeds), n) of random-ellipse phantoms."""
+        torch = self.torch
+        prm = np.ascontiguousarray(ellipse_params(seeds, count).reshape(-1))
+        out = torch.empty((len(seeds), self.n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        check(lib().airt_phantom_ellipses(self.N, len(seeds), count, dptr(prm), 0.0, 1.0,
+                                          C.c_void_p(out.data_ptr()), None))
+        return out
+
+    def sinograms(self, X, eta, seed):
+        """b = A x + e with ||e|| = eta ||A x|| per row of X (device); returns
+        (device b, host delta = ||e||)."""
+        torch = self.torch
+        K = X.shape[0]
+        B0 = torch.empty((K, self.m), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        for k in range(K):
+            check(lib().airt_apply_device(self.A.handle, C.c_void_p(X[k].data_ptr()),
+                                          C.c_void_p(B0[k].data_ptr()), 0))
+        g = torch.Generator(device="cuda")
+        g.manual_seed(10_000_019 + int(seed))
+        E = torch.randn((K, self.m), generator=g, dtype=torch.float64, device="cuda")
+        scale = eta * torch.linalg.norm(B0, dim=1) / torch.linalg.norm(E, dim=1)
+        E *= scale[:, None]
+        return B0 + E, torch.linalg.norm(E, dim=1).cpu().numpy()
+
+    def net_input(self, d_b, d_u, K):
+        """u = D.*A'(M.*b), one SART step from zero with relaxpar 1 (device)."""
+        return self.batch(K).sirt_device("sart", d_b, d_u, 1, relaxpar=1.0)
+
+    def dp_solve(self, d_b, d_x, K, taudelta, d_x0=None, kmax=2000):
+        return self.batch(K).sirt_device(self.method, d_b, d_x, kmax, taudelta=taudelta,
+                                         rho=np.full(K, self.rho), d_x0=d_x0)
+
+    def prepare(self, seeds, eta=0.02):
+        """Device tensors u (network input), target (DP-stopped cimmino
+        solution), x (phantom) as FP32 (K, n); b (FP64 (K, m)); host
+        taudelta and DP iteration counts."""
+        torch = self.torch
+        K = len(seeds)
+        U = torch.empty((K, self.n), dtype=torch.float32, device="cuda")
+        T = torch.empty_like(U)
+        Xs = torch.empty_like(U)
+        Bs = torch.empty((K, self.m), dtype=torch.float64, device="cuda")
+        td = np.zeros(K)
+        its = np.zeros(K, np.int64)
+        for c0 in range(0, K, self.chunk):
+            sl = list(seeds[c0:c0 + self.chunk])
+            k = len(sl)
+            X = self.phantoms(sl)
+            b, delta = self.sinograms(X, eta, sl[0])
+            td[c0:c0 + k] = self.tau * delta
+            u = torch.empty((k, self.n), dtype=torch.float64, device="cuda")
+            x = torch.empty_like(u)
+            self.net_input(b.data_ptr(), u.data_ptr(), k)
+            info = self.dp_solve(b.data_ptr(), x.data_ptr(), k, td[c0:c0 + k])
+            U[c0:c0 + k] = u
+            T[c0:c0 + k] = x
+            Xs[c0:c0 + k] = X
+            Bs[c0:c0 + k] = b
+            its[c0:c0 + k] = info["finaliter"]
+        torch.cuda.synchronize()
+        return dict(u=U, target=T, x=Xs, b=Bs, taudelta=td, iters=its)
+
+    # ------------------------------------------------------------ training
+    def train(self, U, T, epochs=4, batch=16, lr=1e-3, log=None):
+        """Adam on (U, T) (device FP32 (K, n)), learning rate halved per epoch."""
+        torch = self.torch
+        K = U.shape[0]
+        rng = np.random.default_rng(0)
+        steps = max(1, K // batch)
+        hist = []
+        for ep in range(epochs):
+            perm = torch.from_numpy(rng.permutation(K)).cuda()
+            lr_e = lr * (0.5 ** ep)
+            tot = 0.0
+            for s in range(steps):
+                idx = perm[s * batch:(s + 1) * batch]
+                bu = U.index_select(0, idx).contiguous()
+                bt = T.index_select(0, idx).contiguous()
+                torch.cuda.current_stream().synchronize()
+                tot += self.net.train_step(bu.data_ptr(), bt.data_ptr(), idx.numel(), lr_e)
+            hist.append(tot / steps)
+            if log:
+                log(f"epoch {ep}: mse {hist[-1]:.3e}")
+        return hist
+
+    def predict(self, d_u, d_x0, K, stream=0):
+        """x0 = net(u) for K FP64 device images."""
+        self.net.forward_f64(d_u, d_x0, K, stream)
+
+    # ------------------------------------------------------------ comparison
+    def compare_batched(self, data, sel=None, kmax=2000):
+        """Time to the DP stop for the instances `sel` of `data`, solved as one
+        batch: plain cimmino from zero vs SART step + network + cimmino from
+        x0.  Both pipelines run from device-resident sinograms to
+        device-resident solutions; times are host wall times around each
+        whole pipeline (synchronised), plus the solvers' device times."""
+        torch = self.torch
+        sel = np.arange(data["b"].shape[0]) if sel is None else np.asarray(sel)
+        K = len(sel)
+        isel = torch.from_numpy(sel).cuda()
+        d_b = data["b"].index_select(0, isel).contiguous()
+        td = data["taudelta"][sel]
+        Bt = self.batch(K)
+        xp = torch.empty((K, self.n), dtype=torch.float64, device="cuda")
+        xw, u, x0 = torch.empty_like(xp), torch.empty_like(xp), torch.empty_like(xp)
+        rho = np.full(K, self.rho)
+        stream = Bt.stream_ptr()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ip = Bt.sirt_device(self.method, d_b.data_ptr(), xp.data_ptr(), kmax, taudelta=td,
+                            rho=rho)
+        torch.cuda.synchronize()
+        wall_plain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        iu = Bt.sirt_device("sart", d_b.data_ptr(), u.data_ptr(), 1, relaxpar=1.0)
+        tn = time.perf_counter()
+        self.predict(u.data_ptr(), x0.data_ptr(), K, stream)
+        iw = Bt.sirt_device(self.method, d_b.data_ptr(), xw.data_ptr(), kmax, taudelta=td,
+                            rho=rho, d_x0=x0.data_ptr())
+        torch.cuda.synchronize()
+        wall_warm = time.perf_counter() - t0
+        # the network alone, for the breakdown
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        self.predict(u.data_ptr(), x0.data_ptr(), K, stream)
+        torch.cuda.synchronize()
+        t_net = time.perf_counter() - t1
+        del tn
+        xt = data["x"].index_select(0, isel).double()
+        err = lambda xs: (torch.linalg.norm(xs - xt, dim=1)  # noqa: E731
+                          / torch.linalg.norm(xt, dim=1)).cpu().numpy()
+        return dict(K=K, plain_iters=ip["finaliter"], warm_iters=iw["finaliter"],
+                    plain_gpu_ms=ip["gpu_ms"], warm_gpu_ms=iu["gpu_ms"] + iw["gpu_ms"],
+                    net_wall_s=t_net, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
+                    plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0))

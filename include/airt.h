@@ -216,11 +216,24 @@ int airt_unet_get_params(airt_unet *h, float *host);
 int airt_unet_set_params(airt_unet *h, const float *host);
 int airt_unet_get_grads(airt_unet *h, float *host);
 int airt_unet_forward(airt_unet *h, const float *d_in, float *d_out, int B);
+/* Inference on FP64 solver vectors: B images of d_in (x(:) order) to d_out,
+ * any B (processed max_batch at a time), ordered after the work queued on
+ * cuda_stream (NULL: the network's own stream) and before later work on it. */
+int airt_unet_forward_f64(airt_unet *h, const double *d_in, double *d_out, int B,
+                          void *cuda_stream);
 /* MSE loss mean((net(in) - target)^2) and its gradient (airt_unet_get_grads). */
 int airt_unet_gradients(airt_unet *h, const float *d_in, const float *d_tgt, int B, float *loss);
 /* One Adam step (beta 0.9/0.999, eps 1e-8) on the batch; returns the loss. */
 int airt_unet_train_step(airt_unet *h, const float *d_in, const float *d_tgt, int B, float lr,
                          float *loss);
+
+/* Random-ellipse phantoms (training data of the warm start): nimg images of
+ * N x N, nell ellipses each given as 7 doubles (amplitude, semi-axes a and b,
+ * centre x0 and y0, cos and sin of the rotation) on the grid of
+ * testprobs/phantomgallery.m:188-190, summed and clipped to [lo, hi], written
+ * as FP64 x(:) images to device memory. */
+int airt_phantom_ellipses(int N, int nimg, int nell, const double *params, double lo, double hi,
+                          double *d_out, void *cuda_stream);
 
 /* ---- allocation-free residual ------------------------------------------------ */
 /* No counterpart in the reference.  r = b - A*x and ||r|| (into d_resnorm) for

@@ -17,11 +17,31 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
 
 
-@pytest.mark.parametrize("levels", [2, 3])
-def test_unet_gradients_vs_oracle(levels):
+def _set_gemm_path(path):
+    import ctypes as C
+    f = airt._lib.lib().airt_test_gemm_path
+    f.restype, f.argtypes = C.c_int, [C.c_int]
+    assert f(path) == 0
+
+
+@pytest.mark.parametrize("path", [0, 1], ids=["tma", "cpasync"])
+@pytest.mark.parametrize("levels,base", [(2, 8), (3, 8), (2, 32)])
+def test_unet_gradients_vs_oracle(levels, base, path):
+    """base 8: channel widths 8 (cp.async gathers), 16 and 32 (TMA, 32- and
+    64-byte swizzle); base 32: widths 32, 64 and 96 (64- and 128-byte
+    swizzle); 16x16 and 8x8 images exercise pixel boxes of one and two
+    images."""
+    _set_gemm_path(path)
+    try:
+        _check_gradients(levels, base)
+    finally:
+        _set_gemm_path(0)
+
+
+def _check_gradients(levels, base):
     import torch
     H = W = 16
-    base, B = 8, 2
+    B = 2
     net = airt.UNet(H, W, base, levels, max_batch=B, seed=7)
     rng = np.random.default_rng(levels)
     x = rng.random((B, H * W)).astype(np.float32)
