@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
   if (s_abort) {
     if (threadIdx.x == 0) atomicExch(g.err, 1);
   } else if (threadIdx.x < kProducers) {
-    gemm_epilogue<BN, EPI>(g, tmem, m0, n0, nk > 0);
+    gemm_epilogue<BN, EPI>(g, tmem + ((uint32_t)(warp * 32) << 16), m0 + warp * 32 + lane, n0, nk > 0);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -304,6 +304,10 @@ void conv3x3_bf16(const GemmArgs &g0, int bn, int epi, cudaStream_t s) {
 }
 
 void conv3x3_wgrad_bf16(const GemmArgs &g0, int bn, cudaStream_t s) {
+  if (g_gemm_path == 0 && conv3x3_wgrad_tma_ok(g0)) {
+    conv3x3_wgrad_bf16_tma(g0, bn, s);
+    return;
+  }
   GemmArgs g = g0;
   AIRT_REQUIRE(g.convX && g.conv_C % 8 == 0 && g.conv_C > 0, "conv3x3: channels must be a multiple of 8");
   AIRT_REQUIRE(((uintptr_t)g.convX & 15) == 0 && ((uintptr_t)g.B & 15) == 0 && g.ldb % 8 == 0,

@@ -1,29 +1,39 @@
-// tcgen05 GEMM with TMA operand loads (K-major A and B).
+// tcgen05 GEMM with TMA operand loads, persistent and warp-specialised.
 //
-// Two operand sources share one kernel:
-//  * MODE_DENSE: A [M][lda] and B [N][ldb] row-major bf16 matrices, 2D
-//    tensor maps, box {KS, 128} and {KS, BN};
+// Three operand sources share one kernel:
+//  * MODE_DENSE: A [M][lda] and B [N][ldb] row-major bf16 matrices
+//    (K-major), 2D tensor maps, boxes {64, 128} and {64, BN};
 //  * MODE_CONV: the implicit 3x3 convolution of an NHWC bf16 image X
-//    [B][H][W][C]: a 4D tensor map (C, W, H, B) whose box {KS, bw, bh, bb}
-//    (bw*bh*bb = 128 pixels, a rectangle of consecutive pixels) is loaded at
-//    the tile origin shifted by the tap (dw, dh); out-of-image coordinates
-//    read as zero, which is the convolution's zero padding.  Stage k is tap
+//    [B][H][W][C] (K-major): a 4D tensor map (C, W, H, B) whose box
+//    {KS, bw, bh, bb} (bw*bh*bb = 128 consecutive pixels) is loaded at the
+//    tile origin shifted by the tap (dw, dh); out-of-image coordinates read
+//    as zero, which is the convolution's zero padding.  Stage k is tap
 //    k / (C/KS), channels (k % (C/KS))*KS.. +KS; the weights W[N][ldb] carry
-//    the same K index (tap*C + ci).
+//    the same K index (tap*C + ci);
+//  * MODE_WGRAD: the weight gradient of that convolution, both operands
+//    MN-major: A^T[pixel][tap*C + ci] gathered as 64-pixel boxes of X
+//    shifted per tap (one box per 64/32/16 channels of the 128-row M tile),
+//    B = dY [pixel][N]; K runs over pixels, split across tiles, and the
+//    epilogue adds into gw[N][M] atomically.
 //
-// A stage holds KS = SW/2 K elements (SW = 128, 64 or 32 bytes per row) in
-// the canonical K-major swizzled UMMA layout that TMA writes with the
-// matching CU_TENSOR_MAP_SWIZZLE_*: rows of SW bytes, 8-row atoms of 8*SW
-// bytes (SBO), 16-byte chunks XOR-swizzled by row; each K=16 MMA step
-// advances the descriptor start address by 32 bytes.
+// Shared-memory tiles use the canonical swizzled UMMA layouts that TMA
+// writes with the matching CU_TENSOR_MAP_SWIZZLE_* (SW = 128, 64 or 32
+// bytes): K-major rows of SW bytes in 8-row atoms (SBO = 8*SW), each K=16
+// MMA step 32 bytes further; MN-major rows of SW bytes (SW/2 elements of M
+// or N) per K index, 8-row atoms along K (SBO = 8*SW), 64-row boxes per MN
+// group (LBO = 64*SW), each K=16 step 16 rows further.
 //
-// Roles (128 threads): thread 0 waits for a free stage and issues its two
-// TMA loads onto the stage's `full` mbarrier (expect-tx bytes); thread 32
-// waits for `full`, issues the tcgen05.mma instructions and commits them to
-// the stage's `empty` mbarrier, and after the last stage to `done`; then all
-// four warps drain TMEM through gemm_epilogue.  No multicast.
+// Roles (192 threads, persistent over tiles): warp 0 lane 0 streams the TMA
+// loads of every tile's K slices through an S-stage ring (`full` barriers
+// with expect-tx bytes, `empty` barriers released by tcgen05.commit); warp 1
+// lane 0 issues the tcgen05.mma instructions into one of two TMEM
+// accumulators and commits the tile to `acc_full`; warps 2-5 drain the other
+// accumulator meanwhile (warp w reads TMEM lanes 32*(w%4)..) and release it
+// through `acc_empty`.  All waits are bounded.  No multicast.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+
+#include <algorithm>
 
 #include "umma.cuh"
 
@@ -33,24 +43,39 @@ namespace {
 
 using namespace umma;
 
-enum { MODE_DENSE = 0, MODE_CONV = 1 };
+enum { MODE_DENSE = 0, MODE_CONV = 1, MODE_WGRAD = 2 };
 
-struct ConvGeo {
-  int W, H, cchunks;  // image width, height, C / KS
+struct TmaGeo {
+  int W, H;                      // image width and height (CONV, WGRAD)
+  int C;                         // channels of X (WGRAD)
+  int cchunks;                   // C / KS (CONV)
+  int tiles_m, tiles_n, splits;  // tile grid
+  int K, ksplit;                 // K extent and K range per split (DENSE, WGRAD)
 };
 
-constexpr uint32_t stage_bytes(int BN, int SW) {
-  return (((uint32_t)(BM + BN) * (uint32_t)SW) + 1023u) & ~1023u;
+constexpr uint32_t round1k(uint32_t b) { return (b + 1023u) & ~1023u; }
+
+// Stages: about 104 KB per CTA when two CTAs share an SM, about 200 KB
+// when one does; between 2 and 8.
+constexpr int ring_stages(uint32_t stage, bool two_per_sm) {
+  return (int)((two_per_sm ? 106496u : 204800u) / stage) > 8 ? 8
+         : (int)((two_per_sm ? 106496u : 204800u) / stage) < 2 ? 2
+                                                                : (int)((two_per_sm ? 106496u : 204800u) / stage);
 }
 
-// About 100 KB per CTA (two CTAs per SM), at least 2 and at most 8 stages;
-// stages above 40 KB take four stages and one CTA per SM.
-constexpr int tma_stages(int BN, int SW) {
-  return stage_bytes(BN, SW) > 40960u ? 4
-         : (int)(102400u / stage_bytes(BN, SW)) > 8 ? 8
-         : (int)(102400u / stage_bytes(BN, SW)) < 2 ? 2
-                                                     : (int)(102400u / stage_bytes(BN, SW));
-}
+template <int BN, int MODE, int SWA>
+struct TmaCfg {
+  static constexpr bool MN = MODE == MODE_WGRAD;
+  static constexpr int KS = MN ? 64 : SWA / 2;  // K elements per stage
+  static constexpr uint32_t A_BYTES = BM * KS * 2, B_BYTES = BN * KS * 2;
+  static constexpr uint32_t ST = round1k(A_BYTES + B_BYTES);
+  static constexpr bool TWO = BN <= 128;  // TMEM: two CTAs x two accumulators x BN columns
+  static constexpr int S = ring_stages(ST, TWO);
+  // the request never falls below 80 KB (two CTAs) or 120 KB (one CTA), so
+  // no third CTA lands on an SM and waits for TMEM columns
+  static constexpr size_t SMEM_RING = (size_t)S * ST + 1024;
+  static constexpr size_t SMEM = SMEM_RING > (TWO ? 81920u : 122880u) ? SMEM_RING : (TWO ? 81920u : 122880u);
+};
 
 __device__ __forceinline__ void expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -73,15 +98,15 @@ __device__ __forceinline__ void tma4d(uint32_t dst, const CUtensorMap *map, int 
       : "memory");
 }
 
-// K-major swizzled shared-memory descriptor: LBO unused (16 B), SBO = one
-// 8-row atom, layout type 2 / 4 / 6 for 128 / 64 / 32-byte swizzle.
+// Swizzled shared-memory descriptor: layout type 2 / 4 / 6 for 128 / 64 /
+// 32-byte swizzle; lbo / sbo in bytes.
 template <int SW>
-__device__ __forceinline__ uint64_t make_desc_sw(uint32_t saddr) {
+__device__ __forceinline__ uint64_t make_desc_sw(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   constexpr uint64_t layout = SW == 128 ? 2 : SW == 64 ? 4 : 6;
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(((8u * SW) >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
   d |= layout << 61;
   return d;
@@ -91,37 +116,59 @@ __device__ __forceinline__ void mbar_arrive_plain(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-template <int BN, int EPI, int MODE, int SW>
-__global__ void __launch_bounds__(128) k_gemm_tma(const __grid_constant__ CUtensorMap mapA,
-                                                  const __grid_constant__ CUtensorMap mapB, GemmArgs g,
-                                                  ConvGeo geo) {
-  constexpr int KS = SW / 2;
-  constexpr uint32_t A_BYTES = BM * SW, B_BYTES = BN * SW;
-  constexpr uint32_t ST_BYTES = stage_bytes(BN, SW);
-  constexpr int S = tma_stages(BN, SW);
+struct TileCoord {
+  int m0, n0, kb, nk;
+};
+
+template <int BN, int MODE, int SWA>
+__device__ __forceinline__ TileCoord tile_coord(const TmaGeo &geo, int t) {
+  using Cfg = TmaCfg<BN, MODE, SWA>;
+  const int mt = t % geo.tiles_m, r = t / geo.tiles_m;
+  const int nt = r % geo.tiles_n, z = r / geo.tiles_n;
+  TileCoord c;
+  c.m0 = mt * BM;
+  c.n0 = nt * BN;
+  if (MODE == MODE_CONV) {
+    c.kb = 0;
+    c.nk = 9 * geo.cchunks;
+  } else {
+    c.kb = z * geo.ksplit;
+    const int ke = min(geo.K, c.kb + geo.ksplit);
+    c.nk = ke > c.kb ? (ke - c.kb + Cfg::KS - 1) / Cfg::KS : 0;
+  }
+  return c;
+}
+
+// Pixel p -> box origin (w, h, image) in an H x W image batch.
+__device__ __forceinline__ void pixel_whb(int p, int W, int H, int &w, int &h, int &b) {
+  w = p % W;
+  const int q = p / W;
+  h = q % H;
+  b = q / H;
+}
+
+template <int BN, int EPI, int MODE, int SWA, int SWB>
+__global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUtensorMap mapA,
+                                                     const __grid_constant__ CUtensorMap mapB, GemmArgs g,
+                                                     TmaGeo geo) {
+  using Cfg = TmaCfg<BN, MODE, SWA>;
+  constexpr int S = Cfg::S, KS = Cfg::KS;
+  constexpr uint32_t A_BYTES = Cfg::A_BYTES, B_BYTES = Cfg::B_BYTES, ST = Cfg::ST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_addr(base);
-  __shared__ __align__(8) uint64_t full[S], empty[S], done;
+  __shared__ __align__(8) uint64_t full[S], empty[S], acc_full[2], acc_empty[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   volatile int *abort_flag = &s_abort;
 
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  int kb = 0, nk;
-  if (MODE == MODE_DENSE) {
-    kb = blockIdx.z * g.ksplit;
-    const int ke = min(g.K, kb + g.ksplit);
-    nk = ke > kb ? (ke - kb + KS - 1) / KS : 0;
-  } else {
-    nk = 9 * geo.cchunks;
-  }
-  const int warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntiles = geo.tiles_m * geo.tiles_n * geo.splits;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&s_tmem)),
-                 "r"((uint32_t)BN));
+                 "r"((uint32_t)(2 * BN)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (threadIdx.x == 0) {
@@ -130,7 +177,10 @@ __global__ void __launch_bounds__(128) k_gemm_tma(const __grid_constant__ CUtens
       mbar_init(smem_addr(&full[i]), 1);
       mbar_init(smem_addr(&empty[i]), 1);
     }
-    mbar_init(smem_addr(&done), 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(smem_addr(&acc_full[i]), 1);
+      mbar_init(smem_addr(&acc_empty[i]), 128);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&mapA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&mapB) : "memory");
@@ -140,68 +190,119 @@ __global__ void __launch_bounds__(128) k_gemm_tma(const __grid_constant__ CUtens
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
 
-  if (threadIdx.x == 0) {
-    // ---- TMA producer
-    int w0 = 0, h0 = 0, b0 = 0;
-    if (MODE == MODE_CONV) {
-      w0 = m0 % geo.W;
-      const int q = m0 / geo.W;
-      h0 = q % geo.H;
-      b0 = q / geo.H;
-    }
-    for (int k = 0; k < nk; ++k) {
-      const int st = k % S;
-      if (k >= S && !mbar_wait(smem_addr(&empty[st]), (uint32_t)((k / S - 1) & 1))) {
-        *abort_flag = 1;
-        break;
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer
+      uint32_t it = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        const TileCoord tc = tile_coord<BN, MODE, SWA>(geo, t);
+        int w0 = 0, h0 = 0, b0 = 0;
+        if (MODE == MODE_CONV) pixel_whb(tc.m0, geo.W, geo.H, w0, h0, b0);
+        for (int k = 0; k < tc.nk; ++k, ++it) {
+          const uint32_t st = it % S;
+          if (it >= (uint32_t)S && !mbar_wait(smem_addr(&empty[st]), ((it / S) - 1) & 1u)) {
+            *abort_flag = 1;
+            break;
+          }
+          const uint32_t sa = sbase + st * ST, sb = sa + A_BYTES;
+          const uint32_t bar = smem_addr(&full[st]);
+          expect_tx(bar, A_BYTES + B_BYTES);
+          if (MODE == MODE_DENSE) {
+            const int kx = tc.kb + k * KS;
+            tma2d(sa, &mapA, kx, tc.m0, bar);
+            tma2d(sb, &mapB, kx, tc.n0, bar);
+          } else if (MODE == MODE_CONV) {
+            const int tap = k / geo.cchunks, cc = k - tap * geo.cchunks;
+            tma4d(sa, &mapA, cc * KS, w0 + tap % 3 - 1, h0 + tap / 3 - 1, b0, bar);
+            tma2d(sb, &mapB, k * KS, tc.n0, bar);
+          } else {
+            constexpr int GA = SWA / 2, GB = SWB / 2;  // M / N elements per box
+            const int p0 = tc.kb + k * KS;
+            int pw, ph, pb;
+            pixel_whb(p0, geo.W, geo.H, pw, ph, pb);
+#pragma unroll
+            for (int j = 0; j < BM / GA; ++j) {
+              const int kk = tc.m0 + j * GA;
+              const int tap = kk / geo.C, ci = kk - tap * geo.C;
+              // taps past the ninth are the K padding: a box far outside the image reads zeros
+              const int dh = tap < 9 ? tap / 3 - 1 : -(1 << 20), dw = tap < 9 ? tap % 3 - 1 : 0;
+              tma4d(sa + j * (64 * SWA), &mapA, tap < 9 ? ci : 0, pw + dw, ph + dh, pb, bar);
+            }
+#pragma unroll
+            for (int j = 0; j < BN / GB; ++j) tma2d(sb + j * (64 * SWB), &mapB, tc.n0 + j * GB, p0, bar);
+          }
+        }
       }
-      const uint32_t sa = sbase + st * ST_BYTES, sb = sa + A_BYTES;
-      const uint32_t bar = smem_addr(&full[st]);
-      expect_tx(bar, A_BYTES + B_BYTES);
-      if (MODE == MODE_DENSE) {
-        const int kx = kb + k * KS;
-        tma2d(sa, &mapA, kx, m0, bar);
-        tma2d(sb, &mapB, kx, n0, bar);
-      } else {
-        const int tap = k / geo.cchunks, cc = k - tap * geo.cchunks;
-        tma4d(sa, &mapA, cc * KS, w0 + tap % 3 - 1, h0 + tap / 3 - 1, b0, bar);
-        tma2d(sb, &mapB, k * KS, n0, bar);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      constexpr bool MN = Cfg::MN;
+      constexpr uint32_t idesc = make_idesc<BN, MN, MN>();
+      uint32_t it = 0, tl = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++tl) {
+        const TileCoord tc = tile_coord<BN, MODE, SWA>(geo, t);
+        const uint32_t buf = tl & 1u;
+        if (tl >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((tl >> 1) - 1) & 1u)) {
+          *abort_flag = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t dtm = tmem + buf * BN;
+        bool ok = true;
+        for (int k = 0; k < tc.nk; ++k, ++it) {
+          const uint32_t st = it % S;
+          if (!mbar_wait(smem_addr(&full[st]), (it / S) & 1u)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sa = sbase + st * ST, sb = sa + A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < KS / 16; ++kk) {
+            uint64_t da, db;
+            if (MN) {
+              da = make_desc_sw<SWA>(sa + kk * 16 * SWA, 64 * SWA, 8 * SWA);
+              db = make_desc_sw<SWB>(sb + kk * 16 * SWB, 64 * SWB, 8 * SWB);
+            } else {
+              da = make_desc_sw<SWA>(sa + kk * 32, 16, 8 * SWA);
+              db = make_desc_sw<SWA>(sb + kk * 32, 16, 8 * SWA);
+            }
+            mma_bf16(dtm, da, db, idesc, (k > 0 || kk > 0) ? 1u : 0u);
+          }
+          commit(smem_addr(&empty[st]));
+        }
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+        if (tc.nk > 0) commit(smem_addr(&acc_full[buf]));
+        else mbar_arrive_plain(smem_addr(&acc_full[buf]));
       }
     }
-  } else if (threadIdx.x == 32) {
-    // ---- MMA issuer
-    constexpr uint32_t idesc = make_idesc<BN, false, false>();
-    int issued = 0;
-    for (int k = 0; k < nk; ++k) {
-      const int st = k % S;
-      if (!mbar_wait(smem_addr(&full[st]), (uint32_t)((k / S) & 1))) {
+  } else {
+    // ---- epilogue warps 2-5
+    const int quad = warp & 3;
+    uint32_t tl = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
+      const TileCoord tc = tile_coord<BN, MODE, SWA>(geo, t);
+      const uint32_t buf = tl & 1u;
+      if (!mbar_wait(smem_addr(&acc_full[buf]), (tl >> 1) & 1u)) {
         *abort_flag = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t sa = sbase + st * ST_BYTES, sb = sa + A_BYTES;
-#pragma unroll
-      for (int kk = 0; kk < KS / 16; ++kk)
-        mma_bf16(tmem, make_desc_sw<SW>(sa + kk * 32), make_desc_sw<SW>(sb + kk * 32), idesc,
-                 (k > 0 || kk > 0) ? 1u : 0u);
-      commit(smem_addr(&empty[st]));
-      ++issued;
+      gemm_epilogue<BN, EPI>(g, tmem + ((uint32_t)(quad * 32) << 16) + buf * BN, tc.m0 + quad * 32 + lane,
+                             tc.n0, tc.nk > 0);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive_plain(smem_addr(&acc_empty[buf]));
     }
-    if (issued > 0) commit(smem_addr(&done));
-    else mbar_arrive_plain(smem_addr(&done));
   }
-  if (!mbar_wait(smem_addr(&done), 0u)) *abort_flag = 1;
+  __syncthreads();
+  if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (s_abort) {
-    if (threadIdx.x == 0) atomicExch(g.err, 1);
-  } else {
-    gemm_epilogue<BN, EPI>(g, tmem, m0, n0, nk > 0);
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * BN)));
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -234,26 +335,43 @@ CUtensorMap make_map(const void *base, int rank, const cuuint64_t *dims, const c
   return m;
 }
 
-template <int BN, int EPI, int MODE, int SW>
-void launch_tma(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, ConvGeo geo, dim3 grid,
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    AIRT_CHECK_CUDA(cudaGetDevice(&dev));
+    AIRT_CHECK_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return n;
+}
+
+template <int BN, int MODE, int SWA>
+int persistent_ctas(int ntiles) {
+  using Cfg = TmaCfg<BN, MODE, SWA>;
+  return std::max(1, std::min(ntiles, sm_count() * (Cfg::TWO ? 2 : 1)));
+}
+
+template <int BN, int EPI, int MODE, int SWA, int SWB>
+void launch_tma(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, const TmaGeo &geo,
                 cudaStream_t s) {
-  const size_t smem = (size_t)tma_stages(BN, SW) * stage_bytes(BN, SW) + 1024;
-  auto kern = k_gemm_tma<BN, EPI, MODE, SW>;
-  AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<grid, 128, smem, s>>>(ma, mb, g, geo);
+  using Cfg = TmaCfg<BN, MODE, SWA>;
+  auto kern = k_gemm_tma<BN, EPI, MODE, SWA, SWB>;
+  AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
+  const int ntiles = geo.tiles_m * geo.tiles_n * geo.splits;
+  kern<<<persistent_ctas<BN, MODE, SWA>(ntiles), 192, Cfg::SMEM, s>>>(ma, mb, g, geo);
   AIRT_LAUNCH_CHECK();
 }
 
-template <int MODE, int SW>
-void dispatch_tma(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, ConvGeo geo, int bn,
-                  int epi, dim3 grid, cudaStream_t s) {
-#define AIRT_T(BNV)                                                                                        \
-  switch (epi) {                                                                                           \
-    case EPI_STORE_F32: launch_tma<BNV, EPI_STORE_F32, MODE, SW>(ma, mb, g, geo, grid, s); break;          \
-    case EPI_BIAS_RELU_BF16: launch_tma<BNV, EPI_BIAS_RELU_BF16, MODE, SW>(ma, mb, g, geo, grid, s); break; \
-    case EPI_BIAS_BF16: launch_tma<BNV, EPI_BIAS_BF16, MODE, SW>(ma, mb, g, geo, grid, s); break;          \
-    case EPI_ADD_F32: launch_tma<BNV, EPI_ADD_F32, MODE, SW>(ma, mb, g, geo, grid, s); break;              \
-    default: launch_tma<BNV, EPI_ATOMIC_F32_T, MODE, SW>(ma, mb, g, geo, grid, s); break;                  \
+template <int MODE, int SWA, int SWB>
+void dispatch_tma(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, const TmaGeo &geo, int bn,
+                  int epi, cudaStream_t s) {
+#define AIRT_T(BNV)                                                                                     \
+  switch (epi) {                                                                                        \
+    case EPI_STORE_F32: launch_tma<BNV, EPI_STORE_F32, MODE, SWA, SWB>(ma, mb, g, geo, s); break;       \
+    case EPI_BIAS_RELU_BF16: launch_tma<BNV, EPI_BIAS_RELU_BF16, MODE, SWA, SWB>(ma, mb, g, geo, s); break; \
+    case EPI_BIAS_BF16: launch_tma<BNV, EPI_BIAS_BF16, MODE, SWA, SWB>(ma, mb, g, geo, s); break;       \
+    case EPI_ADD_F32: launch_tma<BNV, EPI_ADD_F32, MODE, SWA, SWB>(ma, mb, g, geo, s); break;           \
+    default: launch_tma<BNV, EPI_ATOMIC_F32_T, MODE, SWA, SWB>(ma, mb, g, geo, s); break;               \
   }
   switch (bn) {
     case 32: AIRT_T(32) break;
@@ -264,6 +382,8 @@ void dispatch_tma(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &
   }
 #undef AIRT_T
 }
+
+int swizzle_for(int c) { return c % 64 == 0 ? 128 : c % 32 == 0 ? 64 : 32; }
 
 }  // namespace
 
@@ -281,23 +401,26 @@ void gemm_bf16_tma(const GemmArgs &g0, int bn, int epi, cudaStream_t s) {
   const cuuint32_t ba[2] = {64, (cuuint32_t)BM}, bb[2] = {64, (cuuint32_t)bn};
   const CUtensorMap ma = make_map(g.A, 2, da, sa, ba, 128);
   const CUtensorMap mb = make_map(g.B, 2, db, sb, bb, 128);
-  const int splits = (g.K + g.ksplit - 1) / g.ksplit;
-  const dim3 grid((g.M + BM - 1) / BM, (g.N + bn - 1) / bn, splits);
-  dispatch_tma<MODE_DENSE, 128>(ma, mb, g, ConvGeo{}, bn, epi, grid, s);
+  TmaGeo geo{};
+  geo.tiles_m = (g.M + BM - 1) / BM;
+  geo.tiles_n = (g.N + bn - 1) / bn;
+  geo.splits = (g.K + g.ksplit - 1) / g.ksplit;
+  geo.K = g.K;
+  geo.ksplit = g.ksplit;
+  dispatch_tma<MODE_DENSE, 128, 128>(ma, mb, g, geo, bn, epi, s);
 }
 
-// Pixel box of 128 consecutive NHWC pixels, or false when the image shape
-// does not tile that way.
-static bool conv_box(int Bimg, int H, int W, int &bw, int &bh, int &bb) {
-  (void)Bimg;
-  if (W >= 128) {
-    if (W % 128) return false;
-    bw = 128, bh = 1, bb = 1;
+// Box of `pix` consecutive NHWC pixels as a (bw, bh, bb) rectangle, or false
+// when the image shape does not tile that way.
+static bool pixel_box(int pix, int H, int W, int &bw, int &bh, int &bb) {
+  if (W >= pix) {
+    if (W % pix) return false;
+    bw = pix, bh = 1, bb = 1;
     return true;
   }
-  if (128 % W) return false;
+  if (pix % W) return false;
   bw = W;
-  const int rows = 128 / W;
+  const int rows = pix / W;
   if (rows <= H) {
     if (H % rows) return false;
     bh = rows, bb = 1;
@@ -311,17 +434,15 @@ static bool conv_box(int Bimg, int H, int W, int &bw, int &bh, int &bb) {
 bool conv3x3_tma_ok(const GemmArgs &g) {
   int bw, bh, bb;
   return g.conv_C % 16 == 0 && ((uintptr_t)g.convX & 15) == 0 && ((uintptr_t)g.B & 15) == 0 &&
-         g.ldb % 8 == 0 && g.M % (g.conv_H * g.conv_W) == 0 &&
-         conv_box(g.M / (g.conv_H * g.conv_W), g.conv_H, g.conv_W, bw, bh, bb);
+         g.ldb % 8 == 0 && g.M % (g.conv_H * g.conv_W) == 0 && pixel_box(128, g.conv_H, g.conv_W, bw, bh, bb);
 }
 
 void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   AIRT_REQUIRE(conv3x3_tma_ok(g), "conv3x3: shape unsuitable for TMA");
   const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
-  const int sw = C % 64 == 0 ? 128 : C % 32 == 0 ? 64 : 32;
-  const int ks = sw / 2;
+  const int sw = swizzle_for(C), ks = sw / 2;
   int bw, bh, bb;
-  conv_box(Bimg, H, W, bw, bh, bb);
+  pixel_box(128, H, W, bw, bh, bb);
   const cuuint64_t dx[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
   const cuuint64_t sx[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
   const cuuint32_t bx[4] = {(cuuint32_t)ks, (cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)bb};
@@ -329,11 +450,60 @@ void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const cuuint64_t dw[2] = {(cuuint64_t)9 * C, (cuuint64_t)g.N}, swt[1] = {(cuuint64_t)g.ldb * 2};
   const cuuint32_t bwt[2] = {(cuuint32_t)ks, (cuuint32_t)bn};
   const CUtensorMap mb = make_map(g.B, 2, dw, swt, bwt, sw);
-  const ConvGeo geo{W, H, C / ks};
-  const dim3 grid((g.M + BM - 1) / BM, (g.N + bn - 1) / bn, 1);
-  if (sw == 128) dispatch_tma<MODE_CONV, 128>(ma, mb, g, geo, bn, epi, grid, s);
-  else if (sw == 64) dispatch_tma<MODE_CONV, 64>(ma, mb, g, geo, bn, epi, grid, s);
-  else dispatch_tma<MODE_CONV, 32>(ma, mb, g, geo, bn, epi, grid, s);
+  TmaGeo geo{};
+  geo.W = W;
+  geo.H = H;
+  geo.C = C;
+  geo.cchunks = C / ks;
+  geo.tiles_m = (g.M + BM - 1) / BM;
+  geo.tiles_n = (g.N + bn - 1) / bn;
+  geo.splits = 1;
+  if (sw == 128) dispatch_tma<MODE_CONV, 128, 128>(ma, mb, g, geo, bn, epi, s);
+  else if (sw == 64) dispatch_tma<MODE_CONV, 64, 64>(ma, mb, g, geo, bn, epi, s);
+  else dispatch_tma<MODE_CONV, 32, 32>(ma, mb, g, geo, bn, epi, s);
+}
+
+bool conv3x3_wgrad_tma_ok(const GemmArgs &g) {
+  int bw, bh, bb;
+  return g.conv_C % 16 == 0 && g.N % 16 == 0 && ((uintptr_t)g.convX & 15) == 0 &&
+         ((uintptr_t)g.B & 15) == 0 && g.ldb == g.N && g.K % (g.conv_H * g.conv_W) == 0 &&
+         pixel_box(64, g.conv_H, g.conv_W, bw, bh, bb);
+}
+
+void conv3x3_wgrad_bf16_tma(const GemmArgs &g, int bn, cudaStream_t s) {
+  AIRT_REQUIRE(conv3x3_wgrad_tma_ok(g), "conv3x3: shape unsuitable for TMA");
+  const int C = g.conv_C, H = g.conv_H, W = g.conv_W, P = g.K, Bimg = P / (H * W);
+  const int swa = swizzle_for(C), swb = swizzle_for(g.N);
+  int bw, bh, bb;
+  pixel_box(64, H, W, bw, bh, bb);
+  const cuuint64_t dx[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
+  const cuuint64_t sx[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t bx[4] = {(cuuint32_t)(swa / 2), (cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)bb};
+  const CUtensorMap ma = make_map(g.convX, 4, dx, sx, bx, swa);
+  const cuuint64_t dy[2] = {(cuuint64_t)g.N, (cuuint64_t)P}, sy[1] = {(cuuint64_t)g.ldb * 2};
+  const cuuint32_t by[2] = {(cuuint32_t)(swb / 2), 64};
+  const CUtensorMap mb = make_map(g.B, 2, dy, sy, by, swb);
+  TmaGeo geo{};
+  geo.W = W;
+  geo.H = H;
+  geo.C = C;
+  geo.tiles_m = (g.M + BM - 1) / BM;
+  geo.tiles_n = (g.N + bn - 1) / bn;
+  // split the pixels so that about two tiles fall to each CTA
+  const int ctas = sm_count() * (bn <= 128 ? 2 : 1);
+  const int want = std::max(1, (2 * ctas + geo.tiles_m * geo.tiles_n - 1) / (geo.tiles_m * geo.tiles_n));
+  geo.ksplit = std::max(64, (((P + want - 1) / want) + 63) / 64 * 64);
+  geo.splits = (P + geo.ksplit - 1) / geo.ksplit;
+  geo.K = P;
+#define AIRT_W(SA, SB) dispatch_tma<MODE_WGRAD, SA, SB>(ma, mb, g, geo, bn, EPI_ATOMIC_F32_T, s)
+  if (swa == 128) {
+    if (swb == 128) AIRT_W(128, 128); else if (swb == 64) AIRT_W(128, 64); else AIRT_W(128, 32);
+  } else if (swa == 64) {
+    if (swb == 128) AIRT_W(64, 128); else if (swb == 64) AIRT_W(64, 64); else AIRT_W(64, 32);
+  } else {
+    if (swb == 128) AIRT_W(32, 128); else if (swb == 64) AIRT_W(32, 64); else AIRT_W(32, 32);
+  }
+#undef AIRT_W
 }
 
 }  // namespace airt

@@ -99,6 +99,23 @@ __device__ __forceinline__ void commit(uint32_t bar) {
                : "memory");
 }
 
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+      "[%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+        "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
   uint32_t r[8];
   asm volatile(
@@ -153,66 +170,81 @@ struct GemmArgs {
   int conv_H, conv_W, conv_C;
 };
 
-// Epilogue of a 128 x BN tile held in TMEM, run by warps 0-3 (warp w owns
-// TMEM lanes and tile rows 32w..32w+31).  have_acc = false: the tile's K
-// range was empty and the result is zero.
+// Epilogue of one 32-row slice of a 128 x BN tile held in TMEM, run by a
+// whole warp: lane i owns tile row `row` (TMEM lane (taddr >> 16) + i); taddr
+// carries the warp's lane quadrant and the accumulator's first column.
+// 32 columns are read per tcgen05.ld; full, aligned 32-column slices leave
+// as 16-byte vector accesses, the rest element by element.  have_acc =
+// false: the tile's K range was empty and the result is zero.
 template <int BN, int EPI>
-__device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, uint32_t tmem, int m0, int n0,
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, uint32_t taddr, int row, int n0,
                                               bool have_acc) {
   using namespace umma;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = m0 + warp * 32 + lane;
-  // 16-byte row stores when the 8 columns are in range and aligned
+  static_assert(BN % 32 == 0, "BN must be a multiple of 32");
   const bool vec_ok = (g.ldd & 7) == 0 && ((uintptr_t)g.D & 15) == 0 &&
                       (g.bias == nullptr || ((uintptr_t)g.bias & 15) == 0);
 #pragma unroll 1
-  for (int c = 0; c < BN; c += 8) {
-    float v[8];
+  for (int c = 0; c < BN; c += 32) {
+    float v[32];
     if (have_acc) {
-      tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      tmem_ld32(taddr + (uint32_t)c, v);
     } else {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = 0.f;
+      for (int i = 0; i < 32; ++i) v[i] = 0.f;
     }
-    if (EPI != EPI_ATOMIC_F32_T && vec_ok && row < g.M && n0 + c + 8 <= g.N) {
-      const int col = n0 + c;
+    const int col0 = n0 + c;
+    if (EPI != EPI_ATOMIC_F32_T && vec_ok && row < g.M && col0 + 32 <= g.N) {
       if (EPI == EPI_STORE_F32 || EPI == EPI_ADD_F32) {
-        float4 *d = reinterpret_cast<float4 *>((float *)g.D + (size_t)row * g.ldd + col);
-        float4 a = make_float4(v[0], v[1], v[2], v[3]), b = make_float4(v[4], v[5], v[6], v[7]);
+        float4 *d = reinterpret_cast<float4 *>((float *)g.D + (size_t)row * g.ldd + col0);
         if (EPI == EPI_ADD_F32) {
-          const float4 a0 = d[0], b0 = d[1];
-          a.x += a0.x; a.y += a0.y; a.z += a0.z; a.w += a0.w;
-          b.x += b0.x; b.y += b0.y; b.z += b0.z; b.w += b0.w;
+          float4 o[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) o[j] = d[j];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            v[4 * j] += o[j].x;
+            v[4 * j + 1] += o[j].y;
+            v[4 * j + 2] += o[j].z;
+            v[4 * j + 3] += o[j].w;
+          }
         }
-        d[0] = a;
-        d[1] = b;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
       } else {
         if (g.bias) {
-          const float4 b0 = __ldg(reinterpret_cast<const float4 *>(g.bias + col));
-          const float4 b1 = __ldg(reinterpret_cast<const float4 *>(g.bias + col) + 1);
-          v[0] += b0.x; v[1] += b0.y; v[2] += b0.z; v[3] += b0.w;
-          v[4] += b1.x; v[5] += b1.y; v[6] += b1.z; v[7] += b1.w;
-        }
-        uint4 pk;
-        uint32_t *pw = reinterpret_cast<uint32_t *>(&pk);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          float lo = v[2 * i], hi = v[2 * i + 1];
-          if (EPI == EPI_BIAS_RELU_BF16) {
-            lo = fmaxf(lo, 0.f);
-            hi = fmaxf(hi, 0.f);
+          for (int j = 0; j < 8; ++j) {
+            const float4 b = __ldg(reinterpret_cast<const float4 *>(g.bias + col0) + j);
+            v[4 * j] += b.x;
+            v[4 * j + 1] += b.y;
+            v[4 * j + 2] += b.z;
+            v[4 * j + 3] += b.w;
           }
-          const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
-          pw[i] = *reinterpret_cast<const uint32_t *>(&h2);
         }
-        *reinterpret_cast<uint4 *>((__nv_bfloat16 *)g.D + (size_t)row * g.ldd + col) = pk;
+        uint4 *d = reinterpret_cast<uint4 *>((__nv_bfloat16 *)g.D + (size_t)row * g.ldd + col0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          uint4 pk;
+          uint32_t *pw = reinterpret_cast<uint32_t *>(&pk);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            float lo = v[8 * q + 2 * i], hi = v[8 * q + 2 * i + 1];
+            if (EPI == EPI_BIAS_RELU_BF16) {
+              lo = fmaxf(lo, 0.f);
+              hi = fmaxf(hi, 0.f);
+            }
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
+            pw[i] = *reinterpret_cast<const uint32_t *>(&h2);
+          }
+          d[q] = pk;
+        }
       }
       continue;
     }
     if (row < g.M) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int col = n0 + c + i;
+      for (int i = 0; i < 32; ++i) {
+        const int col = col0 + i;
         if (col >= g.N) continue;
         float y = v[i];
         if (EPI == EPI_STORE_F32) {
@@ -246,6 +278,8 @@ bool gemm_tma_ok(const GemmArgs &g);
 void gemm_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s);
 bool conv3x3_tma_ok(const GemmArgs &g);
 void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s);
+bool conv3x3_wgrad_tma_ok(const GemmArgs &g);
+void conv3x3_wgrad_bf16_tma(const GemmArgs &g, int bn, cudaStream_t s);
 // Operand path: 0 = TMA where possible, 1 = always cp.async (a test switch).
 extern int g_gemm_path;
 

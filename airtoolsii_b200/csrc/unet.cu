@@ -34,6 +34,51 @@ namespace {
 
 constexpr int kT = 256;
 
+__device__ __forceinline__ void bf8_to_f(const uint4 &u, float (&f)[8]) {
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float2 t = __bfloat1622float2(h[i]);
+    f[2 * i] = t.x;
+    f[2 * i + 1] = t.y;
+  }
+}
+
+__device__ __forceinline__ uint4 f_to_bf8(const float (&f)[8]) {
+  uint4 u;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+  return u;
+}
+
+__device__ __forceinline__ void ld_f8(const float *p, float (&f)[8]) {
+  const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+  f[0] = a.x, f[1] = a.y, f[2] = a.z, f[3] = a.w, f[4] = b.x, f[5] = b.y, f[6] = b.z, f[7] = b.w;
+}
+
+__device__ __forceinline__ void st_f8(float *p, const float (&f)[8]) {
+  reinterpret_cast<float4 *>(p)[0] = make_float4(f[0], f[1], f[2], f[3]);
+  reinterpret_cast<float4 *>(p)[1] = make_float4(f[4], f[5], f[6], f[7]);
+}
+
+// Per-channel sums over rows.  A 256-thread block walks its rows with
+// thread t owning row offset t / C8 and channel group t % C8 (R = 256 / C8
+// rows per pass, threads t >= R*C8 idle); the per-thread sums of 8 channels
+// meet in shared memory and leave as one atomicAdd per channel.
+__device__ __forceinline__ void colsum_flush(const float (&acc)[8], int C8, float *sh, float *out) {
+  const int t = threadIdx.x, R = 256 / C8;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) sh[i * 256 + t] = acc[i];
+  __syncthreads();
+  for (int c = t; c < C8 * 8; c += 256) {
+    const int cg = c >> 3, i = c & 7;
+    float a = 0.f;
+    for (int r = 0; r < R; ++r) a += sh[i * 256 + r * C8 + cg];
+    atomicAdd(out + c, a);
+  }
+}
+
 __global__ void k_im2col(int B, int H, int W, int C, int Kp, const __nv_bfloat16 *__restrict__ X,
                          __nv_bfloat16 *__restrict__ col) {
   const int64_t total = (int64_t)B * H * W * Kp;
@@ -87,92 +132,105 @@ __global__ void k_col2im(int B, int H, int W, int C, int Kp, const float *__rest
 }
 
 // dYm = bf16(dY * (Y > 0)) and db += column sums (one block per 256 columns-slab)
-// dYm = bf16(dY * (Y > 0)) and db[c] += sum over pixels of dYm[p][c].
-// Each block owns a contiguous range of pixel rows; with C < 256 a pass
-// covers 256 / C rows (thread t: row t / C, column t % C), with C >= 256
-// each thread walks columns t, t + 256, ...  Per-thread sums meet in shared
-// memory and leave the block as one atomicAdd per column.
+// dYm = bf16(dY * (Y > 0)) and db[c] += sum over pixels of dYm[p][c], 8
+// channels per thread (C a multiple of 8); each block owns a contiguous range
+// of pixel rows.
 __global__ void __launch_bounds__(256) k_relu_mask_colsum(int64_t P, int C, int64_t rows_per_block,
                                                           const float *__restrict__ dY,
                                                           const __nv_bfloat16 *__restrict__ Y,
                                                           __nv_bfloat16 *__restrict__ dYm,
                                                           float *__restrict__ db) {
-  __shared__ float sh[256];
-  const int t = threadIdx.x;
+  __shared__ float sh[8 * 256];
+  const int C8 = C / 8, R = 256 / C8, t = threadIdx.x;
   const int64_t r0 = blockIdx.x * rows_per_block;
   const int64_t r1 = min(P, r0 + rows_per_block);
-  if (C < 256) {
-    const int R = 256 / C;
-    float acc = 0.f;
-    if (t < R * C) {
-      const int c = t % C;
-      for (int64_t r = r0 + t / C; r < r1; r += R) {
-        const int64_t i = r * C + c;
-        const __nv_bfloat16 m = __float2bfloat16(__bfloat162float(Y[i]) > 0.f ? dY[i] : 0.f);
-        dYm[i] = m;
-        acc += __bfloat162float(m);
-      }
-    }
-    sh[t] = acc;
-    __syncthreads();
-    if (t < C) {
-      float a = 0.f;
-      for (int k = 0; k < R; ++k) a += sh[t + k * C];
-      atomicAdd(db + t, a);
-    }
-  } else {
-    for (int c = t; c < C; c += 256) {
-      float acc = 0.f;
-      for (int64_t r = r0; r < r1; ++r) {
-        const int64_t i = r * C + c;
-        const __nv_bfloat16 m = __float2bfloat16(__bfloat162float(Y[i]) > 0.f ? dY[i] : 0.f);
-        dYm[i] = m;
-        acc += __bfloat162float(m);
-      }
-      atomicAdd(db + c, acc);
+  float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (t < R * C8) {
+    const int cg = t % C8;
+    for (int64_t r = r0 + t / C8; r < r1; r += R) {
+      const int64_t i = r * C + cg * 8;
+      float d[8], y[8], m[8];
+      ld_f8(dY + i, d);
+      bf8_to_f(*reinterpret_cast<const uint4 *>(Y + i), y);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) m[j] = y[j] > 0.f ? d[j] : 0.f;
+      const uint4 u = f_to_bf8(m);
+      *reinterpret_cast<uint4 *>(dYm + i) = u;
+      bf8_to_f(u, m);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] += m[j];
     }
   }
+  colsum_flush(acc, C8, sh, db);
 }
 
+// 2x2 max pool, 8 channels (16 bytes) per thread.
 __global__ void k_pool(int B, int H, int W, int C, const __nv_bfloat16 *__restrict__ X,
                        __nv_bfloat16 *__restrict__ Y) {
-  const int Ho = H / 2, Wo = W / 2;
-  const int64_t total = (int64_t)B * Ho * Wo * C;
+  const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
+  const int64_t total = (int64_t)B * Ho * Wo * C8;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t % C);
-    const int64_t q = t / C;
+    const int cg = (int)(t % C8);
+    const int64_t q = t / C8;
     const int w = (int)(q % Wo), h = (int)((q / Wo) % Ho), b = (int)(q / ((int64_t)Wo * Ho));
-    float m = -INFINITY;
+    float m[8], v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) m[j] = -INFINITY;
+#pragma unroll
     for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j)
-        m = fmaxf(m, __bfloat162float(X[(((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + c]));
-    Y[t] = __float2bfloat16(m);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        bf8_to_f(*reinterpret_cast<const uint4 *>(X + (((int64_t)b * H + 2 * h + i) * W + 2 * w + k) * C + cg * 8), v);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) m[j] = fmaxf(m[j], v[j]);
+      }
+    reinterpret_cast<uint4 *>(Y)[t] = f_to_bf8(m);
   }
 }
 
-// gradient of the max pool goes to the first maximal element of each window
+// Gradient of the max pool: each window's gradient goes to its first maximal
+// element (row-major window order); 8 channels per thread, every element of
+// dX belongs to exactly one window.
 __global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__restrict__ X,
                             const float *__restrict__ dY, float *__restrict__ dX) {
-  const int Ho = H / 2, Wo = W / 2;
-  const int64_t total = (int64_t)B * Ho * Wo * C;
+  const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
+  const int64_t total = (int64_t)B * Ho * Wo * C8;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t % C);
-    const int64_t q = t / C;
+    const int cg = (int)(t % C8);
+    const int64_t q = t / C8;
     const int w = (int)(q % Wo), h = (int)((q / Wo) % Ho), b = (int)(q / ((int64_t)Wo * Ho));
-    float m = -INFINITY;
-    int bi = 0, bj = 0;
-    for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j) {
-        const float v = __bfloat162float(X[(((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + c]);
-        if (v > m) {
-          m = v;
-          bi = i;
-          bj = j;
+    int64_t off[4];
+    float x[4][8], m[8], g[8];
+    int arg[8];
+#pragma unroll
+    for (int pos = 0; pos < 4; ++pos) {
+      off[pos] = (((int64_t)b * H + 2 * h + pos / 2) * W + 2 * w + pos % 2) * C + cg * 8;
+      bf8_to_f(*reinterpret_cast<const uint4 *>(X + off[pos]), x[pos]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      m[j] = -INFINITY;
+      arg[j] = 0;
+    }
+#pragma unroll
+    for (int pos = 0; pos < 4; ++pos)
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (x[pos][j] > m[j]) {
+          m[j] = x[pos][j];
+          arg[j] = pos;
         }
-      }
-    dX[(((int64_t)b * H + 2 * h + bi) * W + 2 * w + bj) * C + c] += dY[t];
+    ld_f8(dY + q * C + cg * 8, g);
+#pragma unroll
+    for (int pos = 0; pos < 4; ++pos) {
+      float d[8];
+      ld_f8(dX + off[pos], d);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) d[j] += arg[j] == pos ? g[j] : 0.f;
+      st_f8(dX + off[pos], d);
+    }
   }
 }
 
@@ -198,75 +256,165 @@ __global__ void k_up_concat(int B, int H, int W, int C1, int C2, const __nv_bflo
   }
 }
 
+// Backward of [nearest-2x(prev) | skip]: dskip += its channels of dcat,
+// dprev += the sum of the four children; 4 channels (16 bytes) per thread.
 __global__ void k_up_concat_back(int B, int H, int W, int C1, int C2, const float *__restrict__ dcat,
                                  float *__restrict__ dprev, float *__restrict__ dskip) {
-  const int C = C1 + C2;
-  // dskip: direct
-  const int64_t totS = (int64_t)B * H * W * C2;
+  const int C = C1 + C2, C24 = C2 / 4, C14 = C1 / 4;
+  const int64_t totS = (int64_t)B * H * W * C24;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < totS;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t % C2);
-    const int64_t p = t / C2;
-    dskip[t] += dcat[p * C + C1 + c];
+    const int c4 = (int)(t % C24);
+    const int64_t p = t / C24;
+    const float4 g = *reinterpret_cast<const float4 *>(dcat + p * C + C1 + 4 * c4);
+    float4 &d = reinterpret_cast<float4 *>(dskip)[t];
+    float4 v = d;
+    v.x += g.x, v.y += g.y, v.z += g.z, v.w += g.w;
+    d = v;
   }
-  // dprev: sum of the 4 children
   const int Hh = H / 2, Wh = W / 2;
-  const int64_t totP = (int64_t)B * Hh * Wh * C1;
+  const int64_t totP = (int64_t)B * Hh * Wh * C14;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < totP;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t % C1);
-    const int64_t q = t / C1;
+    const int c4 = (int)(t % C14);
+    const int64_t q = t / C14;
     const int w = (int)(q % Wh), h = (int)((q / Wh) % Hh), b = (int)(q / ((int64_t)Wh * Hh));
-    float a = 0.f;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
     for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j) a += dcat[(((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + c];
-    dprev[t] += a;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const float4 g = *reinterpret_cast<const float4 *>(
+            dcat + (((int64_t)b * H + 2 * h + i) * W + 2 * w + j) * C + 4 * c4);
+        a.x += g.x, a.y += g.y, a.z += g.z, a.w += g.w;
+      }
+    float4 &d = reinterpret_cast<float4 *>(dprev)[t];
+    float4 v = d;
+    v.x += a.x, v.y += a.y, v.z += a.z, v.w += a.w;
+    d = v;
   }
 }
 
-// head: out[p] = sum_c w[c]*Y[p][c] + b ; column-major image <-> NHWC
+// head: out[p] = b + sum_c w[c]*Y[p][c] (channels in order), one pixel per
+// thread, 8 channels per 16-byte load.
 __global__ void k_head(int64_t P, int C, const __nv_bfloat16 *__restrict__ Y, const float *__restrict__ w,
                        const float *__restrict__ b, float *__restrict__ out) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
        p += (int64_t)gridDim.x * blockDim.x) {
     float a = b[0];
-    for (int c = 0; c < C; ++c) a += w[c] * __bfloat162float(Y[p * C + c]);
+    for (int cg = 0; cg < C / 8; ++cg) {
+      float y[8];
+      bf8_to_f(*reinterpret_cast<const uint4 *>(Y + p * C + cg * 8), y);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) a += w[cg * 8 + j] * y[j];
+    }
     out[p] = a;
   }
 }
 
-// loss = mean((out - t)^2); dout = 2 (out - t) / P; dY = dout * w; gw, gb
-__global__ void k_head_back(int64_t P, int C, const __nv_bfloat16 *__restrict__ Y, const float *__restrict__ w,
-                            const float *__restrict__ out, const float *__restrict__ tgt,
-                            float *__restrict__ dY, float *__restrict__ gw, float *__restrict__ gb,
-                            float *__restrict__ loss) {
+// loss += mean((out - t)^2); dout = 2 (out - t) / P; dY = dout * w;
+// gw[c] += sum_p dout[p] Y[p][c]; gb += sum_p dout[p].  Rows and channel
+// groups as in k_relu_mask_colsum.
+__global__ void __launch_bounds__(256) k_head_back(int64_t P, int C, int64_t rows_per_block,
+                                                   const __nv_bfloat16 *__restrict__ Y,
+                                                   const float *__restrict__ w, const float *__restrict__ out,
+                                                   const float *__restrict__ tgt, float *__restrict__ dY,
+                                                   float *__restrict__ gw, float *__restrict__ gb,
+                                                   float *__restrict__ loss) {
+  __shared__ float sh[8 * 256];
+  const int C8 = C / 8, R = 256 / C8, t = threadIdx.x;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(P, r0 + rows_per_block);
+  float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float lsum = 0.f, bsum = 0.f;
-  float wsum[64];
-  for (int c = 0; c < C && c < 64; ++c) wsum[c] = 0.f;
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    const float d = out[p] - tgt[p];
-    lsum += d * d;
-    const float g = 2.f * d / (float)P;
-    bsum += g;
-    for (int c = 0; c < C; ++c) {
-      dY[p * C + c] = g * w[c];
-      if (c < 64) wsum[c] += g * __bfloat162float(Y[p * C + c]);
+  if (t < R * C8) {
+    const int cg = t % C8;
+    float wc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) wc[j] = w[cg * 8 + j];
+    for (int64_t r = r0 + t / C8; r < r1; r += R) {
+      const float d = out[r] - tgt[r];
+      const float g = 2.f * d / (float)P;
+      if (cg == 0) {
+        lsum += d * d;
+        bsum += g;
+      }
+      float y[8], o[8];
+      bf8_to_f(*reinterpret_cast<const uint4 *>(Y + r * C + cg * 8), y);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        o[j] = g * wc[j];
+        acc[j] += g * y[j];
+      }
+      st_f8(dY + r * C + cg * 8, o);
     }
   }
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
     bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
   }
-  if ((threadIdx.x & 31) == 0) {
+  if ((t & 31) == 0) {
     atomicAdd(loss, lsum / (float)P);
     atomicAdd(gb, bsum);
   }
-  for (int c = 0; c < C && c < 64; ++c) {
-    float v = wsum[c];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(gw + c, v);
+  colsum_flush(acc, C8, sh, gw);
+}
+
+// First convolution (one input channel): y[p][co] = relu(b[co] +
+// sum_tap w[co][tap] * x[p + tap]), FP32 sums of the BF16 products, 8
+// output channels per thread.
+__global__ void k_conv1_fwd(int64_t P, int H, int W, int Co, int Kp, const __nv_bfloat16 *__restrict__ x,
+                            const __nv_bfloat16 *__restrict__ wt, const float *__restrict__ bias,
+                            __nv_bfloat16 *__restrict__ y) {
+  const int C8 = Co / 8;
+  const int64_t total = P * C8;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int og = (int)(t % C8);
+    const int64_t p = t / C8;
+    const int w = (int)(p % W), h = (int)((p / W) % H);
+    float xv[9];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+      const bool in = h + dh >= 0 && h + dh < H && w + dw >= 0 && w + dw < W;
+      xv[tap] = in ? __bfloat162float(x[p + (int64_t)dh * W + dw]) : 0.f;
+    }
+    float o[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int co = og * 8 + j;
+      float a = 0.f;
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap) a += __bfloat162float(wt[(int64_t)co * Kp + tap]) * xv[tap];
+      o[j] = fmaxf(a + bias[co], 0.f);
+    }
+    reinterpret_cast<uint4 *>(y)[t] = f_to_bf8(o);
   }
+}
+
+// Weight gradient of the first convolution: gw[co][tap] += sum_p dYm[p][co]
+// * x[p + tap].  Block = 9 warps (one per tap), lane -> output channels
+// lane, lane + 32 (Co <= 64); each block owns a contiguous pixel range.
+__global__ void __launch_bounds__(288) k_conv1_wgrad(int64_t P, int H, int W, int Co, int Kp,
+                                                     int64_t rows_per_block, const __nv_bfloat16 *__restrict__ x,
+                                                     const __nv_bfloat16 *__restrict__ dYm,
+                                                     float *__restrict__ gw) {
+  const int tap = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(P, r0 + rows_per_block);
+  float a0 = 0.f, a1 = 0.f;
+  for (int64_t p = r0; p < r1; ++p) {
+    const int w = (int)(p % W), h = (int)((p / W) % H);
+    if (h + dh < 0 || h + dh >= H || w + dw < 0 || w + dw >= W) continue;
+    const float xv = __bfloat162float(x[p + (int64_t)dh * W + dw]);
+    if (lane < Co) a0 += __bfloat162float(dYm[p * Co + lane]) * xv;
+    if (lane + 32 < Co) a1 += __bfloat162float(dYm[p * Co + lane + 32]) * xv;
+  }
+  if (lane < Co) atomicAdd(gw + (int64_t)lane * Kp + tap, a0);
+  if (lane + 32 < Co) atomicAdd(gw + (int64_t)(lane + 32) * Kp + tap, a1);
 }
 
 __global__ void k_to_bf16(int64_t n, const float *__restrict__ a, __nv_bfloat16 *__restrict__ b) {
@@ -366,8 +514,22 @@ void ensure_act(UNet &U, Tensor *t, int B) {
 
 int bn_for(int n) { return n >= 256 ? 256 : n >= 128 ? 128 : n >= 64 ? 64 : 32; }
 
+// Blocks of contiguous pixel rows for the row-reduction kernels: about 8
+// per SM, at least 64 rows each.
+void row_blocks(int64_t P, int64_t &blocks, int64_t &rpb) {
+  blocks = std::min<int64_t>(1184, std::max<int64_t>(1, P / 64));
+  rpb = (P + blocks - 1) / blocks;
+  blocks = (P + rpb - 1) / rpb;
+}
+
 void conv_forward(UNet &U, Conv &c, int B) {
   const int64_t P = (int64_t)B * c.H * c.W;
+  if (c.cin == 1 && c.cout % 8 == 0) {  // first convolution: direct kernel
+    k_conv1_fwd<<<gsz(P * c.cout / 8), kT, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, c.in->y.p, c.w16.p, c.b.p,
+                                                     c.out->y.p);
+    AIRT_LAUNCH_CHECK();
+    return;
+  }
   if (c.cin % 8 == 0 && c.cout % 8 == 0) {  // implicit GEMM: taps gathered from the NHWC input
     GemmArgs g{};
     g.M = (int)P;
@@ -386,6 +548,7 @@ void conv_forward(UNet &U, Conv &c, int B) {
     conv3x3_bf16(g, bn_for(c.cout), EPI_BIAS_RELU_BF16, U.s);
     return;
   }
+  AIRT_REQUIRE(U.col.n >= (size_t)(P * c.kp), "im2col buffer too small");
   k_im2col<<<gsz(P * c.kp), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, c.in->y.p, U.col.p);
   AIRT_LAUNCH_CHECK();
   GemmArgs g{};
@@ -408,11 +571,20 @@ void conv_backward(UNet &U, Conv &c, int B, bool need_dx) {
   const int64_t P = (int64_t)B * c.H * c.W;
   const int64_t ksplit = std::max<int64_t>(64, ((P / 64 + 63) / 64) * 64);  // ~64 K-splits
   {
-    const int64_t blocks = std::min<int64_t>(1184, std::max<int64_t>(1, P / 64));
-    const int64_t rpb = (P + blocks - 1) / blocks;
-    k_relu_mask_colsum<<<(unsigned)((P + rpb - 1) / rpb), 256, 0, U.s>>>(
-        P, c.cout, rpb, c.out->g.p, c.out->y.p, U.dym.p, c.gb.p);
+    int64_t blocks, rpb;
+    row_blocks(P, blocks, rpb);
+    k_relu_mask_colsum<<<(unsigned)blocks, 256, 0, U.s>>>(P, c.cout, rpb, c.out->g.p, c.out->y.p, U.dym.p,
+                                                         c.gb.p);
     AIRT_LAUNCH_CHECK();
+  }
+  if (c.cin == 1) {  // first convolution: direct weight gradient, no dX
+    AIRT_REQUIRE(!need_dx && c.cout <= 64, "first convolution: unsupported configuration");
+    int64_t blocks, rpb;
+    row_blocks(P, blocks, rpb);
+    k_conv1_wgrad<<<(unsigned)blocks, 288, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, rpb, c.in->y.p, U.dym.p,
+                                                     c.gw.p);
+    AIRT_LAUNCH_CHECK();
+    return;
   }
   if (c.cin % 8 == 0 && c.cout % 8 == 0) {
     GemmArgs gw{};
@@ -450,6 +622,8 @@ void conv_backward(UNet &U, Conv &c, int B, bool need_dx) {
     conv3x3_bf16(gd, bn_for(c.cin), EPI_ADD_F32, U.s);
     return;
   }
+  AIRT_REQUIRE(U.col.n >= (size_t)(P * c.kp) && (!need_dx || U.dcol.n >= (size_t)(P * c.kp)),
+               "im2col buffer too small");
   k_im2col<<<gsz(P * c.kp), kT, 0, U.s>>>(B, c.H, c.W, c.cin, c.kp, c.in->y.p, U.col.p);
   AIRT_LAUNCH_CHECK();
   // dW^T[Kp][Co] += col^T * dYm, stored transposed into gw[Co][Kp]
@@ -564,7 +738,7 @@ UNet *unet_create(int H, int W, int base, int levels, int maxB, uint64_t seed) {
     for (size_t i = 0; i < U->convs.size(); ++i) {
       const Conv &c = U->convs[i];
       const size_t ncol = (size_t)maxB * c.H * c.W * c.kp;
-      if (c.cin % 8 != 0 || c.cout % 8 != 0) {
+      if (c.cin != 1 && (c.cin % 8 != 0 || c.cout % 8 != 0)) {
         colmax = std::max(colmax, ncol);
         if (i > 0) dcolmax = std::max(dcolmax, ncol);
       }
@@ -649,7 +823,7 @@ void unet_forward_body(UNet &U, int B) {
   for (int l = 0; l < U.levels; ++l) {
     if (l > 0) {
       Tensor *src = U.eb[l - 1];
-      k_pool<<<gsz((int64_t)B * U.pool[l]->H * U.pool[l]->W * src->C), kT, 0, U.s>>>(
+      k_pool<<<gsz((int64_t)B * U.pool[l]->H * U.pool[l]->W * src->C / 8), kT, 0, U.s>>>(
           B, src->H, src->W, src->C, src->y.p, U.pool[l]->y.p);
     }
     conv_forward(U, U.convs[ci++], B);
@@ -689,8 +863,12 @@ float unet_gradients(UNet &U, const float *d_in, const float *d_tgt, int B) {
     AIRT_CHECK_CUDA(cudaMemsetAsync(t->g.p, 0, (size_t)B * t->H * t->W * t->C * 4, U.s));
   float *tgt = U.tgt.p;
   k_img_tgt<<<gsz(P0), kT, 0, U.s>>>(B, U.H, U.W, d_tgt, tgt);
-  k_head_back<<<gsz(P0), kT, 0, U.s>>>(P0, U.base, U.db[0]->y.p, U.hw.p, U.out.p, tgt,
-                                        U.db[0]->g.p, U.hgw.p, U.hgb.p, U.loss.p);
+  {
+    int64_t blocks, rpb;
+    row_blocks(P0, blocks, rpb);
+    k_head_back<<<(unsigned)blocks, 256, 0, U.s>>>(P0, U.base, rpb, U.db[0]->y.p, U.hw.p, U.out.p, tgt,
+                                                   U.db[0]->g.p, U.hgw.p, U.hgb.p, U.loss.p);
+  }
   AIRT_LAUNCH_CHECK();
   int ci = (int)U.convs.size() - 1;
   // decoder, in reverse of the forward order (levels 0 .. L-2)
@@ -699,7 +877,7 @@ float unet_gradients(UNet &U, const float *d_in, const float *d_tgt, int B) {
     conv_backward(U, U.convs[ci--], B, true);  // cat[l] -> da[l]
     Tensor *prev = (l == U.levels - 2) ? U.eb[U.levels - 1] : U.db[l + 1];
     Tensor *cat = U.cat[l];
-    k_up_concat_back<<<gsz((int64_t)B * cat->H * cat->W * cat->C), kT, 0, U.s>>>(
+    k_up_concat_back<<<gsz((int64_t)B * cat->H * cat->W * cat->C / 4), kT, 0, U.s>>>(
         B, cat->H, cat->W, prev->C, U.eb[l]->C, cat->g.p, prev->g.p, U.eb[l]->g.p);
     AIRT_LAUNCH_CHECK();
   }
@@ -709,7 +887,7 @@ float unet_gradients(UNet &U, const float *d_in, const float *d_tgt, int B) {
     conv_backward(U, U.convs[ci--], B, l > 0);   // in -> ea[l]
     if (l > 0) {
       Tensor *src = U.eb[l - 1];
-      k_pool_back<<<gsz((int64_t)B * U.pool[l]->H * U.pool[l]->W * src->C), kT, 0, U.s>>>(
+      k_pool_back<<<gsz((int64_t)B * U.pool[l]->H * U.pool[l]->W * src->C / 8), kT, 0, U.s>>>(
           B, src->H, src->W, src->C, src->y.p, U.pool[l]->g.p, src->g.p);
       AIRT_LAUNCH_CHECK();
     }
