@@ -35,6 +35,7 @@ def _batch_signatures():
         "airt_batch_sirt_device": (C.c_int, [C.c_void_p, C.c_int, _lib._dp, C.c_void_p, _lib._dp,
                                              C.c_int64, C.c_int, C.c_double, C.c_int, C.c_double,
                                              C.c_void_p, C.c_void_p, i64p, _ip, _lib._dp]),
+        "airt_batch_backproject": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _lib._dp]),
         "airt_batch_kaczmarz": (C.c_int, [C.c_void_p, _lib._dp, C.c_int64, C.c_double, C.c_int,
                                           C.c_double, C.c_int, C.c_double, _lib._dp, _lib._dp]),
         "airt_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -177,6 +178,14 @@ class ParallelBatch:
                                              _lib.i64ptr(fin), rule.ctypes.data_as(_ip),
                                              C.byref(ms)))
         return {"finaliter": fin, "stoprule": rule, "relaxpar": lam, "gpu_ms": float(ms.value)}
+
+    def backproject_device(self, method, d_b, d_x) -> float:
+        """x = D .* A'(M .* b) per instance on device vectors (the first SIRT
+        iterate from zero with relaxpar 1); returns the device time in ms."""
+        ms = C.c_double()
+        check(self._L.airt_batch_backproject(self._h, _lib.METHODS[method], C.c_void_p(d_b),
+                                             C.c_void_p(d_x), C.byref(ms)))
+        return float(ms.value)
 
     def kaczmarz(self, b, sweeps, relaxpar=1.0, lbound=None, ubound=None):
         """Kaczmarz sweeps (row order of art.m:188) on every instance from x0 = 0."""

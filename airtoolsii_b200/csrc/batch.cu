@@ -39,7 +39,13 @@ struct Bucket {
   int64_t r0, r1;      // rows
   int64_t c0, c1;      // columns
   int lanes_fwd = 8, lanes_bwd = 8;
+  int idx = 0;                 // position in Batch::buckets
+  int rt_off = 0, ct_off = 0;  // first row / column tile in Batch::rtiles / ctiles
+  int nrt = 0, nct = 0;        // row / column tiles of the bucket
 };
+
+// Segment tiles of the active-tile lists: 2048 rows or columns.
+constexpr int kTileShift = 11;
 
 struct Batch {
   Problem P;                 // block-diagonal CSR/CSC and work vectors
@@ -52,6 +58,11 @@ struct Batch {
   DevBuf<int> inst_row, inst_col, stop, iters, rule;
   DevBuf<double> rsq, nrm2, lam, taud, resn_last;
   bool tuned = false;
+  // tiles of each bucket holding at least one instance that has not stopped,
+  // rebuilt after every stop-rule update; tcount[b] / tcount[nb + b] count
+  // bucket b's listed row / column tiles
+  DevBuf<int> rtiles, ctiles, tcount;
+  int wmethod = -1;  // method whose M and D are in P.M / P.D (the matrix never changes)
 };
 
 namespace {
@@ -150,10 +161,12 @@ struct BFwd {
 
 template <int L>
 __global__ void __launch_bounds__(256, 4)
-    k_batch_fwd(int64_t nseg, const int64_t *__restrict__ rp, const int *__restrict__ ci,
-                const float *__restrict__ rv, const float *__restrict__ x32, BFwd o) {
-  for_each_segment_vp<L>(
-      nseg, rp + o.r0, ci, rv, x32, [&](int64_t i) { return o.stop[o.inst_row[o.r0 + i]] == 0; },
+    k_batch_fwd(int64_t nseg, const int *__restrict__ tiles, const int *__restrict__ ntiles,
+                const int64_t *__restrict__ rp, const int *__restrict__ ci, const float *__restrict__ rv,
+                const float *__restrict__ x32, BFwd o) {
+  for_each_segment_vt<L>(
+      nseg, tiles, ntiles, kTileShift, rp + o.r0, ci, rv, x32,
+      [&](int64_t i) { return o.stop[o.inst_row[o.r0 + i]] == 0; },
       [&](int64_t i, double s, bool lead) {
         if (!lead) return;
         const int64_t r = o.r0 + i;
@@ -175,10 +188,12 @@ struct BUpd {
 
 template <int L>
 __global__ void __launch_bounds__(256, 4)
-    k_batch_bwd(int64_t nseg, const int64_t *__restrict__ cp, const int *__restrict__ ri,
-                const float *__restrict__ cv, const float *__restrict__ mr32, BUpd u) {
-  for_each_segment_vp<L>(
-      nseg, cp + u.c0, ri, cv, mr32, [&](int64_t j) { return u.stop[u.inst_col[u.c0 + j]] == 0; },
+    k_batch_bwd(int64_t nseg, const int *__restrict__ tiles, const int *__restrict__ ntiles,
+                const int64_t *__restrict__ cp, const int *__restrict__ ri, const float *__restrict__ cv,
+                const float *__restrict__ mr32, BUpd u) {
+  for_each_segment_vt<L>(
+      nseg, tiles, ntiles, kTileShift, cp + u.c0, ri, cv, mr32,
+      [&](int64_t j) { return u.stop[u.inst_col[u.c0 + j]] == 0; },
       [&](int64_t j, double g, bool lead) {
         if (!lead) return;
         const int64_t c = u.c0 + j;
@@ -188,6 +203,23 @@ __global__ void __launch_bounds__(256, 4)
         u.x64[c] = x;
         u.x32[c] = (float)x;
       });
+}
+
+// List the tiles of segments [seg0, seg0 + nseg) (tile t: seg0 + t*2^shift
+// ..) that hold at least one instance with stop == 0; inst_of maps a segment
+// to its instance (instances are contiguous, so a tile spans inst_of[first]
+// .. inst_of[last]).  *count must start at zero; list order is arbitrary.
+__global__ void k_active_tiles(int ntiles, int64_t seg0, int64_t nseg, const int *__restrict__ inst_of,
+                               const int *__restrict__ stop, int *__restrict__ list, int *__restrict__ count) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int64_t s0 = seg0 + ((int64_t)t << kTileShift);
+  const int64_t s1 = min(seg0 + nseg, s0 + ((int64_t)1 << kTileShift));
+  for (int k = inst_of[s0]; k <= inst_of[s1 - 1]; ++k)
+    if (!stop[k]) {
+      list[atomicAdd(count, 1)] = t;
+      return;
+    }
 }
 
 // ||r_k||^2 per active instance: one block per instance, fixed order.
@@ -296,32 +328,58 @@ float time_launch(cudaStream_t s, F &&f, int reps = 3) {
   return ms / reps;
 }
 
-void launch_bfwd(Batch &B, const Bucket &bk, int L, const BFwd &o) {
+void launch_bfwd(Batch &B, const Bucket &bk, int L, const BFwd &o, const float *x32 = nullptr) {
   Problem &P = B.P;
+  if (!x32) x32 = P.x32.p;
   cudaStream_t s = P.stream;
   const int64_t ns = bk.r1 - bk.r0;
   if (ns <= 0) return;
   const unsigned g = grid_for(ns * L, 256, 4);
   switch (L) {
-    case 16: k_batch_fwd<16><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
-    case 8: k_batch_fwd<8><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
-    case 4: k_batch_fwd<4><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
-    default: k_batch_fwd<2><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, P.x32.p, o); break;
+#define AIRT_F(LV) \
+  k_batch_fwd<LV><<<g, 256, 0, s>>>(ns, B.rtiles.p + bk.rt_off, B.tcount.p + bk.idx, P.rp.p, P.ci.p, P.rv.p, x32, o)
+    case 16: AIRT_F(16); break;
+    case 8: AIRT_F(8); break;
+    case 4: AIRT_F(4); break;
+    default: AIRT_F(2); break;
+#undef AIRT_F
   }
 }
 
-void launch_bbwd(Batch &B, const Bucket &bk, int L, const BUpd &u) {
+void launch_bbwd(Batch &B, const Bucket &bk, int L, const BUpd &u, const float *mr32 = nullptr) {
   Problem &P = B.P;
+  if (!mr32) mr32 = P.mr32.p;
   cudaStream_t s = P.stream;
   const int64_t ns = bk.c1 - bk.c0;
   if (ns <= 0) return;
   const unsigned g = grid_for(ns * L, 256, 4);
   switch (L) {
-    case 16: k_batch_bwd<16><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
-    case 8: k_batch_bwd<8><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
-    case 4: k_batch_bwd<4><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
-    default: k_batch_bwd<2><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, P.mr32.p, u); break;
+#define AIRT_B(LV)                                                                                      \
+  k_batch_bwd<LV><<<g, 256, 0, s>>>(ns, B.ctiles.p + bk.ct_off, B.tcount.p + B.buckets.size() + bk.idx, \
+                                    P.cp.p, P.ri.p, P.cv.p, mr32, u)
+    case 16: AIRT_B(16); break;
+    case 8: AIRT_B(8); break;
+    case 4: AIRT_B(4); break;
+    default: AIRT_B(2); break;
+#undef AIRT_B
   }
+}
+
+// Rebuild every bucket's active row and column tile lists from stop[].
+void build_tiles(Batch &B, const int *stop) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  const int nb = (int)B.buckets.size();
+  AIRT_CHECK_CUDA(cudaMemsetAsync(B.tcount.p, 0, 2 * nb * sizeof(int), s));
+  for (const Bucket &bk : B.buckets) {
+    if (bk.nrt > 0)
+      k_active_tiles<<<(bk.nrt + 127) / 128, 128, 0, s>>>(bk.nrt, bk.r0, bk.r1 - bk.r0, B.inst_row.p, stop,
+                                                          B.rtiles.p + bk.rt_off, B.tcount.p + bk.idx);
+    if (bk.nct > 0)
+      k_active_tiles<<<(bk.nct + 127) / 128, 128, 0, s>>>(bk.nct, bk.c0, bk.c1 - bk.c0, B.inst_col.p, stop,
+                                                          B.ctiles.p + bk.ct_off, B.tcount.p + nb + bk.idx);
+  }
+  AIRT_LAUNCH_CHECK();
 }
 
 }  // namespace
@@ -375,8 +433,23 @@ Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const d
       bk.r1 = B->row_off[e];
       bk.c0 = B->col_off[k];
       bk.c1 = B->col_off[e];
+      bk.idx = (int)B->buckets.size();
       B->buckets.push_back(bk);
       k = e;
+    }
+    {
+      int rt = 0, ct = 0;
+      for (Bucket &bk : B->buckets) {
+        bk.nrt = (int)((bk.r1 - bk.r0 + (1 << kTileShift) - 1) >> kTileShift);
+        bk.nct = (int)((bk.c1 - bk.c0 + (1 << kTileShift) - 1) >> kTileShift);
+        bk.rt_off = rt;
+        bk.ct_off = ct;
+        rt += bk.nrt;
+        ct += bk.nct;
+      }
+      B->rtiles.ensure(rt > 0 ? rt : 1);
+      B->ctiles.ensure(ct > 0 ? ct : 1);
+      B->tcount.ensure(2 * B->buckets.size());
     }
     // generation: count, scan, fill, transpose (as generate_matrix)
     DevBuf<int64_t> counts;
@@ -437,6 +510,12 @@ void batch_destroy(Batch *B) {
 }
 
 namespace {
+__global__ void k_batch_mb(int64_t m, const double *__restrict__ M, const double *__restrict__ b,
+                           float *__restrict__ mr32) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    mr32[i] = (float)(M[i] * b[i]);
+}
+
 __global__ void k_fill1(int64_t n, double *__restrict__ a) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -448,8 +527,10 @@ __global__ void k_fill1(int64_t n, double *__restrict__ a) {
 // the instance; every other weight is a per-row or per-column quantity.
 void batch_weights(Batch &B, int method) {
   Problem &P = B.P;
+  if (B.wmethod == method) return;
   P.M.ensure(P.m);
   P.D.ensure(P.n);
+  B.wmethod = method;
   if (method != AIRT_CIMMINO) {
     compute_weights(P, method, P.M.p, P.D.p);
     return;
@@ -515,6 +596,7 @@ void batch_tune(Batch &B) {
   DevBuf<int> nostop;
   nostop.ensure(B.ninst);
   AIRT_CHECK_CUDA(cudaMemsetAsync(nostop.p, 0, B.ninst * sizeof(int), s));
+  build_tiles(B, nostop.p);
   DevBuf<double> zero;
   zero.ensure(P.m > P.n ? P.m : P.n);
   AIRT_CHECK_CUDA(cudaMemsetAsync(zero.p, 0, zero.n * sizeof(double), s));
@@ -528,27 +610,9 @@ void batch_tune(Batch &B) {
     float best_f = 1e30f, best_b = 1e30f;
     for (int L : cands) {
       BFwd o{zero.p, zero.p, mtmp.p, yr.p, B.inst_row.p, nostop.p, bk.r0};
-      const float tf = time_launch(s, [&] {
-        const int64_t ns = bk.r1 - bk.r0;
-        const unsigned g = grid_for(ns * L, 256, 4);
-        switch (L) {
-          case 16: k_batch_fwd<16><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
-          case 8: k_batch_fwd<8><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
-          case 4: k_batch_fwd<4><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
-          default: k_batch_fwd<2><<<g, 256, 0, s>>>(ns, P.rp.p, P.ci.p, P.rv.p, xc.p, o); break;
-        }
-      });
+      const float tf = time_launch(s, [&] { launch_bfwd(B, bk, L, o, xc.p); });
       BUpd u{zero.p, zero.p, xtmp.p, x32tmp.p, B.inst_col.p, nostop.p, 0, 0, 0.0, 0.0, bk.c0};
-      const float tb = time_launch(s, [&] {
-        const int64_t ns = bk.c1 - bk.c0;
-        const unsigned g = grid_for(ns * L, 256, 4);
-        switch (L) {
-          case 16: k_batch_bwd<16><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
-          case 8: k_batch_bwd<8><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
-          case 4: k_batch_bwd<4><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
-          default: k_batch_bwd<2><<<g, 256, 0, s>>>(ns, P.cp.p, P.ri.p, P.cv.p, xr.p, u); break;
-        }
-      });
+      const float tb = time_launch(s, [&] { launch_bbwd(B, bk, L, u, xr.p); });
       AIRT_LAUNCH_CHECK();
       if (tf < best_f) {
         best_f = tf;
@@ -596,6 +660,7 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
   AIRT_CHECK_CUDA(cudaMemsetAsync(B.stop.p, 0, K * sizeof(int), s));
   AIRT_CHECK_CUDA(cudaMemsetAsync(B.iters.p, 0, K * sizeof(int), s));
   AIRT_CHECK_CUDA(cudaMemsetAsync(B.rule.p, 0, K * sizeof(int), s));
+  build_tiles(B, B.stop.p);
   BFwd fo{d_b, P.M.p, P.mr32.p, B.rsq.p, B.inst_row.p, B.stop.p, 0};
   BUpd uo{P.D.p, B.lam.p, P.x64.p, P.x32.p, B.inst_col.p, B.stop.p, lbk, ubk, lb, ub, 0};
   const double *taud = taud_host ? B.taud.p : nullptr;
@@ -619,6 +684,7 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
   k_batch_ctrl<<<gk, 128, 0, s>>>(K, 1, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
                                   B.resn_last.p);
   AIRT_LAUNCH_CHECK();
+  build_tiles(B, B.stop.p);
   std::vector<int> hstop(K);
   const int64_t chunk = 8;
   for (int64_t it = 1; it <= kmax;) {
@@ -628,6 +694,7 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
       fwd_all();
       k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
                                       B.resn_last.p);
+      build_tiles(B, B.stop.p);
     }
     AIRT_LAUNCH_CHECK();
     it += cnt;
@@ -652,6 +719,47 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
     if (finaliter) finaliter[k] = hit[k];
     if (stoprule) stoprule[k] = hrule[k];
   }
+  if (gpu_ms) *gpu_ms = ms;
+}
+
+// x = D .* A'(M .* b) per instance: the first SIRT iterate from x0 = 0 with
+// relaxpar 1 and no bounds, in one transpose pass (the residual of x0 = 0 is
+// b itself, so the forward pass of a one-iteration SIRT call is skipped).
+void batch_backproject(Batch &B, int method, const double *d_b, double *d_x, double *gpu_ms) {
+  Problem &P = B.P;
+  cudaStream_t s = P.stream;
+  const int K = B.ninst;
+  cudaEvent_t t0, t1;
+  AIRT_CHECK_CUDA(cudaEventCreate(&t0));
+  AIRT_CHECK_CUDA(cudaEventCreate(&t1));
+  batch_tune(B);
+  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
+  batch_weights(B, method);
+  P.x64.ensure(P.n);
+  P.x32.ensure(P.n);
+  P.mr32.ensure(P.m);
+  B.stop.ensure(K);
+  B.lam.ensure(K);
+  const std::vector<double> ones(K, 1.0);
+  B.lam.upload(ones.data(), K, s);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(B.stop.p, 0, K * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.x64.p, 0, P.n * sizeof(double), s));
+  build_tiles(B, B.stop.p);
+  k_batch_mb<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, P.M.p, d_b, P.mr32.p);
+  AIRT_LAUNCH_CHECK();
+  BUpd uo{P.D.p, B.lam.p, P.x64.p, P.x32.p, B.inst_col.p, B.stop.p, 0, 0, 0.0, 0.0, 0};
+  for (const Bucket &bk : B.buckets) {
+    BUpd u = uo;
+    u.c0 = bk.c0;
+    launch_bbwd(B, bk, bk.lanes_bwd, u);
+  }
+  AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(d_x, P.x64.p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
   if (gpu_ms) *gpu_ms = ms;
 }
 

@@ -407,6 +407,14 @@ int airt_batch_sirt(airt_batch *h, int method, const double *relaxpar, const dou
   AIRT_API_END
 }
 
+int airt_batch_backproject(airt_batch *h, int method, const double *d_b, double *d_x, double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && d_b && d_x, "null pointer argument");
+  AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+  batch_backproject(*reinterpret_cast<Batch *>(h), method, d_b, d_x, gpu_ms);
+  AIRT_API_END
+}
+
 int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double relaxpar,
                         int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms) {
   AIRT_API_BEGIN

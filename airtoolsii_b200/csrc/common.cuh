@@ -242,6 +242,7 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
                 int64_t *finaliter, int *stoprule, double *gpu_ms);
 void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int lbk, double lb,
                     int ubk, double ub, double *d_x, double *gpu_ms);
+void batch_backproject(Batch &B, int method, const double *d_b, double *d_x, double *gpu_ms);
 
 // Exclusive scan of counts[0..n) into offs[0..n] (offs[n] = total), device.
 void exclusive_scan_i64(const int64_t *counts, int64_t *offs, int64_t n, cudaStream_t s);

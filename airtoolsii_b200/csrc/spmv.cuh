@@ -92,11 +92,17 @@ __device__ __forceinline__ void for_each_segment_v(int64_t nseg, const int64_t *
   }
 }
 
-// for_each_segment_v with a per-segment predicate: segments for which
-// active(i) is false are skipped without touching their nonzeros (all lanes
-// of a group evaluate it, so the group stays converged).
+// for_each_segment_v over a list of segment tiles, with a per-segment
+// predicate.  Tile t covers segments t << tshift .. +(1 << tshift); the
+// groups walk the *ntiles listed tiles (tiles[0 .. *ntiles)), so ranges left
+// out of the list cost nothing, and segments for which active(i) is false
+// are skipped without touching their nonzeros (all lanes of a group evaluate
+// it, so the group stays converged).  epi(i, sum, lead) sees lead = false
+// for skipped segments.
 template <int LANES, typename TX, class Act, class Epi>
-__device__ __forceinline__ void for_each_segment_vp(int64_t nseg, const int64_t *__restrict__ ptr,
+__device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__restrict__ tiles,
+                                                    const int *__restrict__ ntiles, int tshift,
+                                                    const int64_t *__restrict__ ptr,
                                                     const int *__restrict__ idx,
                                                     const float *__restrict__ val,
                                                     const TX *__restrict__ x, Act &&active,
@@ -104,11 +110,14 @@ __device__ __forceinline__ void for_each_segment_vp(int64_t nseg, const int64_t 
   const int lane = threadIdx.x % LANES;
   const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / LANES;
   const int64_t ng = (int64_t)gridDim.x * blockDim.x / LANES;
-  const int64_t trips = (nseg + ng - 1) / ng;
+  const int64_t total = (int64_t)__ldg(ntiles) << tshift;
+  const int64_t tmask = ((int64_t)1 << tshift) - 1;
+  const int64_t trips = (total + ng - 1) / ng;
   const float4 *__restrict__ V4 = reinterpret_cast<const float4 *>(val);
   const int4 *__restrict__ I4 = reinterpret_cast<const int4 *>(idx);
   for (int64_t t = 0; t < trips; ++t) {
-    const int64_t i = gid + t * ng;
+    const int64_t u = gid + t * ng;
+    const int64_t i = u < total ? ((int64_t)__ldg(tiles + (u >> tshift)) << tshift) + (u & tmask) : nseg;
     const bool on = i < nseg && active(i);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (on) {

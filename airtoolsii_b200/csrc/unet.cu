@@ -395,26 +395,56 @@ __global__ void k_conv1_fwd(int64_t P, int H, int W, int Co, int Kp, const __nv_
 }
 
 // Weight gradient of the first convolution: gw[co][tap] += sum_p dYm[p][co]
-// * x[p + tap].  Block = 9 warps (one per tap), lane -> output channels
-// lane, lane + 32 (Co <= 64); each block owns a contiguous pixel range.
-__global__ void __launch_bounds__(288) k_conv1_wgrad(int64_t P, int H, int W, int Co, int Kp,
+// * x[p + tap].  Lane -> output channels lane and lane + 32 (Co <= 64), all
+// nine taps in registers; the 8 warps of a block take every 8th pixel of the
+// block's range, and the block's sums meet in shared memory before one
+// atomicAdd per (co, tap).
+__global__ void __launch_bounds__(256) k_conv1_wgrad(int64_t P, int H, int W, int Co, int Kp,
                                                      int64_t rows_per_block, const __nv_bfloat16 *__restrict__ x,
                                                      const __nv_bfloat16 *__restrict__ dYm,
                                                      float *__restrict__ gw) {
-  const int tap = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+  __shared__ float sh[9 * 64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < 9 * 64; i += blockDim.x) sh[i] = 0.f;
+  __syncthreads();
   const int64_t r0 = blockIdx.x * rows_per_block;
   const int64_t r1 = min(P, r0 + rows_per_block);
-  float a0 = 0.f, a1 = 0.f;
-  for (int64_t p = r0; p < r1; ++p) {
-    const int w = (int)(p % W), h = (int)((p / W) % H);
-    if (h + dh < 0 || h + dh >= H || w + dw < 0 || w + dw >= W) continue;
-    const float xv = __bfloat162float(x[p + (int64_t)dh * W + dw]);
-    if (lane < Co) a0 += __bfloat162float(dYm[p * Co + lane]) * xv;
-    if (lane + 32 < Co) a1 += __bfloat162float(dYm[p * Co + lane + 32]) * xv;
+  float a0[9], a1[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) a0[t] = a1[t] = 0.f;
+  int64_t p = r0 + warp;
+  int w = (int)(p % W), h = (int)((p / W) % H);
+  for (; p < r1; p += 8) {
+    float xv[9];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+      const bool in = h + dh >= 0 && h + dh < H && w + dw >= 0 && w + dw < W;
+      xv[tap] = in ? __bfloat162float(x[p + (int64_t)dh * W + dw]) : 0.f;
+    }
+    const float d0 = lane < Co ? __bfloat162float(dYm[p * Co + lane]) : 0.f;
+    const float d1 = lane + 32 < Co ? __bfloat162float(dYm[p * Co + lane + 32]) : 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      a0[tap] += d0 * xv[tap];
+      a1[tap] += d1 * xv[tap];
+    }
+    w += 8;
+    while (w >= W) {
+      w -= W;
+      if (++h == H) h = 0;
+    }
   }
-  if (lane < Co) atomicAdd(gw + (int64_t)lane * Kp + tap, a0);
-  if (lane + 32 < Co) atomicAdd(gw + (int64_t)(lane + 32) * Kp + tap, a1);
+#pragma unroll
+  for (int tap = 0; tap < 9; ++tap) {
+    if (lane < Co) atomicAdd(&sh[tap * 64 + lane], a0[tap]);
+    if (lane + 32 < Co) atomicAdd(&sh[tap * 64 + lane + 32], a1[tap]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 9 * Co; i += blockDim.x) {
+    const int tap = i / Co, co = i - tap * Co;
+    atomicAdd(gw + (int64_t)co * Kp + tap, sh[tap * 64 + co]);
+  }
 }
 
 __global__ void k_to_bf16(int64_t n, const float *__restrict__ a, __nv_bfloat16 *__restrict__ b) {
@@ -581,7 +611,7 @@ void conv_backward(UNet &U, Conv &c, int B, bool need_dx) {
     AIRT_REQUIRE(!need_dx && c.cout <= 64, "first convolution: unsupported configuration");
     int64_t blocks, rpb;
     row_blocks(P, blocks, rpb);
-    k_conv1_wgrad<<<(unsigned)blocks, 288, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, rpb, c.in->y.p, U.dym.p,
+    k_conv1_wgrad<<<(unsigned)blocks, 256, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, rpb, c.in->y.p, U.dym.p,
                                                      c.gw.p);
     AIRT_LAUNCH_CHECK();
     return;

@@ -192,6 +192,10 @@ int airt_batch_sirt_device(airt_batch *h, int method, const double *relaxpar, co
                            const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
                            double ub, const double *d_x0, double *d_x, int64_t *finaliter,
                            int *stoprule, double *gpu_ms);
+/* x = D .* A'(M .* b) per instance with the weights of `method` (device
+ * vectors): the first iterate of sirt (sirt/sirt.m:229) from x0 = 0
+ * with relaxpar 1 and no bounds, computed with one transpose pass. */
+int airt_batch_backproject(airt_batch *h, int method, const double *d_b, double *d_x, double *gpu_ms);
 /* Kaczmarz sweeps in the kaczmarz row order, one CTA per instance, x0 = 0. */
 int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double relaxpar,
                         int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms);

@@ -83,3 +83,23 @@ def test_batch_kaczmarz(batch):
     for k, A in enumerate(mats):
         Xo, _ = O.art("kaczmarz", A, bs[k], [3], options={"lbound": 0.0})
         assert relerr(xs[k], Xo[:, -1]) <= RTOL
+
+
+@pytest.mark.parametrize("method", ["sart", "cimmino"])
+def test_batch_backproject_is_first_sirt_iterate(batch, method):
+    """airt_batch_backproject equals a one-iteration batched SIRT call from
+    zero with relaxpar 1 bit for bit, and the oracle's first iterate."""
+    import torch
+    B, mats, bs, _, _ = batch
+    b = np.concatenate(bs)
+    xs, _ = B.sirt(method, b, 1, relaxpar=1.0)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.full((B.n,), float("nan"), dtype=torch.float64, device="cuda")
+    for _ in range(2):  # the second call reuses the cached weights
+        B.backproject_device(method, db.data_ptr(), dx.data_ptr())
+        torch.cuda.synchronize()
+        got = B.split_cols(dx.cpu().numpy())
+        for k, A in enumerate(mats):
+            assert np.array_equal(got[k], xs[k])
+            Xo, _, _ = O.sirt(method, A, bs[k], [1], options={"relaxpar": 1.0})
+            assert relerr(got[k], Xo[:, -1]) <= RTOL
