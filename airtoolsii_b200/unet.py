@@ -14,6 +14,12 @@ from . import _lib
 from ._lib import check, lib
 
 
+def _bf16_rne(w: np.ndarray) -> np.ndarray:
+    """FP32 -> BF16 bit patterns (uint16), round to nearest even."""
+    u = np.ascontiguousarray(w, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
 class UNet:
     """levels-level U-Net on H x W images, widths base*2^l."""
 
@@ -53,6 +59,52 @@ class UNet:
         out = np.zeros(self.num_params, np.float32)
         check(lib().airt_unet_get_grads(self._h, out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
+
+    def layer_shapes(self):
+        """(cin, cout) of every 3x3 convolution in the order of the flattened
+        parameters: encoder levels 0..L-1, then decoder levels L-2..0."""
+        b, L = self.base, self.levels
+        shapes = []
+        for lv in range(L):
+            shapes += [(1 if lv == 0 else b << (lv - 1), b << lv), (b << lv, b << lv)]
+        for lv in range(L - 2, -1, -1):
+            shapes += [((b << (lv + 1)) + (b << lv), b << lv), (b << lv, b << lv)]
+        return shapes
+
+    def _weight_mask(self) -> np.ndarray:
+        """True for convolution weights, False for biases and the 1x1 head."""
+        mask = np.zeros(self.num_params, bool)
+        off = 0
+        for cin, cout in self.layer_shapes():
+            mask[off:off + 9 * cin * cout] = True
+            off += 9 * cin * cout + cout
+        assert off + self.base + 1 == self.num_params
+        return mask
+
+    def save(self, path, **meta) -> None:
+        """Checkpoint for inference: 3x3 convolution weights as BF16 (the
+        values the tensor cores use, so inference from the file is identical),
+        biases and head in FP32, plus metadata."""
+        p = self.get_params()
+        mask = self._weight_mask()
+        np.savez_compressed(path, w_bf16=_bf16_rne(p[mask]), rest_f32=p[~mask],
+                            H=self.H, W=self.W, base=self.base, levels=self.levels,
+                            meta=np.array(repr(meta)))
+
+    def load(self, path) -> dict:
+        """Load a checkpoint written by save (shape must match); returns its
+        metadata."""
+        z = np.load(path)
+        if (int(z["H"]), int(z["W"]), int(z["base"]), int(z["levels"])) != (
+                self.H, self.W, self.base, self.levels):
+            raise ValueError("checkpoint was made for a different network shape")
+        mask = self._weight_mask()
+        p = np.zeros(self.num_params, np.float32)
+        p[mask] = (z["w_bf16"].astype(np.uint32) << 16).view(np.float32)
+        p[~mask] = z["rest_f32"]
+        self.set_params(p)
+        import ast
+        return ast.literal_eval(str(z["meta"]))
 
     def forward(self, d_in, d_out, B: int) -> None:
         """d_in, d_out: device float32 buffers of B images (x(:) order)."""

@@ -214,3 +214,50 @@ class WarmStart:
                     plain_gpu_ms=ip["gpu_ms"], warm_gpu_ms=u_ms + iw["gpu_ms"],
                     net_wall_s=t_net, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
                     plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0))
+
+
+# ---------------------------------------------------------------- training CLI
+# The configuration the checkpoint in airtoolsii_b200/weights was trained
+# with: N=256, 60 angles (0:3:177 degrees), 2% noise, 20000 phantoms (seeds
+# 1000..20999), 8 epochs of Adam, batch 16, learning rate 1e-3 halved every
+# 2 epochs.  Training runs on the GPU only (the network's gradients use
+# atomics, so runs agree statistically, not bit for bit).
+C5 = dict(N=256, theta_step=3.0, angles=60, eta=0.02, base=32, levels=4, train_seeds=(1000, 21000),
+          epochs=8, batch=16, lr=1e-3, decay_every=2, net_seed=0)
+CHECKPOINT = "weights/unet_paralleltomo_n256_a60.npz"
+
+
+def checkpoint_path() -> str:
+    import os
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), CHECKPOINT)
+
+
+def c5_warmstart(max_batch=32, chunk=128) -> WarmStart:
+    c = C5
+    return WarmStart(N=c["N"], theta=np.arange(c["angles"]) * c["theta_step"], base=c["base"],
+                     levels=c["levels"], max_batch=max_batch, seed=c["net_seed"], chunk=chunk)
+
+
+def train_c5(out=None, log=print) -> dict:
+    """Generate the training pairs on the GPU, train, and write the checkpoint."""
+    c = C5
+    ws = c5_warmstart()
+    t0 = time.perf_counter()
+    tr = ws.prepare(list(range(*c["train_seeds"])), eta=c["eta"])
+    t1 = time.perf_counter()
+    hist = ws.train(tr["u"], tr["target"], epochs=c["epochs"], batch=c["batch"], lr=c["lr"],
+                    decay_every=c["decay_every"], log=log)
+    ws.torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    meta = dict(c, prepare_s=round(t1 - t0, 2), train_s=round(t2 - t1, 2), final_mse=hist[-1],
+                mean_dp_iters=float(tr["iters"].mean()))
+    ws.net.save(out or checkpoint_path(), **meta)
+    return meta
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="train the N=256 / 60-angle warm-start U-Net")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    print(train_c5(a.out))

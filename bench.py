@@ -11,8 +11,14 @@ the CSR+CSC model, (16*nnz + 16*m + 16*n) bytes per iteration, times 200,
 divided by the step's device time.  Inputs exceed L2 (A is ~1.9 GB), so no
 extra L2 flush is needed between steps.
 
+The line's "time_to_dp" object (one GPU only) holds the second half of the
+headline metric: time from device-resident sinograms to the discrepancy-
+principle stop for the learned warm start against plain batched GPU SIRT on
+1000 held-out N=256 problems (see warm_leg).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl airt|reference]
                   [--small]  (N=256 case for ncu captures; A ~0.25 GB > L2)
+                  [--no-warm] [--warm-heldout 1000] [--warm-batch 250]
 """
 from __future__ import annotations
 
@@ -41,6 +47,9 @@ def parse():
     ap.add_argument("--iters", type=int, default=200)
     ap.add_argument("--small", action="store_true", help="N=256 problem (profiling captures)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-warm", action="store_true", help="skip the warm-start time-to-DP leg")
+    ap.add_argument("--warm-heldout", type=int, default=1000, help="held-out seeds of the time-to-DP leg")
+    ap.add_argument("--warm-batch", type=int, default=250, help="instances per batched solve")
     return ap.parse_args()
 
 
@@ -119,6 +128,63 @@ def cpu_leg(A_csc, b, M, D, lam, iters, m, n, nnz):
             "cores": cbind.num_threads(), "kind": "port",
             "sample": f"{iters} cimmino iterations of the same problem, FP64 CSR+CSC "
                       f"(C restatement, OpenMP), {dt:.2f} s"}
+
+
+def warm_leg(a):
+    """Time to the DP stop, learned warm start vs plain batched GPU SIRT.
+
+    Workload: paralleltomo N=256, 60 angles (0:3:177 degrees), 2% noise,
+    held-out random-ellipse phantoms (seeds 500000..), solved `warm_batch` at
+    a time as one block-diagonal batch with a per-instance DP stop (tau =
+    1.02).  plain: cimmino from x0 = 0.  warm: u = D.*A'(M.*b) (one SART
+    step), x0 = U-Net(u) from the committed checkpoint, cimmino from x0.  Both
+    pipelines start from the sinograms resident on the device and end with
+    the solutions resident on the device; times are host wall clocks around
+    each synchronised pipeline (after one untimed pass), summed over the
+    batches.  The network was trained on 20000 other seeds (seeds 1000..20999)
+    by this project's kernels (airtoolsii_b200/warmstart.py, train_c5)."""
+    import torch
+    from airtoolsii_b200 import warmstart as W
+    ws = W.c5_warmstart()
+    meta = ws.net.load(W.checkpoint_path())
+    seeds = list(range(500000, 500000 + a.warm_heldout))
+    te = ws.prepare(seeds, eta=W.C5["eta"])
+    torch.cuda.synchronize()
+    tot = {"plain_wall_s": 0.0, "warm_wall_s": 0.0, "net_wall_s": 0.0, "plain_gpu_ms": 0.0,
+           "warm_gpu_ms": 0.0}
+    keys = ["plain_iters", "warm_iters", "plain_relerr", "warm_relerr", "x0_relerr"]
+    cat = {k: [] for k in keys}
+    for c0 in range(0, len(seeds), a.warm_batch):
+        sel = np.arange(c0, min(len(seeds), c0 + a.warm_batch))
+        if len(sel) != a.warm_batch:
+            break
+        ws.compare_batched(te, sel)          # untimed pass (tuning, first-touch)
+        r = ws.compare_batched(te, sel)
+        for k in tot:
+            tot[k] += r[k]
+        for k in keys:
+            cat[k].append(np.asarray(r[k], dtype=float))
+    cat = {k: np.concatenate(v) for k, v in cat.items()}
+    done = len(cat["plain_iters"])
+    return {
+        "metric": "time to the DP stop, warm start vs plain batched GPU SIRT (cimmino)",
+        "config": {"workload": "paralleltomo N=256, 60 angles, 2% noise, DP tau=1.02",
+                   "held_out": done, "batch": a.warm_batch,
+                   "network": "U-Net 4 levels, base 32, BF16 tcgen05 convolutions",
+                   "checkpoint": W.CHECKPOINT, "trained_on": meta.get("train_seeds"),
+                   "epochs": meta.get("epochs")},
+        "plain_s": round(tot["plain_wall_s"], 4), "warm_s": round(tot["warm_wall_s"], 4),
+        "speedup": round(tot["plain_wall_s"] / tot["warm_wall_s"], 3),
+        "net_s": round(tot["net_wall_s"], 4),
+        "plain_solver_gpu_ms": round(tot["plain_gpu_ms"], 2),
+        "warm_solver_gpu_ms": round(tot["warm_gpu_ms"], 2),
+        "plain_iters_mean": round(float(cat["plain_iters"].mean()), 3),
+        "warm_iters_mean": round(float(cat["warm_iters"].mean()), 3),
+        "plain_relerr_mean": round(float(cat["plain_relerr"].mean()), 5),
+        "warm_relerr_mean": round(float(cat["warm_relerr"].mean()), 5),
+        "x0_relerr_mean": round(float(cat["x0_relerr"].mean()), 5),
+        "warm_not_worse_frac": round(float(np.mean(cat["warm_relerr"] <= cat["plain_relerr"] * 1.0001)), 4),
+    }
 
 
 def main():
@@ -297,6 +363,8 @@ def main():
             M, D = A.weights(a.method)
             line["cpu_baseline"] = cpu_leg(A.to_scipy(), b, M, D, lam, 5 if not a.small else 20,
                                            m, n, nnz)
+        if not a.no_warm and world == 1:
+            line["time_to_dp"] = warm_leg(a)
         print(json.dumps(line), flush=True)
         del x_gpu
     if dist is not None:
