@@ -127,3 +127,44 @@ class UNet:
         check(lib().airt_unet_train_step(self._h, C.c_void_p(d_in), C.c_void_p(d_tgt), int(B),
                                          float(lr), C.byref(loss)))
         return float(loss.value)
+
+
+def _timing_main():
+    """python -m airtoolsii_b200.unet [--batch B] [--reps R]: device time per
+    image of the forward pass and of one Adam training step of the N=256,
+    4-level, base-32 network (random inputs), CUDA events on its stream."""
+    import argparse
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args()
+    B = a.batch
+    net = UNet(256, 256, 32, 4, B, 0)
+    u = torch.rand(B, 65536, device="cuda")
+    t = torch.rand_like(u)
+    o = torch.empty_like(u)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        net.forward(u.data_ptr(), o.data_ptr(), B)
+        net.train_step(u.data_ptr(), t.data_ptr(), B, 1e-4)
+    torch.cuda.synchronize()
+    s = torch.cuda.ExternalStream(net.stream_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(a.reps):
+        net.forward(u.data_ptr(), o.data_ptr(), B)
+    e1.record(s)
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1) / a.reps / B
+    e0.record(s)
+    for _ in range(a.reps):
+        net.train_step(u.data_ptr(), t.data_ptr(), B, 1e-4)
+    e1.record(s)
+    torch.cuda.synchronize()
+    print({"forward_ms_per_image": round(fwd, 5),
+           "train_ms_per_image": round(e0.elapsed_time(e1) / a.reps / B, 5)})
+
+
+if __name__ == "__main__":
+    _timing_main()
