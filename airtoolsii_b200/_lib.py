@@ -23,7 +23,7 @@ AIRT_ERR_UNSUPPORTED = 5
 
 METHODS = {"landweber": 0, "cimmino": 1, "cav": 2, "drop": 3, "sart": 4}
 AIRT_CUSTOM = 5
-STOP = {"NONE": 0, "DP": 1, "ME": 2}
+STOP = {"NONE": 0, "DP": 1, "ME": 2, "NCP": 3}
 RELAX_CONST, RELAX_LINE, RELAX_TABLE = 1, 2, 3
 BOUND_NONE, BOUND_SCALAR, BOUND_VECTOR = 0, 1, 2
 
@@ -37,7 +37,8 @@ class SirtOpts(C.Structure):
                 ("relaxpar", C.c_double), ("relax_table", _dp), ("stoprule", C.c_int),
                 ("taudelta", C.c_double), ("lb_kind", C.c_int), ("ub_kind", C.c_int),
                 ("lb", C.c_double), ("ub", C.c_double), ("lbv", _dp), ("ubv", _dp),
-                ("kmax", C.c_int64)]
+                ("kmax", C.c_int64), ("ncp_rows", C.c_int), ("ncp_cols", C.c_int),
+                ("ncp_smooth", C.c_int)]
 
 
 class ArtOpts(C.Structure):

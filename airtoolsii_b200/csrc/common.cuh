@@ -127,6 +127,10 @@ struct SirtParams {
   const double *relax_table;  // device, kmax entries
   double *resn_hist;          // device, kmax+1
   double *lam_hist;           // device, kmax+1
+  // NCP: per-column distances of the current residual, history of ncc
+  const double *ncc_col;      // device, ncp_cols
+  double *dk;                 // device, ncp_smooth (starts at +inf)
+  int ncp_cols, ncp_smooth;
 };
 
 // ---------------------------------------------------------------- problem
@@ -159,6 +163,9 @@ struct Problem {
 
   // solver work vectors
   DevBuf<double> x64, r64, rprev, g64, b64, M, D, lbv, ubv, vin, vout, table, resn, lamh, Xd;
+  // NCP stopping rule: DFT twiddles (cos, sin pairs), power spectra, column distances, history
+  DevBuf<double> ncp_tw, ncp_pk, ncp_col, ncp_dk;
+  int ncp_len = 0;  // column length the twiddles were made for
   DevBuf<float> x32, mr32;
   DevBuf<SirtState> state;
   DevBuf<SirtParams> params;

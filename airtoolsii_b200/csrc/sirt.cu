@@ -241,6 +241,68 @@ __global__ void __launch_bounds__(kThreads) k_dg2(int64_t n, const double *__res
   if (threadIdx.x == 0) atomicAdd(&st->acc[4], a);
 }
 
+// NCP (check_stoprules.m:97-150), part 1: periodogram of every residual
+// column.  Block row j = column j of the residual reshaped to L x ncols
+// (column-major), thread -> frequency f = 1..q (q = floor(L/2)); |sum_n
+// r[n] exp(-2 pi i f n / L)|^2 by direct summation with a twiddle table
+// (tw[2k], tw[2k+1] = cos, sin of 2 pi k / L).  The residual of the ME
+// variant of the forward kernel (rprev holds r after it).
+__global__ void __launch_bounds__(256) k_ncp_power(int L, int q, const double *__restrict__ r,
+                                                   const double *__restrict__ tw, double *__restrict__ pk,
+                                                   const SirtState *st) {
+  if (stopped(st)) return;
+  const int j = blockIdx.x;
+  const int f = blockIdx.y * blockDim.x + threadIdx.x + 1;
+  if (f > q) return;
+  const double *rc = r + (int64_t)j * L;
+  double re = 0.0, im = 0.0;
+  int idx = 0;  // (f * n) mod L
+  for (int n = 0; n < L; ++n) {
+    const double v = __ldg(rc + n);
+    re = fma(v, __ldg(tw + 2 * idx), re);
+    im = fma(v, __ldg(tw + 2 * idx + 1), im);
+    idx += f;
+    if (idx >= L) idx -= L;
+  }
+  pk[(int64_t)j * q + (f - 1)] = re * re + im * im;
+}
+
+// NCP part 2: per column, c = cumsum(pk)/sum(pk) and the distance
+// sqrt(sum((c - (1:q)/q).^2)) to the white-noise line.  256 threads own
+// contiguous chunks of the q values; chunk sums meet in a block scan.
+__global__ void __launch_bounds__(256) k_ncp_col(int q, const double *__restrict__ pk,
+                                                 double *__restrict__ ncc_col, const SirtState *st) {
+  if (stopped(st)) return;
+  __shared__ double sh[256];
+  __shared__ double tot_sh;
+  const int t = threadIdx.x, j = blockIdx.x;
+  const double *p = pk + (int64_t)j * q;
+  const int per = (q + 255) / 256, f0 = min(q, t * per), f1 = min(q, f0 + per);
+  double loc = 0.0;
+  for (int f = f0; f < f1; ++f) loc += p[f];
+  sh[t] = loc;
+  __syncthreads();
+  if (t == 0) {  // exclusive prefix of the chunk sums; the total
+    double run = 0.0;
+    for (int i = 0; i < 256; ++i) {
+      const double v = sh[i];
+      sh[i] = run;
+      run += v;
+    }
+    tot_sh = run;
+  }
+  __syncthreads();
+  const double tot = tot_sh;
+  double c = sh[t], acc = 0.0;
+  for (int f = f0; f < f1; ++f) {
+    c += p[f];
+    const double d = c / tot - (double)(f + 1) / (double)q;
+    acc += d * d;
+  }
+  acc = block_sum<256>(acc);
+  if (t == 0) ncc_col[j] = sqrt(acc);
+}
+
 // Stopping rule of check_stoprules.m on the sums of the residual just
 // computed, then the relaxpar of the next iteration (sirt.m:216-226).
 __global__ void k_sirt_ctrl(SirtState *st, const SirtParams *p) {
@@ -269,6 +331,23 @@ __global__ void k_sirt_ctrl(SirtState *st, const SirtParams *p) {
       } else if (k >= kmax) {
         stop = true;
         rule = 0;
+      }
+      break;
+    }
+    case AIRT_STOP_NCP: {  // check_stoprules.m:97-150
+      double sum = 0.0;
+      for (int j = 0; j < p->ncp_cols; ++j) sum += p->ncc_col[j];
+      const double ncc = sum / p->ncp_cols;
+      const int ns = p->ncp_smooth;
+      double mx = -INFINITY, mxn = ncc;  // max(dk), max([dk(2:end); ncc]); NaN ignored
+      for (int i = 0; i < ns; ++i) mx = fmax(mx, p->dk[i]);
+      for (int i = 1; i < ns; ++i) mxn = fmax(mxn, p->dk[i]);
+      if (mx < mxn || k >= kmax) {
+        stop = true;
+        rule = (k != kmax) ? 1 : 0;
+      } else {
+        for (int i = 0; i + 1 < ns; ++i) p->dk[i] = p->dk[i + 1];
+        p->dk[ns - 1] = ncc;
       }
       break;
     }
@@ -418,14 +497,21 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   AIRT_REQUIRE(o.kmax >= 0 && o.kmax < (int64_t)INT32_MAX, "kmax out of range");
   AIRT_REQUIRE(K[0] >= 0, "iteration numbers must be nonnegative");
   AIRT_REQUIRE(o.stoprule == AIRT_STOP_NONE || o.stoprule == AIRT_STOP_DP ||
-                   o.stoprule == AIRT_STOP_ME,
+                   o.stoprule == AIRT_STOP_ME || o.stoprule == AIRT_STOP_NCP,
                "The chosen stopping rule is not valid.");
+  const bool ncp = o.stoprule == AIRT_STOP_NCP;
+  if (ncp) {
+    AIRT_REQUIRE(o.ncp_rows >= 2 && o.ncp_cols >= 1 && (int64_t)o.ncp_rows * o.ncp_cols == m,
+                 "NCP: res_dims must multiply to the number of rows of A");
+    AIRT_REQUIRE(o.ncp_smooth >= 1 && o.ncp_smooth <= 4096, "NCP: ncp_smooth must be in 1..4096");
+  }
   AIRT_REQUIRE(o.relax_kind >= AIRT_RELAX_CONST && o.relax_kind <= AIRT_RELAX_TABLE,
                "invalid relaxation strategy");
   AIRT_REQUIRE(o.relax_kind != AIRT_RELAX_TABLE || o.relax_table || o.kmax == 0,
                "relax_table required");
   const int64_t kmax = o.kmax;
-  const bool me = o.stoprule == AIRT_STOP_ME;
+  // NCP needs the residual itself: the ME variant of the forward kernel keeps it
+  const bool me = o.stoprule == AIRT_STOP_ME || ncp;
 
   cudaEvent_t t0, t1;
   AIRT_CHECK_CUDA(cudaEventCreate(&t0));
@@ -496,7 +582,31 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   prm.relax_table = P.table.p;
   prm.resn_hist = P.resn.p;
   prm.lam_hist = P.lamh.p;
+  int ncp_q = 0;
+  if (ncp) {
+    const int L = o.ncp_rows;
+    ncp_q = L / 2;
+    if (P.ncp_len != L) {
+      std::vector<double> tw(2 * (size_t)L);
+      const double two_pi = 6.283185307179586476925286766559;
+      for (int k = 0; k < L; ++k) {
+        tw[2 * k] = std::cos(two_pi * k / L);
+        tw[2 * k + 1] = std::sin(two_pi * k / L);
+      }
+      P.ncp_tw.upload(tw.data(), tw.size(), s);
+      P.ncp_len = L;
+    }
+    P.ncp_pk.ensure((size_t)o.ncp_cols * ncp_q);
+    P.ncp_col.ensure(o.ncp_cols);
+    const std::vector<double> dk0(o.ncp_smooth, INFINITY);
+    P.ncp_dk.upload(dk0.data(), dk0.size(), s);
+    prm.ncc_col = P.ncp_col.p;
+    prm.dk = P.ncp_dk.p;
+    prm.ncp_cols = o.ncp_cols;
+    prm.ncp_smooth = o.ncp_smooth;
+  }
   P.params.upload(&prm, 1, s);
+
 
   FwdOut fo{d_b, P.M.p, P.mr32.p, me ? P.rprev.p : nullptr, P.state.p};
   UpdArgs ua{};
@@ -515,8 +625,18 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   ua.st = P.state.p;
   ua.g64 = P.g64.p;
 
+  // forward pass, and with NCP the periodogram of the new residual
+  auto fwd = [&]() {
+    launch_fwd(P, fo, me);
+    if (ncp) {
+      k_ncp_power<<<dim3(o.ncp_cols, (ncp_q + 255) / 256), 256, 0, s>>>(o.ncp_rows, ncp_q, P.rprev.p,
+                                                                      P.ncp_tw.p, P.ncp_pk.p, P.state.p);
+      k_ncp_col<<<o.ncp_cols, 256, 0, s>>>(ncp_q, P.ncp_pk.p, P.ncp_col.p, P.state.p);
+      AIRT_LAUNCH_CHECK();
+    }
+  };
   // initial residual and stop check (sirt.m:153-162)
-  launch_fwd(P, fo, me);
+  fwd();
   k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
   AIRT_LAUNCH_CHECK();
 
@@ -543,7 +663,7 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
     AIRT_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int64_t j = 0; j < chunk; ++j) {
       launch_bwd(P, ua, o.relax_kind);
-      launch_fwd(P, fo, me);
+      fwd();
       k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
     }
     const cudaError_t ec = cudaStreamEndCapture(s, &g);
@@ -560,7 +680,7 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
     } else {
       for (int64_t j = 0; j < cnt; ++j) {
         launch_bwd(P, ua, o.relax_kind);
-        launch_fwd(P, fo, me);
+        fwd();
         k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
       }
     }

@@ -86,15 +86,34 @@ def _parse(A, b, K, x0, options, caller):
                       "not the one currently specified.")
     if stype == "ME" and caller != "sirt":
         raise ValueError("Stopping rule ME is only available for SIRT methods, not ART and CART.")
+    ncp = None
     if stype == "NCP":
-        raise NotImplementedError("the NCP stopping rule is not available on the GPU path; "
-                                  "use 'DP', 'ME' or 'none'")
+        # check_inputs.m:171-209, check_stoprules.m:100-122: a 1D res_dims means the
+        # whole residual as one signal; a 2D one a column-major reshape
+        rd = np.atleast_1d(np.asarray(sr["res_dims"])).astype(np.int64)
+        if rd.size == 1:
+            rows, cols = m, 1
+        elif rd.size == 2:
+            rows, cols = int(rd[0]), int(rd[1])
+            if rows * cols != m:
+                raise ValueError("To RESHAPE the number of elements must not change.")
+        else:
+            raise ValueError("NCP stopping rule only implemented for 1D and 2D residuals, the size "
+                             "of which should be given using options.stoprule.res_dims.")
+        smooth = int(sr.get("ncp_smooth", 2))
+        if caller != "sirt":
+            raise NotImplementedError("the NCP stopping rule is available for SIRT methods; "
+                                      "ART on the GPU takes 'DP' or 'none'")
+        ncp = (rows, cols, smooth)
+    elif "ncp_smooth" in sr:
+        warnings.warn("options.stoprule.ncp_smooth given but only used by NCP stopping rule, "
+                      "not the one currently specified.")
     damp = float(options.get("damp", 0.0))
     if damp < 0:
         raise ValueError("Damping must be positive")
     verbose = int(options.get("verbose", 0) or 0)
     return dict(op=op, m=m, n=n, b=b, K=K, kmax=int(K[-1]), x0=x0, bounds=bounds, stype=stype,
-                taudelta=taudelta, damp=damp, verbose=verbose, options=options)
+                taudelta=taudelta, damp=damp, verbose=verbose, options=options, ncp=ncp)
 
 
 def _bound_fields(o, bounds):
@@ -237,6 +256,8 @@ def sirt(sirt_method, A, b, K, x0=None, options=None):
     o.relax_table = dptr(table)
     o.stoprule = _lib.STOP[c["stype"]]
     o.taudelta = c["taudelta"]
+    if c["ncp"] is not None:
+        o.ncp_rows, o.ncp_cols, o.ncp_smooth = c["ncp"]
     _bound_fields(o, c["bounds"])
     o.kmax = kmax
     X = np.zeros((n, K.size), dtype=np.float64, order="F")

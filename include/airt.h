@@ -49,6 +49,7 @@ extern "C" {
 #define AIRT_STOP_NONE 0
 #define AIRT_STOP_DP 1
 #define AIRT_STOP_ME 2
+#define AIRT_STOP_NCP 3 /* normalized cumulative periodogram, check_stoprules.m:97-150 */
 
 /* ---- relaxation strategy (auxil/calc_relaxpar.m: casel) ----------------- */
 #define AIRT_RELAX_CONST 1 /* relaxpar constant                     */
@@ -75,6 +76,10 @@ typedef struct {
     double lb, ub;            /* scalar bounds                                   */
     const double *lbv, *ubv;  /* vector bounds (n entries)                       */
     int64_t kmax;             /* maximum number of iterations (K(end))           */
+    /* NCP only (options.stoprule.res_dims / ncp_smooth, check_inputs.m:171-209):
+       the residual is reshaped column-major to ncp_rows x ncp_cols (ncp_cols = 1
+       for a 1D res_dims) and ncp_smooth values are compared.                    */
+    int ncp_rows, ncp_cols, ncp_smooth;
 } airt_sirt_opts;
 
 typedef struct {
@@ -98,7 +103,7 @@ typedef struct {
 } airt_art_opts;
 
 typedef struct {
-    int stoprule;       /* 0 max iterations, 2 DP, 3 ME (check_stoprules.m:27-31) */
+    int stoprule;       /* 0 max iterations, 1 NCP, 2 DP, 3 ME (check_stoprules.m:27-31) */
     int64_t finaliter;  /* iterations performed                                 */
     double relaxpar;    /* relaxpar of the final iteration                      */
     int64_t nsaved;     /* columns written to X                                 */

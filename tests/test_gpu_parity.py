@@ -226,6 +226,35 @@ def test_sirt_me_stop(c1):
     assert relerr(X, Xo) <= RTOL
 
 
+@pytest.mark.parametrize("method,dims,smooth", [("cimmino", "2d", 2), ("sart", "2d", 4),
+                                                ("cimmino", "1d", 2), ("drop", "2d", 3)])
+def test_sirt_ncp_stop(c1, method, dims, smooth):
+    """NCP (check_stoprules.m:97-150) on the C1 problem: res_dims = [p, nA]
+    (column-wise periodograms of the sinogram) or a scalar (the whole
+    residual as one signal); same stop iteration and iterates as the oracle."""
+    A, A_ref, b, _, _ = c1
+    rd = [91, 180] if dims == "2d" else A.m
+    opts = {"stoprule": {"type": "NCP", "res_dims": rd, "ncp_smooth": smooth}}
+    if method != "sart":
+        _, io, _ = O.sirt(method, A_ref, b, [1])
+        opts["rho"] = io["rho"]
+    Xo, io2, _ = O.sirt(method, A_ref, b, [5, 800], options=opts)
+    X, info = airt.sirt(method, A, b, [5, 800], None, opts)
+    assert io2["stoprule"] == 1
+    assert info["stoprule"] == 1 and info["finaliter"] == io2["finaliter"]
+    assert relerr(X, Xo) <= RTOL
+
+
+def test_sirt_ncp_reaches_kmax(c1):
+    """NCP with kmax below its stop: stoprule 0 at kmax, as the reference."""
+    A, A_ref, b, _, _ = c1
+    opts = {"stoprule": {"type": "NCP", "res_dims": [91, 180]}, "rho": 1.0}
+    Xo, io, _ = O.sirt("sart", A_ref, b, [7], options=opts)
+    X, info = airt.sart(A, b, [7], None, opts)
+    assert info["stoprule"] == io["stoprule"] == 0 and info["finaliter"] == 7
+    assert relerr(X, Xo) <= RTOL
+
+
 def test_sirt_dp_at_k0_returns_empty(c1):
     A, _, b, _, _ = c1
     X, info = airt.cimmino(A, b, [10], None, {"stoprule": {"type": "DP", "taudelta": 1e12}})
@@ -272,6 +301,14 @@ def test_sirt_input_errors(c1):
         airt.kaczmarz(A, b, 2, None, {"stoprule": {"type": "ME", "taudelta": 1.0}})
     with pytest.raises(ValueError, match="SIRT method not defined"):
         airt.sirt("nosuch", A, b, 5)
+    with pytest.raises(ValueError, match="res_dims must be specified"):
+        airt.cimmino(A, b, 5, None, {"stoprule": {"type": "NCP"}})
+    with pytest.raises(ValueError, match="RESHAPE"):
+        airt.cimmino(A, b, 5, None, {"stoprule": {"type": "NCP", "res_dims": [90, 180]}})
+    with pytest.raises(ValueError, match="1D and 2D"):
+        airt.cimmino(A, b, 5, None, {"stoprule": {"type": "NCP", "res_dims": [91, 90, 2]}})
+    with pytest.warns(UserWarning, match="ncp_smooth"):
+        airt.cimmino(A, b, 2, None, {"stoprule": {"type": "NONE", "ncp_smooth": 3}})
 
 
 # ------------------------------------------------------------ ART
