@@ -35,6 +35,8 @@ def _batch_signatures():
         "airt_batch_sirt_device": (C.c_int, [C.c_void_p, C.c_int, _lib._dp, C.c_void_p, _lib._dp,
                                              C.c_int64, C.c_int, C.c_double, C.c_int, C.c_double,
                                              C.c_void_p, C.c_void_p, i64p, _ip, _lib._dp]),
+        "airt_batch_nnz": (C.c_int, [C.c_void_p, i64p]),
+        "airt_batch_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
         "airt_batch_backproject": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _lib._dp]),
         "airt_batch_kaczmarz": (C.c_int, [C.c_void_p, _lib._dp, C.c_int64, C.c_double, C.c_int,
                                           C.c_double, C.c_int, C.c_double, _lib._dp, _lib._dp]),
@@ -178,6 +180,16 @@ class ParallelBatch:
                                              _lib.i64ptr(fin), rule.ctypes.data_as(_ip),
                                              C.byref(ms)))
         return {"finaliter": fin, "stoprule": rule, "relaxpar": lam, "gpu_ms": float(ms.value)}
+
+    def inst_nnz(self) -> np.ndarray:
+        """Nonzeros of every instance's matrix."""
+        out = np.zeros(self.K, np.int64)
+        check(self._L.airt_batch_nnz(self._h, _lib.i64ptr(out)))
+        return out
+
+    def apply_device(self, d_in, d_out, transp=False) -> None:
+        """y = A*x (or A'*x) of the whole block-diagonal batch, device vectors."""
+        check(self._L.airt_batch_apply(self._h, C.c_void_p(d_in), C.c_void_p(d_out), int(transp)))
 
     def backproject_device(self, method, d_b, d_x) -> float:
         """x = D .* A'(M .* b) per instance on device vectors (the first SIRT

@@ -6,16 +6,21 @@
 // matrices are generated on the GPU in one pass over every ray of every
 // instance and stored as one FP32 CSR + CSC.  An iteration is therefore a
 // handful of full-bandwidth launches over all instances:
-//   bwd (per size bucket)  x += lambda_k * D.*A'(M.*r), box clamp
-//   fwd (per size bucket)  r = b - A*x, M.*r, r.^2 per row
-//   reduce                 ||r_k||^2 per instance (one block per instance)
-//   ctrl                   per-instance DP / max-iteration rule
+//   bwd (per lane class)  x += lambda_k * D.*A'(M.*r), box clamp
+//   fwd (per lane class)  r = b - A*x, M.*r, r.^2 per row
+//   reduce                ||r_k||^2 per instance (one block per instance)
+//   ctrl                  per-instance DP / max-iteration rule
+//   tiles                 lists of the segment tiles still holding an
+//                         unstopped instance
 // Per-instance scalars (lambda, tau*delta, stop flag, iteration count) are
 // read through the row->instance and column->instance maps; stopped
-// instances skip their rows and columns entirely.  Instances of equal N are
-// contiguous "size buckets"; an autotuner times the candidate lane widths of
-// the segment kernels on every bucket once and launches each bucket with its
-// fastest width.  Kaczmarz runs one CTA per instance.
+// instances skip their rows and columns entirely.  Rows and columns are cut
+// into tiles of 2048 segments; a tile's lane class follows its mean segment
+// length (<= 16, <= 128, > 128 nonzeros), so instances of any size mix in any
+// order still give at most three launches per direction.  An autotuner times
+// the candidate lane widths on every class once.  A chunk of iterations is
+// captured as one CUDA graph (all loop state lives in device memory).
+// Kaczmarz runs one CTA per instance.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -34,34 +39,39 @@ struct InstGeom {
   int64_t col0;  // first global column
 };
 
-struct Bucket {
-  int k0, k1;          // instances
-  int64_t r0, r1;      // rows
-  int64_t c0, c1;      // columns
-  int lanes_fwd = 8, lanes_bwd = 8;
-  int idx = 0;                 // position in Batch::buckets
-  int rt_off = 0, ct_off = 0;  // first row / column tile in Batch::rtiles / ctiles
-  int nrt = 0, nct = 0;        // row / column tiles of the bucket
+// Segment tiles of the active-tile lists: 2048 rows or columns, in
+// kClasses lane classes by mean segment length.
+constexpr int kTileShift = 11;
+constexpr int kClasses = 3;
+
+// Per-direction tile bookkeeping: class of every tile, tiles per class, and
+// the region of each class in the active list.
+struct TileSet {
+  int ntiles = 0;
+  DevBuf<int> cls, list;
+  int count[kClasses] = {0, 0, 0};
+  int off[kClasses] = {0, 0, 0};
+  int lanes[kClasses] = {2, 4, 8};
 };
 
-// Segment tiles of the active-tile lists: 2048 rows or columns.
-constexpr int kTileShift = 11;
+struct ClassOffsets {
+  int off[kClasses];
+};
 
 struct Batch {
   Problem P;                 // block-diagonal CSR/CSC and work vectors
   int ninst = 0;
   std::vector<InstGeom> hg;
   std::vector<int64_t> row_off, col_off;
-  std::vector<Bucket> buckets;
+  TileSet rt, ct;  // row (CSR) and column (CSC) tiles
   DevBuf<InstGeom> g;
   DevBuf<int64_t> d_row_off, d_col_off;
   DevBuf<int> inst_row, inst_col, stop, iters, rule;
   DevBuf<double> rsq, nrm2, lam, taud, resn_last;
   bool tuned = false;
-  // tiles of each bucket holding at least one instance that has not stopped,
-  // rebuilt after every stop-rule update; tcount[b] / tcount[nb + b] count
-  // bucket b's listed row / column tiles
-  DevBuf<int> rtiles, ctiles, tcount;
+  // active tiles per class, rebuilt after every stop-rule update:
+  // tcount[c] row tiles, tcount[kClasses + c] column tiles of class c
+  DevBuf<int> tcount;
   int wmethod = -1;  // method whose M and D are in P.M / P.D (the matrix never changes)
 };
 
@@ -205,19 +215,33 @@ __global__ void __launch_bounds__(256, 4)
       });
 }
 
-// List the tiles of segments [seg0, seg0 + nseg) (tile t: seg0 + t*2^shift
-// ..) that hold at least one instance with stop == 0; inst_of maps a segment
-// to its instance (instances are contiguous, so a tile spans inst_of[first]
-// .. inst_of[last]).  *count must start at zero; list order is arbitrary.
-__global__ void k_active_tiles(int ntiles, int64_t seg0, int64_t nseg, const int *__restrict__ inst_of,
-                               const int *__restrict__ stop, int *__restrict__ list, int *__restrict__ count) {
+// Class of every tile of segments [0, nseg): its mean segment length from
+// the pointer array.
+__global__ void k_tile_class(int ntiles, int64_t nseg, const int64_t *__restrict__ ptr, int *__restrict__ cls) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
-  const int64_t s0 = seg0 + ((int64_t)t << kTileShift);
-  const int64_t s1 = min(seg0 + nseg, s0 + ((int64_t)1 << kTileShift));
+  const int64_t s0 = (int64_t)t << kTileShift;
+  const int64_t s1 = min(nseg, s0 + ((int64_t)1 << kTileShift));
+  const double avg = (double)(ptr[s1] - ptr[s0]) / (double)(s1 - s0);
+  cls[t] = avg > 128.0 ? 2 : avg > 16.0 ? 1 : 0;
+}
+
+// List the tiles (2^kTileShift segments each) that hold at least one
+// instance with stop == 0, in the region of the tile's class; inst_of maps a
+// segment to its instance (instances are contiguous, so a tile spans
+// inst_of[first] .. inst_of[last]).  count[] must start at zero; the order
+// within a class is arbitrary.
+__global__ void k_active_tiles(int ntiles, int64_t nseg, const int *__restrict__ inst_of,
+                               const int *__restrict__ stop, const int *__restrict__ cls, ClassOffsets co,
+                               int *__restrict__ list, int *__restrict__ count) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int64_t s0 = (int64_t)t << kTileShift;
+  const int64_t s1 = min(nseg, s0 + ((int64_t)1 << kTileShift));
   for (int k = inst_of[s0]; k <= inst_of[s1 - 1]; ++k)
     if (!stop[k]) {
-      list[atomicAdd(count, 1)] = t;
+      const int c = cls[t];
+      list[co.off[c] + atomicAdd(count + c, 1)] = t;
       return;
     }
 }
@@ -328,16 +352,19 @@ float time_launch(cudaStream_t s, F &&f, int reps = 3) {
   return ms / reps;
 }
 
-void launch_bfwd(Batch &B, const Bucket &bk, int L, const BFwd &o, const float *x32 = nullptr) {
+// Launch class c of the forward / transpose kernel with L lanes per
+// segment; the grid covers every tile of the class (graph-capturable), the
+// kernel walks only the listed ones.
+void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullptr) {
   Problem &P = B.P;
   if (!x32) x32 = P.x32.p;
+  if (B.rt.count[c] == 0) return;
   cudaStream_t s = P.stream;
-  const int64_t ns = bk.r1 - bk.r0;
-  if (ns <= 0) return;
-  const unsigned g = grid_for(ns * L, 256, 4);
+  const int64_t ns = P.m;
+  const unsigned g = grid_for((int64_t)B.rt.count[c] * (1 << kTileShift) * L, 256, 4);
+  const int *tl = B.rt.list.p + B.rt.off[c], *cnt = B.tcount.p + c;
   switch (L) {
-#define AIRT_F(LV) \
-  k_batch_fwd<LV><<<g, 256, 0, s>>>(ns, B.rtiles.p + bk.rt_off, B.tcount.p + bk.idx, P.rp.p, P.ci.p, P.rv.p, x32, o)
+#define AIRT_F(LV) k_batch_fwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.rp.p, P.ci.p, P.rv.p, x32, o)
     case 16: AIRT_F(16); break;
     case 8: AIRT_F(8); break;
     case 4: AIRT_F(4); break;
@@ -346,17 +373,16 @@ void launch_bfwd(Batch &B, const Bucket &bk, int L, const BFwd &o, const float *
   }
 }
 
-void launch_bbwd(Batch &B, const Bucket &bk, int L, const BUpd &u, const float *mr32 = nullptr) {
+void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = nullptr) {
   Problem &P = B.P;
   if (!mr32) mr32 = P.mr32.p;
+  if (B.ct.count[c] == 0) return;
   cudaStream_t s = P.stream;
-  const int64_t ns = bk.c1 - bk.c0;
-  if (ns <= 0) return;
-  const unsigned g = grid_for(ns * L, 256, 4);
+  const int64_t ns = P.n;
+  const unsigned g = grid_for((int64_t)B.ct.count[c] * (1 << kTileShift) * L, 256, 4);
+  const int *tl = B.ct.list.p + B.ct.off[c], *cnt = B.tcount.p + kClasses + c;
   switch (L) {
-#define AIRT_B(LV)                                                                                      \
-  k_batch_bwd<LV><<<g, 256, 0, s>>>(ns, B.ctiles.p + bk.ct_off, B.tcount.p + B.buckets.size() + bk.idx, \
-                                    P.cp.p, P.ri.p, P.cv.p, mr32, u)
+#define AIRT_B(LV) k_batch_bwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.cp.p, P.ri.p, P.cv.p, mr32, u)
     case 16: AIRT_B(16); break;
     case 8: AIRT_B(8); break;
     case 4: AIRT_B(4); break;
@@ -365,21 +391,50 @@ void launch_bbwd(Batch &B, const Bucket &bk, int L, const BUpd &u, const float *
   }
 }
 
-// Rebuild every bucket's active row and column tile lists from stop[].
+void fwd_classes(Batch &B, const BFwd &o) {
+  for (int c = 0; c < kClasses; ++c) launch_bfwd(B, c, B.rt.lanes[c], o);
+}
+
+void bwd_classes(Batch &B, const BUpd &u) {
+  for (int c = 0; c < kClasses; ++c) launch_bbwd(B, c, B.ct.lanes[c], u);
+}
+
+// Rebuild the active row and column tile lists from stop[].
 void build_tiles(Batch &B, const int *stop) {
   Problem &P = B.P;
   cudaStream_t s = P.stream;
-  const int nb = (int)B.buckets.size();
-  AIRT_CHECK_CUDA(cudaMemsetAsync(B.tcount.p, 0, 2 * nb * sizeof(int), s));
-  for (const Bucket &bk : B.buckets) {
-    if (bk.nrt > 0)
-      k_active_tiles<<<(bk.nrt + 127) / 128, 128, 0, s>>>(bk.nrt, bk.r0, bk.r1 - bk.r0, B.inst_row.p, stop,
-                                                          B.rtiles.p + bk.rt_off, B.tcount.p + bk.idx);
-    if (bk.nct > 0)
-      k_active_tiles<<<(bk.nct + 127) / 128, 128, 0, s>>>(bk.nct, bk.c0, bk.c1 - bk.c0, B.inst_col.p, stop,
-                                                          B.ctiles.p + bk.ct_off, B.tcount.p + nb + bk.idx);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(B.tcount.p, 0, 2 * kClasses * sizeof(int), s));
+  ClassOffsets ro, co;
+  for (int c = 0; c < kClasses; ++c) {
+    ro.off[c] = B.rt.off[c];
+    co.off[c] = B.ct.off[c];
   }
+  k_active_tiles<<<(B.rt.ntiles + 127) / 128, 128, 0, s>>>(B.rt.ntiles, P.m, B.inst_row.p, stop, B.rt.cls.p, ro,
+                                                           B.rt.list.p, B.tcount.p);
+  k_active_tiles<<<(B.ct.ntiles + 127) / 128, 128, 0, s>>>(B.ct.ntiles, P.n, B.inst_col.p, stop, B.ct.cls.p, co,
+                                                           B.ct.list.p, B.tcount.p + kClasses);
   AIRT_LAUNCH_CHECK();
+}
+
+// Tiles of one direction: classes on the device, counts and list regions on
+// the host.
+void setup_tileset(TileSet &T, int64_t nseg, const int64_t *ptr, cudaStream_t s) {
+  T.ntiles = (int)((nseg + (1 << kTileShift) - 1) >> kTileShift);
+  T.cls.ensure(T.ntiles > 0 ? T.ntiles : 1);
+  T.list.ensure(T.ntiles > 0 ? T.ntiles : 1);
+  for (int c = 0; c < kClasses; ++c) T.count[c] = 0;
+  if (T.ntiles == 0) return;
+  k_tile_class<<<(T.ntiles + 127) / 128, 128, 0, s>>>(T.ntiles, nseg, ptr, T.cls.p);
+  AIRT_LAUNCH_CHECK();
+  std::vector<int> h(T.ntiles);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(h.data(), T.cls.p, T.ntiles * sizeof(int), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  for (int v : h) ++T.count[v];
+  int off = 0;
+  for (int c = 0; c < kClasses; ++c) {
+    T.off[c] = off;
+    off += T.count[c];
+  }
 }
 
 }  // namespace
@@ -422,35 +477,6 @@ Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const d
     B->g.upload(B->hg.data(), ninst, s);
     B->d_row_off.upload(B->row_off.data(), ninst + 1, s);
     B->d_col_off.upload(B->col_off.data(), ninst + 1, s);
-    // size buckets: maximal runs of equal N
-    for (int k = 0; k < ninst;) {
-      int e = k + 1;
-      while (e < ninst && N[e] == N[k]) ++e;
-      Bucket bk;
-      bk.k0 = k;
-      bk.k1 = e;
-      bk.r0 = B->row_off[k];
-      bk.r1 = B->row_off[e];
-      bk.c0 = B->col_off[k];
-      bk.c1 = B->col_off[e];
-      bk.idx = (int)B->buckets.size();
-      B->buckets.push_back(bk);
-      k = e;
-    }
-    {
-      int rt = 0, ct = 0;
-      for (Bucket &bk : B->buckets) {
-        bk.nrt = (int)((bk.r1 - bk.r0 + (1 << kTileShift) - 1) >> kTileShift);
-        bk.nct = (int)((bk.c1 - bk.c0 + (1 << kTileShift) - 1) >> kTileShift);
-        bk.rt_off = rt;
-        bk.ct_off = ct;
-        rt += bk.nrt;
-        ct += bk.nct;
-      }
-      B->rtiles.ensure(rt > 0 ? rt : 1);
-      B->ctiles.ensure(ct > 0 ? ct : 1);
-      B->tcount.ensure(2 * B->buckets.size());
-    }
     // generation: count, scan, fill, transpose (as generate_matrix)
     DevBuf<int64_t> counts;
     DevBuf<int> bad;
@@ -483,6 +509,9 @@ Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const d
     k_fill_inst<<<grid_for(P.m, 256), 256, 0, s>>>(ninst, B->d_row_off.p, P.m, B->inst_row.p);
     k_fill_inst<<<grid_for(P.n, 256), 256, 0, s>>>(ninst, B->d_col_off.p, P.n, B->inst_col.p);
     AIRT_LAUNCH_CHECK();
+    setup_tileset(B->rt, P.m, P.rp.p, s);
+    setup_tileset(B->ct, P.n, P.cp.p, s);
+    B->tcount.ensure(2 * kClasses);
     AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
     if (B->P.stream) cudaStreamSynchronize(B->P.stream);
@@ -606,22 +635,26 @@ void batch_tune(Batch &B) {
   mtmp.ensure(P.m);
   x32tmp.ensure(P.n);
   const int cands[4] = {2, 4, 8, 16};
-  for (Bucket &bk : B.buckets) {
+  for (int c = 0; c < kClasses; ++c) {
     float best_f = 1e30f, best_b = 1e30f;
     for (int L : cands) {
-      BFwd o{zero.p, zero.p, mtmp.p, yr.p, B.inst_row.p, nostop.p, bk.r0};
-      const float tf = time_launch(s, [&] { launch_bfwd(B, bk, L, o, xc.p); });
-      BUpd u{zero.p, zero.p, xtmp.p, x32tmp.p, B.inst_col.p, nostop.p, 0, 0, 0.0, 0.0, bk.c0};
-      const float tb = time_launch(s, [&] { launch_bbwd(B, bk, L, u, xr.p); });
+      if (B.rt.count[c] > 0) {
+        BFwd o{zero.p, zero.p, mtmp.p, yr.p, B.inst_row.p, nostop.p, 0};
+        const float tf = time_launch(s, [&] { launch_bfwd(B, c, L, o, xc.p); });
+        if (tf < best_f) {
+          best_f = tf;
+          B.rt.lanes[c] = L;
+        }
+      }
+      if (B.ct.count[c] > 0) {
+        BUpd u{zero.p, zero.p, xtmp.p, x32tmp.p, B.inst_col.p, nostop.p, 0, 0, 0.0, 0.0, 0};
+        const float tb = time_launch(s, [&] { launch_bbwd(B, c, L, u, xr.p); });
+        if (tb < best_b) {
+          best_b = tb;
+          B.ct.lanes[c] = L;
+        }
+      }
       AIRT_LAUNCH_CHECK();
-      if (tf < best_f) {
-        best_f = tf;
-        bk.lanes_fwd = L;
-      }
-      if (tb < best_b) {
-        best_b = tb;
-        bk.lanes_bwd = L;
-      }
     }
   }
   B.tuned = true;
@@ -664,37 +697,46 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
   BFwd fo{d_b, P.M.p, P.mr32.p, B.rsq.p, B.inst_row.p, B.stop.p, 0};
   BUpd uo{P.D.p, B.lam.p, P.x64.p, P.x32.p, B.inst_col.p, B.stop.p, lbk, ubk, lb, ub, 0};
   const double *taud = taud_host ? B.taud.p : nullptr;
-  auto fwd_all = [&]() {
-    for (const Bucket &bk : B.buckets) {
-      BFwd o = fo;
-      o.r0 = bk.r0;
-      launch_bfwd(B, bk, bk.lanes_fwd, o);
-    }
+  const unsigned gk = (unsigned)((K + 127) / 128);
+  auto fwd_reduce = [&]() {
+    fwd_classes(B, fo);
     k_batch_reduce<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, B.stop.p, B.nrm2.p);
   };
-  auto bwd_all = [&]() {
-    for (const Bucket &bk : B.buckets) {
-      BUpd u = uo;
-      u.c0 = bk.c0;
-      launch_bbwd(B, bk, bk.lanes_bwd, u);
-    }
+  auto iteration = [&]() {
+    bwd_classes(B, uo);
+    fwd_reduce();
+    k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
+                                    B.resn_last.p);
+    build_tiles(B, B.stop.p);
   };
-  const unsigned gk = (unsigned)((K + 127) / 128);
-  fwd_all();
+  fwd_reduce();
   k_batch_ctrl<<<gk, 128, 0, s>>>(K, 1, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
                                   B.resn_last.p);
   AIRT_LAUNCH_CHECK();
   build_tiles(B, B.stop.p);
-  std::vector<int> hstop(K);
+  // A chunk of iterations is captured once as a CUDA graph and replayed:
+  // every argument is fixed for the solve and the loop state lives in device
+  // memory.  The host reads the stop flags after each chunk.
   const int64_t chunk = 8;
+  cudaGraphExec_t gexec = nullptr;
+  if (kmax >= chunk) {
+    cudaGraph_t g = nullptr;
+    AIRT_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int64_t j = 0; j < chunk; ++j) iteration();
+    const cudaError_t ec = cudaStreamEndCapture(s, &g);
+    if (ec == cudaSuccess && g) {
+      if (cudaGraphInstantiate(&gexec, g, 0) != cudaSuccess) gexec = nullptr;
+      cudaGraphDestroy(g);
+    }
+    cudaGetLastError();
+  }
+  std::vector<int> hstop(K);
   for (int64_t it = 1; it <= kmax;) {
     const int64_t cnt = std::min<int64_t>(chunk, kmax - it + 1);
-    for (int64_t j = 0; j < cnt; ++j) {
-      bwd_all();
-      fwd_all();
-      k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
-                                      B.resn_last.p);
-      build_tiles(B, B.stop.p);
+    if (cnt == chunk && gexec) {
+      AIRT_CHECK_CUDA(cudaGraphLaunch(gexec, s));
+    } else {
+      for (int64_t j = 0; j < cnt; ++j) iteration();
     }
     AIRT_LAUNCH_CHECK();
     it += cnt;
@@ -705,6 +747,7 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
     for (int k = 0; k < K && all; ++k) all = hstop[k] != 0;
     if (all) break;
   }
+  if (gexec) cudaGraphExecDestroy(gexec);
   AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
   AIRT_CHECK_CUDA(cudaMemcpyAsync(d_x, P.x64.p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   std::vector<int> hit(K), hrule(K);
@@ -748,11 +791,7 @@ void batch_backproject(Batch &B, int method, const double *d_b, double *d_x, dou
   k_batch_mb<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, P.M.p, d_b, P.mr32.p);
   AIRT_LAUNCH_CHECK();
   BUpd uo{P.D.p, B.lam.p, P.x64.p, P.x32.p, B.inst_col.p, B.stop.p, 0, 0, 0.0, 0.0, 0};
-  for (const Bucket &bk : B.buckets) {
-    BUpd u = uo;
-    u.c0 = bk.c0;
-    launch_bbwd(B, bk, bk.lanes_bwd, u);
-  }
+  bwd_classes(B, uo);
   AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
   AIRT_CHECK_CUDA(cudaMemcpyAsync(d_x, P.x64.p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));

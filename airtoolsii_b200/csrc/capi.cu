@@ -6,6 +6,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace airt {
@@ -403,6 +405,29 @@ int airt_batch_sirt(airt_batch *h, int method, const double *relaxpar, const dou
   batch_sirt(B, method, relaxpar, P.b64.p, taudelta, kmax, lb_kind, lb, ub_kind, ub,
              x0 ? P.vin.p : nullptr, P.Xd.p, finaliter, stoprule, gpu_ms);
   AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P.Xd.p, P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  AIRT_API_END
+}
+
+int airt_batch_nnz(const airt_batch *h, int64_t *nnz) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && nnz, "null pointer argument");
+  Batch &B = *reinterpret_cast<Batch *>(const_cast<airt_batch *>(h));
+  Problem &P = batch_problem(B);
+  const int K = batch_ninst(B);
+  const int64_t *roff = batch_row_off(B);
+  std::vector<int64_t> ptr(K + 1);
+  for (int k = 0; k <= K; ++k)
+    AIRT_CHECK_CUDA(cudaMemcpy(&ptr[k], P.rp.p + roff[k], sizeof(int64_t), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < K; ++k) nnz[k] = ptr[k + 1] - ptr[k];
+  AIRT_API_END
+}
+
+int airt_batch_apply(airt_batch *h, const double *d_in, double *d_out, int transp) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && d_in && d_out, "null pointer argument");
+  Problem &P = batch_problem(*reinterpret_cast<Batch *>(h));
+  apply_operator(P, d_in, d_out, transp);
   AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
   AIRT_API_END
 }

@@ -197,6 +197,11 @@ int airt_batch_sirt_device(airt_batch *h, int method, const double *relaxpar, co
                            const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
                            double ub, const double *d_x0, double *d_x, int64_t *finaliter,
                            int *stoprule, double *gpu_ms);
+/* Nonzeros of each instance's matrix (ninst entries). */
+int airt_batch_nnz(const airt_batch *h, int64_t *nnz);
+/* The batch's operator (afun of the block-diagonal system, afun_matrix.m:44-53):
+ * y = A*x (transp = 0) or y = A'*x (transp = 1) on device vectors. */
+int airt_batch_apply(airt_batch *h, const double *d_in, double *d_out, int transp);
 /* x = D .* A'(M .* b) per instance with the weights of `method` (device
  * vectors): the first iterate of sirt (sirt/sirt.m:229) from x0 = 0
  * with relaxpar 1 and no bounds, computed with one transpose pass. */

@@ -38,6 +38,7 @@ def batch():
 def test_batch_layout(batch):
     B, mats, *_ = batch
     assert B.K == len(mats)
+    assert list(B.inst_nnz()) == [A.nnz for A in mats]
     for k, A in enumerate(mats):
         assert B.row_off[k + 1] - B.row_off[k] == A.shape[0]
         assert B.col_off[k + 1] - B.col_off[k] == A.shape[1]
@@ -103,3 +104,23 @@ def test_batch_backproject_is_first_sirt_iterate(batch, method):
             assert np.array_equal(got[k], xs[k])
             Xo, _, _ = O.sirt(method, A, bs[k], [1], options={"relaxpar": 1.0})
             assert relerr(got[k], Xo[:, -1]) <= RTOL
+
+
+def test_batch_apply_matches_instances(batch):
+    import torch
+    B, mats, _, _, xs = batch
+    x = np.concatenate(xs)
+    y = np.concatenate([rng_vec(A.shape[0], k) for k, A in enumerate(mats)])
+    dx, dy = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    out_f = torch.empty(B.m, dtype=torch.float64, device="cuda")
+    out_t = torch.empty(B.n, dtype=torch.float64, device="cuda")
+    B.apply_device(dx.data_ptr(), out_f.data_ptr(), False)
+    B.apply_device(dy.data_ptr(), out_t.data_ptr(), True)
+    f, t = B.split_rows(out_f.cpu().numpy()), B.split_cols(out_t.cpu().numpy())
+    for k, A in enumerate(mats):
+        assert relerr(f[k], A @ xs[k]) <= 1e-6
+        assert relerr(t[k], A.T @ B.split_rows(y)[k]) <= 1e-6
+
+
+def rng_vec(n, seed):
+    return np.random.default_rng(900 + seed).standard_normal(n)
