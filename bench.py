@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--small", action="store_true", help="N=256 problem (profiling captures)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start time-to-DP leg")
+    ap.add_argument("--no-extra", action="store_true", help="skip the C2-methods / C3 / C4 legs")
     ap.add_argument("--warm-heldout", type=int, default=1000, help="held-out seeds of the time-to-DP leg")
     ap.add_argument("--warm-batch", type=int, default=250, help="instances per batched solve")
     return ap.parse_args()
@@ -128,6 +129,123 @@ def cpu_leg(A_csc, b, M, D, lam, iters, m, n, nnz):
             "cores": cbind.num_threads(), "kind": "port",
             "sample": f"{iters} cimmino iterations of the same problem, FP64 CSR+CSC "
                       f"(C restatement, OpenMP), {dt:.2f} s"}
+
+
+def _sync_s():
+    import torch
+    torch.cuda.synchronize()
+    return time.perf_counter()
+
+
+def extra_legs(A_c2, b_c2, wl):
+    """The other workloads of the hot path, each timed once after an untimed
+    pass (device times from the solvers' CUDA events):
+
+    * C2 methods: paralleltomo N=512, 360 angles x 724 rays, cimmino / cav /
+      drop / sart, 200 iterations, box [0,1], on the stored FP32 CSR+CSC and
+      on the matrix-free projector (rays traced on the fly every product).
+      GB/s uses the CSR+CSC byte model (CSR-equivalent for matrix-free);
+      rays/s counts the 2m rays traced per matrix-free iteration.
+    * C3 fan: fanlineartomo N=1024, 720 angles over 360 deg, 1448 detectors,
+      source at 2N, matrix-free, 10-ellipse phantom, 1% noise, SART to the DP
+      stop (tau = 1.02).
+    * C3 ART: paralleltomo N=256, 180 angles, kaczmarz and symkaczmarz, 20
+      sweeps, lbound 0.
+    * C4: 512 instances, N uniform in {64,96,128,192,256}, 30-180 angles,
+      1-3% noise (seeded), one block-diagonal batch; cimmino and drop to the
+      per-instance DP stop (tau = 1.02, kmax 2000); Kaczmarz 5 sweeps, one
+      CTA per instance."""
+    import torch
+    import airtoolsii_b200 as airt
+    from airtoolsii_b200.batch import ParallelBatch
+    out = {}
+    m, n, nnz = A_c2.m, A_c2.n, A_c2.nnz
+    theta = np.arange(wl["nA"]) * wl["step"]
+    Amf, *_ = airt.paralleltomo(wl["N"], theta, wl["p"], None, 0, 0)
+    rows = []
+    for kind, op in (("stored", A_c2), ("matrix_free", Amf)):
+        for meth in ("cimmino", "cav", "drop", "sart"):
+            opts = {"lbound": 0.0, "ubound": 1.0}
+            airt.sirt(meth, op, b_c2, [2], None, opts)
+            t0 = _sync_s()
+            X, info = airt.sirt(meth, op, b_c2, [200], None, opts)
+            t1 = _sync_s()
+            ms_it = info["gpu_ms"] / 200
+            row = {"storage": kind, "method": meth, "iterations": 200,
+                   "ms_per_iteration": round(ms_it, 4), "wall_s": round(t1 - t0, 3),
+                   "GBps_model": round(model_bytes(nnz, m, n) / (ms_it / 1e3) / 1e9, 1)}
+            if kind == "matrix_free":
+                row["rays_per_s"] = round(2 * m / (ms_it / 1e3), 0)
+            rows.append(row)
+    out["c2_methods"] = rows
+    del Amf
+    # C3 fan, matrix-free SART to DP
+    theta = np.arange(720) * 0.5
+    Af, *_ = airt.fanlineartomo(1024, theta, 1448, 2.0, None, None, 0, 0)
+    xf = airt.random_ellipses(1024, 10, seed=300)
+    bf, ef = airt.add_noise(Af(xf, "notransp"), 0.01, seed=301)
+    opts = {"stoprule": {"type": "DP", "taudelta": 1.02 * ef}}
+    airt.sart(Af, bf, [2], None, opts)
+    t0 = _sync_s()
+    X, info = airt.sart(Af, bf, [1000], None, opts)
+    t1 = _sync_s()
+    it = int(info["finaliter"])
+    out["c3_fan_sart_dp"] = {
+        "workload": "fanlineartomo N=1024, 720 angles / 360 deg, 1448 detectors, R=2N, matrix-free",
+        "finaliter": it, "stoprule": int(info["stoprule"]), "wall_s": round(t1 - t0, 3),
+        "gpu_ms": round(info["gpu_ms"], 2), "rays_per_s": round(2 * Af.m * it / (info["gpu_ms"] / 1e3), 0),
+        "relerr": round(float(np.linalg.norm(X[:, -1] - xf) / np.linalg.norm(xf)), 5)}
+    del Af
+    # C3 ART
+    Aa, *_ = airt.paralleltomo(256, np.arange(180.0))
+    xa = airt.random_ellipses(256, 10, seed=31)
+    ba, _ = airt.add_noise(Aa(xa, "notransp"), 0.01, seed=32)
+    art = {}
+    for meth in ("kaczmarz", "symkaczmarz"):
+        getattr(airt, meth)(Aa, ba, [2], None, {"lbound": 0.0})
+        X, info = getattr(airt, meth)(Aa, ba, [20], None, {"lbound": 0.0})
+        ms = info["gpu_ms"] / 20
+        art[meth] = {"sweeps": 20, "ms_per_sweep": round(ms, 4),
+                     "GBps_model": round((8 * Aa.nnz + 16 * Aa.m) / (ms / 1e3) / 1e9, 1)}
+    out["c3_art_n256"] = art
+    del Aa
+    # C4 batch
+    rng = np.random.default_rng(4)
+    K = 512
+    Ns = rng.choice([64, 96, 128, 192, 256], K)
+    nAs = rng.integers(30, 181, K)
+    etas = rng.uniform(0.005, 0.03, K)
+    t0 = _sync_s()
+    B = ParallelBatch(list(Ns), [np.arange(a) * (180.0 / a) for a in nAs])
+    t_build = _sync_s() - t0
+    xs = [airt.random_ellipses(int(N), 10, seed=10_000 + k) for k, N in enumerate(Ns)]
+    dx = torch.from_numpy(np.concatenate(xs)).cuda()
+    db0 = torch.empty(B.m, dtype=torch.float64, device="cuda")
+    B.apply_device(dx.data_ptr(), db0.data_ptr())
+    b0 = B.split_rows(db0.cpu().numpy())
+    bs, tds = [], []
+    for k in range(K):
+        bk, ek = airt.add_noise(b0[k], float(etas[k]), seed=20_000 + k)
+        bs.append(bk)
+        tds.append(1.02 * ek)
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dxo = torch.empty(B.n, dtype=torch.float64, device="cuda")
+    nz = B.inst_nnz()
+    mi, ni = np.diff(B.row_off), np.diff(B.col_off)
+    c4 = {"instances": K, "nnz": int(B.nnz), "build_s": round(t_build, 3)}
+    for meth in ("cimmino", "drop"):
+        rho = B.rho(meth)
+        B.sirt_device(meth, db.data_ptr(), dxo.data_ptr(), 2000, taudelta=np.array(tds), rho=rho)
+        info = B.sirt_device(meth, db.data_ptr(), dxo.data_ptr(), 2000, taudelta=np.array(tds), rho=rho)
+        its = info["finaliter"]
+        byts = float(np.sum(its * (16 * nz + 16 * mi + 16 * ni)))
+        c4[meth] = {"gpu_ms": round(info["gpu_ms"], 2), "iters_mean": round(float(its.mean()), 2),
+                    "iters_max": int(its.max()), "dp_stopped": int(np.sum(info["stoprule"] == 2)),
+                    "GBps_model": round(byts / (info["gpu_ms"] / 1e3) / 1e9, 1)}
+    _, ik = B.kaczmarz(np.concatenate(bs), 5)
+    c4["kaczmarz_5_sweeps_ms"] = round(ik["gpu_ms"], 2)
+    out["c4_batch"] = c4
+    return out
 
 
 def warm_leg(a):
@@ -363,6 +481,8 @@ def main():
             M, D = A.weights(a.method)
             line["cpu_baseline"] = cpu_leg(A.to_scipy(), b, M, D, lam, 5 if not a.small else 20,
                                            m, n, nnz)
+        if not a.no_extra and world == 1:
+            line["workloads"] = extra_legs(A, b, wl)
         if not a.no_warm and world == 1:
             line["time_to_dp"] = warm_leg(a)
         print(json.dumps(line), flush=True)

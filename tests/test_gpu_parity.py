@@ -380,3 +380,35 @@ def test_art_dp_stop_c3_sized():
     assert info["finaliter"] == io["finaliter"] and info["stoprule"] == io["stoprule"]
     for k in range(X.shape[1]):
         assert relerr(X[:, k], Xo[:, k]) <= RTOL
+
+
+@pytest.fixture(scope="module")
+def c3art():
+    """C3-ART: paralleltomo N=256, 180 angles, p=362 (m=65,160, n=65,536), a
+    10-ellipse phantom with 1% noise; the FP64 CSR from the C tracer."""
+    theta = np.arange(180.0)
+    th, p, d, ct, st, off = O.parallel_geometry(256, theta, None)
+    rows, cols, vals = cbind.trace_coo(256, list(O.parallel_rays(256, ct, st, off)), True)
+    Rm = O.coo_to_csc(rows, cols, vals, len(th) * p, 256 * 256).tocsr()
+    A, *_ = airt.paralleltomo(256, theta)
+    x = airt.random_ellipses(256, 10, seed=31)
+    b, _ = airt.add_noise(Rm @ x, 0.01, seed=32)
+    nrm = np.asarray(Rm.multiply(Rm).sum(axis=1)).ravel()
+    return A, Rm, b, nrm
+
+
+@pytest.mark.parametrize("method", ["kaczmarz", "symkaczmarz"])
+def test_art_c3_sized_iterate_by_iterate(c3art, method):
+    """20 sweeps of kaczmarz / symkaczmarz (art.m:188-191 row orders, the
+    last row of the symmetric sweep applied twice) against the C oracle,
+    every sweep's iterate within 1e-5."""
+    A, Rm, b, nrm = c3art
+    I = np.flatnonzero(nrm > 0)
+    order = I if method == "kaczmarz" else np.concatenate([I, I[::-1]])
+    K = list(range(1, 21)) if method == "kaczmarz" else list(range(2, 21, 2))
+    X, info = getattr(airt, method)(A, b, K, None, {"lbound": 0.0})
+    assert info["finaliter"] == 20 and X.shape[1] == len(K)
+    x = np.zeros(A.n)
+    for j in range(len(K)):
+        x = cbind.kaczmarz(Rm, b, nrm, order, 1.0, 0.0, None, 1, x0=x)
+        assert relerr(X[:, j], x) <= RTOL, (method, K[j], relerr(X[:, j], x))
