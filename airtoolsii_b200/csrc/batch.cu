@@ -20,7 +20,8 @@
 // order still give at most three launches per direction.  An autotuner times
 // the candidate lane widths on every class once.  A chunk of iterations is
 // captured as one CUDA graph (all loop state lives in device memory).
-// Kaczmarz runs one CTA per instance.
+// Kaczmarz runs one CTA per instance over a level schedule of the
+// instance's row order, built on the device once per batch.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -73,6 +74,11 @@ struct Batch {
   // tcount[c] row tiles, tcount[kClasses + c] column tiles of class c
   DevBuf<int> tcount;
   int wmethod = -1;  // method whose M and D are in P.M / P.D (the matrix never changes)
+  // Kaczmarz level schedules (built on first use): per instance k, levels
+  // kz_lev_ptr[base_k .. base_k + kz_nlev[k]] with base_k = row_off[k] + k,
+  // row steps of level L at kz_steps[kz_lev_ptr[base_k + L] ..)
+  bool kz_ready = false;
+  DevBuf<int> kz_lev_ptr, kz_steps, kz_nlev;
 };
 
 namespace {
@@ -804,41 +810,113 @@ void batch_backproject(Batch &B, int method, const double *d_b, double *d_x, dou
 
 // ---------------------------------------------------------------- Kaczmarz
 namespace {
-// One CTA per instance: the instance's rows with nonzero norm in order,
-// sequentially (art.m:248-285 with kaczmarz order), all threads on one row.
-__global__ void __launch_bounds__(256)
-    k_batch_kacz(const int64_t *__restrict__ roff, const int64_t *__restrict__ rp,
-                 const int *__restrict__ ci, const float *__restrict__ rv, const double *__restrict__ b,
-                 const double *__restrict__ nrm, double lam, int lbk, double lb, int ubk, double ub,
-                 int sweeps, double *__restrict__ x) {
-  const int k = blockIdx.x;
-  __shared__ double sh[8];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int sw = 0; sw < sweeps; ++sw) {
-    for (int64_t i = roff[k]; i < roff[k + 1]; ++i) {
-      const double ni = nrm[i];
-      if (!(ni > 0)) continue;
-      const int64_t s0 = rp[i], s1 = rp[i + 1];
-      double a = 0;
-      for (int64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) a = fma((double)rv[e], x[ci[e]], a);
-      a = warp_sum(a);
-      if (lane == 0) sh[w] = a;
-      __syncthreads();
-      double dot = 0;
+// Level schedule of every instance's kaczmarz order (rows with nonzero norm,
+// ascending; art.m:188), one warp per instance: level(row) = 1 + max level
+// of the earlier steps touching one of its pixels (last[] holds the latest
+// level per pixel, -1 initially).  Rows with zero norm get level -1.
+__global__ void k_inst_levels(int ninst, const int64_t *__restrict__ roff, const int64_t *__restrict__ rp,
+                              const int *__restrict__ ci, const double *__restrict__ nrm, int *__restrict__ last,
+                              int *__restrict__ level, int *__restrict__ nlev) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (k >= ninst) return;
+  int maxl = -1;
+  for (int64_t r = roff[k]; r < roff[k + 1]; ++r) {
+    if (!(nrm[r] > 0)) {
+      if (lane == 0) level[r] = -1;
+      continue;
+    }
+    int L = 0;
+    for (int64_t e = rp[r] + lane; e < rp[r + 1]; e += 32) L = max(L, last[ci[e]] + 1);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) dot += sh[q];
-      const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(b[i], dot)), ni);
-      for (int64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) {
-        const int j = ci[e];
-        double v = __dadd_rn(x[j], __dmul_rn(c, (double)rv[e]));
-        if (lbk) v = fmax(v, lb);
-        if (ubk) v = fmin(v, ub);
-        x[j] = v;
+    for (int o = 16; o > 0; o >>= 1) L = max(L, __shfl_xor_sync(0xffffffffu, L, o));
+    __syncwarp();
+    for (int64_t e = rp[r] + lane; e < rp[r + 1]; e += 32) last[ci[e]] = L;
+    __syncwarp();
+    if (lane == 0) level[r] = L;
+    maxl = max(maxl, L);
+  }
+  if (lane == 0) nlev[k] = maxl + 1;
+}
+
+// Steps per level: lev_ptr[base_k + L + 1] counts instance k's rows of
+// level L (base_k = roff[k] + k; lev_ptr starts at zero).
+__global__ void k_level_hist(int64_t m, const int64_t *__restrict__ roff, const int *__restrict__ level,
+                             const int *__restrict__ inst_row, int *__restrict__ lev_ptr) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int L = level[r];
+    if (L >= 0) {
+      const int k = inst_row[r];
+      atomicAdd(lev_ptr + roff[k] + k + L + 1, 1);
+    }
+  }
+}
+
+// Inclusive scan of each instance's level counts (one thread per instance)
+// and a copy as fill cursors.
+__global__ void k_level_scan(int ninst, const int64_t *__restrict__ roff, const int *__restrict__ nlev,
+                             int *__restrict__ lev_ptr, int *__restrict__ cursor) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ninst) return;
+  int *p = lev_ptr + roff[k] + k;
+  int *c = cursor + roff[k] + k;
+  int run = (int)roff[k];  // steps of instance k start at its first row
+  p[0] = run;
+  c[0] = run;
+  for (int L = 0; L < nlev[k]; ++L) {
+    run += p[L + 1];
+    p[L + 1] = run;
+    c[L + 1] = run;
+  }
+}
+
+__global__ void k_level_fill(int64_t m, const int64_t *__restrict__ roff, const int *__restrict__ level,
+                             const int *__restrict__ inst_row, int *__restrict__ cursor, int *__restrict__ steps) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int L = level[r];
+    if (L >= 0) {
+      const int k = inst_row[r];
+      steps[atomicAdd(cursor + roff[k] + k + L, 1)] = (int)r;
+    }
+  }
+}
+
+// Kaczmarz sweeps of one instance per CTA over its level schedule: the steps
+// of a level touch disjoint pixels and run one per warp (fixed lane order and
+// shuffle tree); a block barrier separates levels, so every pixel sees the
+// update sequence of the sequential sweep (art.m:248-285).
+__global__ void __launch_bounds__(512)
+    k_batch_kacz_levels(const int64_t *__restrict__ roff, const int *__restrict__ lev_ptr,
+                        const int *__restrict__ nlev, const int *__restrict__ steps,
+                        const int64_t *__restrict__ rp, const int *__restrict__ ci, const float *__restrict__ rv,
+                        const double *__restrict__ b, const double *__restrict__ nrm, double lam, int lbk,
+                        double lb, int ubk, double ub, int sweeps, double *__restrict__ x) {
+  const int k = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int *lp = lev_ptr + roff[k] + k;
+  const int nl = nlev[k];
+  for (int sw = 0; sw < sweeps; ++sw) {
+    for (int L = 0; L < nl; ++L) {
+      const int q1 = lp[L + 1];
+      for (int q = lp[L] + warp; q < q1; q += nw) {
+        const int row = steps[q];
+        const int64_t s0 = rp[row], s1 = rp[row + 1];
+        double acc = 0.0;
+        for (int64_t e = s0 + lane; e < s1; e += 32) acc = fma((double)rv[e], x[ci[e]], acc);
+        acc = warp_sum(acc);
+        const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(b[row], acc)), nrm[row]);
+        for (int64_t e = s0 + lane; e < s1; e += 32) {
+          const int j = ci[e];
+          double v = __dadd_rn(x[j], __dmul_rn(c, (double)rv[e]));
+          if (lbk) v = fmax(v, lb);
+          if (ubk) v = fmin(v, ub);
+          x[j] = v;
+        }
       }
       __syncthreads();
     }
   }
 }
+
 }  // namespace
 
 void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int lbk, double lb,
@@ -851,14 +929,37 @@ void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int
   AIRT_CHECK_CUDA(cudaEventCreate(&t1));
   P.w1.ensure(P.m > P.n ? P.m : P.n);
   row_sums_sq(P, P.w1.p);
-  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
   // x0 = 0 is feasible for lb <= 0 <= ub, so the whole-vector clamp after the
   // first row step (art.m:279-284) only matters on each row's support.
   AIRT_REQUIRE((lbk == 0 || lb <= 0) && (ubk == 0 || ub >= 0),
                "batched Kaczmarz starts from x0 = 0 and needs lbound <= 0 <= ubound");
+  if (!B.kz_ready) {
+    // level schedules, once per batch (the pattern and the row norms never change)
+    const int K = B.ninst;
+    DevBuf<int> last, level, cursor;
+    last.ensure(P.n);
+    level.ensure(P.m);
+    cursor.ensure(P.m + K + 1);
+    B.kz_lev_ptr.ensure(P.m + K + 1);
+    B.kz_steps.ensure(P.m > 0 ? P.m : 1);
+    B.kz_nlev.ensure(K);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(last.p, 0xff, P.n * sizeof(int), s));  // -1
+    AIRT_CHECK_CUDA(cudaMemsetAsync(B.kz_lev_ptr.p, 0, (P.m + K + 1) * sizeof(int), s));
+    k_inst_levels<<<(K + 3) / 4, 128, 0, s>>>(K, B.d_row_off.p, P.rp.p, P.ci.p, P.w1.p, last.p, level.p,
+                                              B.kz_nlev.p);
+    k_level_hist<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, B.d_row_off.p, level.p, B.inst_row.p, B.kz_lev_ptr.p);
+    k_level_scan<<<(K + 127) / 128, 128, 0, s>>>(K, B.d_row_off.p, B.kz_nlev.p, B.kz_lev_ptr.p, cursor.p);
+    k_level_fill<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, B.d_row_off.p, level.p, B.inst_row.p, cursor.p,
+                                                    B.kz_steps.p);
+    AIRT_LAUNCH_CHECK();
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    B.kz_ready = true;
+  }
+  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
   AIRT_CHECK_CUDA(cudaMemsetAsync(d_x, 0, P.n * sizeof(double), s));
-  k_batch_kacz<<<B.ninst, 256, 0, s>>>(B.d_row_off.p, P.rp.p, P.ci.p, P.rv.p, d_b, P.w1.p, lam, lbk,
-                                       lb, ubk, ub, (int)sweeps, d_x);
+  k_batch_kacz_levels<<<B.ninst, 512, 0, s>>>(B.d_row_off.p, B.kz_lev_ptr.p, B.kz_nlev.p, B.kz_steps.p, P.rp.p,
+                                              P.ci.p, P.rv.p, d_b, P.w1.p, lam, lbk, lb, ubk, ub, (int)sweeps,
+                                              d_x);
   AIRT_LAUNCH_CHECK();
   AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
   AIRT_CHECK_CUDA(cudaEventSynchronize(t1));
