@@ -215,6 +215,64 @@ class WarmStart:
                     net_wall_s=t_net, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
                     plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0))
 
+    def time_to_dp(self, data, batch, kmax=2000):
+        """Time to the DP stop for all instances of `data`, `batch` at a time
+        (a multiple of batch instances), plain vs warm start.
+
+        plain: batched cimmino from zero, batch after batch.
+        warm: per batch, the back-projection u, the network's x0 and batched
+        cimmino from x0, in that order on the solver's stream.  (Running the
+        next batch's network on its own stream during a solve was measured
+        slower: the convolutions take bandwidth from the HBM-bound SpMVs.)
+
+        Inputs (sinograms) are resident on the device before the clocks start
+        and the solutions stay there; times are host wall clocks around each
+        synchronised pipeline.  Returns per-instance iterations and relative
+        errors and the two wall times."""
+        torch = self.torch
+        total = data["b"].shape[0]
+        nb = total // batch
+        if nb < 1:
+            raise ValueError("need at least one full batch")
+        Bt = self.batch(batch)
+        sels = [np.arange(i * batch, (i + 1) * batch) for i in range(nb)]
+        d_b = [data["b"].index_select(0, torch.from_numpy(sl).cuda()).contiguous() for sl in sels]
+        xp = [torch.empty((batch, self.n), dtype=torch.float64, device="cuda") for _ in range(nb)]
+        xw = [torch.empty_like(xp[0]) for _ in range(nb)]
+        u = [torch.empty_like(xp[0]) for _ in range(nb)]
+        x0 = [torch.empty_like(xp[0]) for _ in range(nb)]
+        rho = np.full(batch, self.rho)
+        tds = [data["taudelta"][sl] for sl in sels]
+        stream = Bt.stream_ptr()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ip = [Bt.sirt_device(self.method, d_b[i].data_ptr(), xp[i].data_ptr(), kmax, taudelta=tds[i],
+                             rho=rho) for i in range(nb)]
+        torch.cuda.synchronize()
+        wall_plain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        iw = []
+        for i in range(nb):
+            self.net_input(d_b[i].data_ptr(), u[i].data_ptr(), batch)
+            self.predict(u[i].data_ptr(), x0[i].data_ptr(), batch, stream)
+            iw.append(Bt.sirt_device(self.method, d_b[i].data_ptr(), xw[i].data_ptr(), kmax,
+                                     taudelta=tds[i], rho=rho, d_x0=x0[i].data_ptr()))
+        torch.cuda.synchronize()
+        wall_warm = time.perf_counter() - t0
+        xt = data["x"].double()
+        def err(xs):  # noqa: E306
+            out = []
+            for i, sl in enumerate(sels):
+                ref = xt.index_select(0, torch.from_numpy(sl).cuda())
+                out.append((torch.linalg.norm(xs[i] - ref, dim=1) / torch.linalg.norm(ref, dim=1)).cpu().numpy())
+            return np.concatenate(out)
+        return dict(instances=nb * batch, batch=batch, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
+                    plain_iters=np.concatenate([r["finaliter"] for r in ip]),
+                    warm_iters=np.concatenate([r["finaliter"] for r in iw]),
+                    plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0),
+                    plain_solver_gpu_ms=sum(r["gpu_ms"] for r in ip),
+                    warm_solver_gpu_ms=sum(r["gpu_ms"] for r in iw))
+
 
 # ---------------------------------------------------------------- training CLI
 # The configuration the checkpoint in airtoolsii_b200/weights was trained

@@ -84,3 +84,11 @@ def test_checkpoint_cuts_dp_iterations():
     assert np.mean(r["warm_iters"]) < 0.4 * np.mean(r["plain_iters"])
     assert np.mean(r["warm_relerr"]) <= 1.02 * np.mean(r["plain_relerr"])
     assert np.mean(r["x0_relerr"]) < 1.1 * np.mean(r["plain_relerr"])
+    # the multi-batch pipeline (network of batch i+1 overlapping the solve of
+    # batch i) solves the same problems to the same stop iterations
+    ws16 = W.c5_warmstart(max_batch=16, chunk=8)
+    ws16.net.load(W.checkpoint_path())
+    t = ws16.time_to_dp(te, 8)
+    np.testing.assert_array_equal(t["plain_iters"], r["plain_iters"])
+    np.testing.assert_array_equal(t["warm_iters"], r["warm_iters"])
+    np.testing.assert_allclose(t["warm_relerr"], r["warm_relerr"], rtol=1e-6)
