@@ -34,6 +34,12 @@ namespace {
 
 constexpr int kT = 256;
 
+// Grid-stride loop with 32-bit indices: every tensor of the network holds
+// fewer than 2^30 elements (checked in unet_create), and 32-bit index
+// decoding avoids the long 64-bit division sequences.
+#define AIRT_FOR32(t, total) \
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (total); t += gridDim.x * blockDim.x)
+
 __device__ __forceinline__ void bf8_to_f(const uint4 &u, float (&f)[8]) {
   const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
 #pragma unroll
@@ -168,12 +174,9 @@ __global__ void __launch_bounds__(256) k_relu_mask_colsum(int64_t P, int C, int6
 __global__ void k_pool(int B, int H, int W, int C, const __nv_bfloat16 *__restrict__ X,
                        __nv_bfloat16 *__restrict__ Y) {
   const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
-  const int64_t total = (int64_t)B * Ho * Wo * C8;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int cg = (int)(t % C8);
-    const int64_t q = t / C8;
-    const int w = (int)(q % Wo), h = (int)((q / Wo) % Ho), b = (int)(q / ((int64_t)Wo * Ho));
+  AIRT_FOR32(t, B * Ho * Wo * C8) {
+    const int cg = t % C8, q = t / C8;
+    const int w = q % Wo, h = (q / Wo) % Ho, b = q / (Wo * Ho);
     float m[8], v[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) m[j] = -INFINITY;
@@ -195,12 +198,9 @@ __global__ void k_pool(int B, int H, int W, int C, const __nv_bfloat16 *__restri
 __global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__restrict__ X,
                             const float *__restrict__ dY, float *__restrict__ dX) {
   const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
-  const int64_t total = (int64_t)B * Ho * Wo * C8;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int cg = (int)(t % C8);
-    const int64_t q = t / C8;
-    const int w = (int)(q % Wo), h = (int)((q / Wo) % Ho), b = (int)(q / ((int64_t)Wo * Ho));
+  AIRT_FOR32(t, B * Ho * Wo * C8) {
+    const int cg = t % C8, q = t / C8;
+    const int w = q % Wo, h = (q / Wo) % Ho, b = q / (Wo * Ho);
     int64_t off[4];
     float x[4][8], m[8], g[8];
     int arg[8];
@@ -222,7 +222,7 @@ __global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__r
           m[j] = x[pos][j];
           arg[j] = pos;
         }
-    ld_f8(dY + q * C + cg * 8, g);
+    ld_f8(dY + (int64_t)q * C + cg * 8, g);
 #pragma unroll
     for (int pos = 0; pos < 4; ++pos) {
       float d[8];
@@ -240,15 +240,12 @@ __global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__r
 __global__ void k_up_concat(int B, int H, int W, int C1, int C2, const __nv_bfloat16 *__restrict__ prev,
                             const __nv_bfloat16 *__restrict__ skip, __nv_bfloat16 *__restrict__ cat) {
   const int C8 = (C1 + C2) / 8, c18 = C1 / 8;
-  const int64_t total = (int64_t)B * H * W * C8;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int c8 = (int)(t % C8);
-    const int64_t p = t / C8;
+  AIRT_FOR32(t, B * H * W * C8) {
+    const int c8 = t % C8, p = t / C8;
     uint4 v;
     if (c8 < c18) {
-      const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
-      v = reinterpret_cast<const uint4 *>(prev)[(((int64_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * c18 + c8];
+      const int w = p % W, h = (p / W) % H, b = p / (W * H);
+      v = reinterpret_cast<const uint4 *>(prev)[((b * (H / 2) + h / 2) * (W / 2) + w / 2) * c18 + c8];
     } else {
       v = reinterpret_cast<const uint4 *>(skip)[p * (C2 / 8) + (c8 - c18)];
     }
@@ -261,24 +258,18 @@ __global__ void k_up_concat(int B, int H, int W, int C1, int C2, const __nv_bflo
 __global__ void k_up_concat_back(int B, int H, int W, int C1, int C2, const float *__restrict__ dcat,
                                  float *__restrict__ dprev, float *__restrict__ dskip) {
   const int C = C1 + C2, C24 = C2 / 4, C14 = C1 / 4;
-  const int64_t totS = (int64_t)B * H * W * C24;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < totS;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int c4 = (int)(t % C24);
-    const int64_t p = t / C24;
-    const float4 g = *reinterpret_cast<const float4 *>(dcat + p * C + C1 + 4 * c4);
+  AIRT_FOR32(t, B * H * W * C24) {
+    const int c4 = t % C24, p = t / C24;
+    const float4 g = *reinterpret_cast<const float4 *>(dcat + (int64_t)p * C + C1 + 4 * c4);
     float4 &d = reinterpret_cast<float4 *>(dskip)[t];
     float4 v = d;
     v.x += g.x, v.y += g.y, v.z += g.z, v.w += g.w;
     d = v;
   }
   const int Hh = H / 2, Wh = W / 2;
-  const int64_t totP = (int64_t)B * Hh * Wh * C14;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < totP;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int c4 = (int)(t % C14);
-    const int64_t q = t / C14;
-    const int w = (int)(q % Wh), h = (int)((q / Wh) % Hh), b = (int)(q / ((int64_t)Wh * Hh));
+  AIRT_FOR32(t, B * Hh * Wh * C14) {
+    const int c4 = t % C14, q = t / C14;
+    const int w = q % Wh, h = (q / Wh) % Hh, b = q / (Wh * Hh);
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -367,19 +358,21 @@ __global__ void __launch_bounds__(256) k_head_back(int64_t P, int C, int64_t row
 __global__ void k_conv1_fwd(int64_t P, int H, int W, int Co, int Kp, const __nv_bfloat16 *__restrict__ x,
                             const __nv_bfloat16 *__restrict__ wt, const float *__restrict__ bias,
                             __nv_bfloat16 *__restrict__ y) {
+  __shared__ float sw[64 * 9], sb[64];  // Co <= 64
+  for (int i = threadIdx.x; i < Co * 9; i += blockDim.x)
+    sw[i] = __bfloat162float(wt[(int64_t)(i / 9) * Kp + i % 9]);
+  for (int i = threadIdx.x; i < Co; i += blockDim.x) sb[i] = bias[i];
+  __syncthreads();
   const int C8 = Co / 8;
-  const int64_t total = P * C8;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int og = (int)(t % C8);
-    const int64_t p = t / C8;
-    const int w = (int)(p % W), h = (int)((p / W) % H);
+  AIRT_FOR32(t, (int)P * C8) {
+    const int og = t % C8, p = t / C8;
+    const int w = p % W, h = (p / W) % H;
     float xv[9];
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
       const int dh = tap / 3 - 1, dw = tap % 3 - 1;
       const bool in = h + dh >= 0 && h + dh < H && w + dw >= 0 && w + dw < W;
-      xv[tap] = in ? __bfloat162float(x[p + (int64_t)dh * W + dw]) : 0.f;
+      xv[tap] = in ? __bfloat162float(x[p + dh * W + dw]) : 0.f;
     }
     float o[8];
 #pragma unroll
@@ -387,8 +380,8 @@ __global__ void k_conv1_fwd(int64_t P, int H, int W, int Co, int Kp, const __nv_
       const int co = og * 8 + j;
       float a = 0.f;
 #pragma unroll
-      for (int tap = 0; tap < 9; ++tap) a += __bfloat162float(wt[(int64_t)co * Kp + tap]) * xv[tap];
-      o[j] = fmaxf(a + bias[co], 0.f);
+      for (int tap = 0; tap < 9; ++tap) a += sw[co * 9 + tap] * xv[tap];
+      o[j] = fmaxf(a + sb[co], 0.f);
     }
     reinterpret_cast<uint4 *>(y)[t] = f_to_bf8(o);
   }
@@ -760,7 +753,11 @@ UNet *unet_create(int H, int W, int base, int levels, int maxB, uint64_t seed) {
       d->ensure(1);
       AIRT_CHECK_CUDA(cudaMemsetAsync(d->p, 0, 4, U->s));
     }
-    for (Tensor *t : U->tensors) ensure_act(*U, t, maxB);
+    for (Tensor *t : U->tensors) {
+      AIRT_REQUIRE((int64_t)maxB * t->H * t->W * t->C < ((int64_t)1 << 30),
+                   "max_batch too large: every activation tensor must hold fewer than 2^30 values");
+      ensure_act(*U, t, maxB);
+    }
     // col / dcol only for convolutions without the implicit path (Cin = 1);
     // the first convolution never needs dX.
     size_t colmax = 1, dcolmax = 1;
@@ -809,27 +806,21 @@ cudaStream_t unet_stream(UNet &U) { return U.s; }
 namespace {
 template <typename TI>
 __global__ void k_img_in(int B, int H, int W, const TI *__restrict__ in, __nv_bfloat16 *__restrict__ x) {
-  const int64_t total = (int64_t)B * H * W;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
+  AIRT_FOR32(t, B * H * W) {
+    const int w = t % W, h = (t / W) % H, b = t / (W * H);
     x[t] = __float2bfloat16((float)in[(int64_t)b * H * W + (int64_t)w * H + h]);
   }
 }
 template <typename TO>
 __global__ void k_img_out(int B, int H, int W, const float *__restrict__ o, TO *__restrict__ out) {
-  const int64_t total = (int64_t)B * H * W;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
+  AIRT_FOR32(t, B * H * W) {
+    const int w = t % W, h = (t / W) % H, b = t / (W * H);
     out[(int64_t)b * H * W + (int64_t)w * H + h] = (TO)o[t];
   }
 }
 __global__ void k_img_tgt(int B, int H, int W, const float *__restrict__ in, float *__restrict__ o) {
-  const int64_t total = (int64_t)B * H * W;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((int64_t)W * H));
+  AIRT_FOR32(t, B * H * W) {
+    const int w = t % W, h = (t / W) % H, b = t / (W * H);
     o[t] = in[(int64_t)b * H * W + (int64_t)w * H + h];
   }
 }
