@@ -326,6 +326,7 @@ def main():
 
     import airtoolsii_b200 as airt
     from airtoolsii_b200 import _lib
+    from airtoolsii_b200 import dist as D
     from airtoolsii_b200.testprobs import parallel_operator, parallel_tables
 
     theta = np.arange(wl["nA"]) * wl["step"]
@@ -387,12 +388,7 @@ def main():
             fn()
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return D.max_over_ranks(e0.elapsed_time(e1), device="cuda")
 
     clocks = Clocks(local)
     clocks.start()                    # sampler runs from before warm-up to the end
