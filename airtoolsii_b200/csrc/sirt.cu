@@ -45,6 +45,22 @@ struct Acc4 {
 };
 
 template <bool ME>
+__device__ __forceinline__ void resid_row_pre(int64_t i, double s, const FwdOut &o, Acc4 &a, double bi,
+                                              double Mi) {
+  const double r = bi - s;
+  const double mr = Mi * r;
+  o.mr32[i] = (float)mr;
+  a.r2 += r * r;
+  a.rmr += r * mr;
+  if (ME) {
+    const double p = o.rprev[i];
+    a.p2 += p * p;
+    a.pr += p * (p + r);
+    o.rprev[i] = r;
+  }
+}
+
+template <bool ME>
 __device__ __forceinline__ void resid_row(int64_t i, double s, const FwdOut &o, Acc4 &a) {
   const double r = o.b[i] - s;
   const double mr = o.M[i] * r;
@@ -88,9 +104,14 @@ __global__ void __launch_bounds__(kThreads, 4)
                const float *__restrict__ rv, const float *__restrict__ x32, FwdOut o) {
   if (stopped(o.st)) return;
   Acc4 a;
-  for_each_segment_v<LANES>(m, rp, ci, rv, x32, [&](int64_t i, double s, bool lead) {
-    if (lead) resid_row<ME>(i, s, o, a);
-  });
+  struct BM {
+    double b, m;
+  };
+  for_each_segment_vpre<LANES>(
+      m, rp, ci, rv, x32, [&](int64_t i) { return BM{o.b[i], o.M[i]}; },
+      [&](int64_t i, double s, bool lead, BM pv) {
+        if (lead) resid_row_pre<ME>(i, s, o, a, pv.b, pv.m);
+      });
   flush<ME>(o.st, a);
 }
 
@@ -162,6 +183,19 @@ __device__ __forceinline__ void update_x(int64_t j, double g, double lam, const 
   if (slot >= 0) u.X[(int64_t)slot * u.n + j] = x;
 }
 
+// update_x with x64[j] and D[j] already loaded.
+__device__ __forceinline__ void update_x_pre(int64_t j, double g, double lam, const UpdArgs &u, int slot,
+                                             double x0, double dj) {
+  double x = x0 + lam * (dj * g);
+  if (u.lbk == AIRT_BOUND_SCALAR) x = fmax(x, u.lb);
+  else if (u.lbk == AIRT_BOUND_VECTOR) x = fmax(x, u.lbv[j]);
+  if (u.ubk == AIRT_BOUND_SCALAR) x = fmin(x, u.ub);
+  else if (u.ubk == AIRT_BOUND_VECTOR) x = fmin(x, u.ubv[j]);
+  u.x64[j] = x;
+  u.x32[j] = (float)x;
+  if (slot >= 0) u.X[(int64_t)slot * u.n + j] = x;
+}
+
 // MODE 0: fused update with st->lam_cur.  MODE 1: line-search pass that
 // stores g and accumulates sum(D.*g.^2) (sirt.m:219-222).
 template <int LANES, int MODE>
@@ -173,15 +207,20 @@ __global__ void __launch_bounds__(kThreads, 4)
   const int slot = u.save_slot[it];
   const double lam = u.st->lam_cur;
   double a4 = 0;
-  for_each_segment_v<LANES>(n, cp, ri, cv, mr32, [&](int64_t j, double g, bool lead) {
-    if (!lead) return;
-    if (MODE == 0) {
-      update_x(j, g, lam, u, slot);
-    } else {
-      u.g64[j] = g;
-      a4 += u.D[j] * (g * g);
-    }
-  });
+  struct XD {
+    double x, d;
+  };
+  for_each_segment_vpre<LANES>(
+      n, cp, ri, cv, mr32, [&](int64_t j) { return XD{MODE == 0 ? u.x64[j] : 0.0, u.D[j]}; },
+      [&](int64_t j, double g, bool lead, XD pv) {
+        if (!lead) return;
+        if (MODE == 0) {
+          update_x_pre(j, g, lam, u, slot, pv.x, pv.d);
+        } else {
+          u.g64[j] = g;
+          a4 += pv.d * (g * g);
+        }
+      });
   if (MODE == 1) {
     a4 = block_sum<kThreads>(a4);
     if (threadIdx.x == 0) atomicAdd(&u.st->acc[4], a4);
