@@ -46,7 +46,8 @@ class ArtOpts(C.Structure):
                 ("rows_stride", C.c_int64), ("relaxpar", C.c_double), ("relax_table", _dp),
                 ("damp", C.c_double), ("stoprule", C.c_int), ("taudelta", C.c_double),
                 ("lb_kind", C.c_int), ("ub_kind", C.c_int), ("lb", C.c_double),
-                ("ub", C.c_double), ("lbv", _dp), ("ubv", _dp), ("kmax", C.c_int64)]
+                ("ub", C.c_double), ("lbv", _dp), ("ubv", _dp), ("kmax", C.c_int64),
+                ("ncp_rows", C.c_int), ("ncp_cols", C.c_int), ("ncp_smooth", C.c_int)]
 
 
 class Info(C.Structure):

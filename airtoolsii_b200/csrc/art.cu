@@ -19,6 +19,7 @@
 #include <numeric>
 
 #include "common.cuh"
+#include "ncp.cuh"
 #include "spmv.cuh"
 
 namespace airt {
@@ -85,16 +86,18 @@ __global__ void __launch_bounds__(1024)
   for (int64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) a.x[a.ci[e]] = keep[e - s0];
 }
 
+// ||b - A*x||^2 into *out; with rout the residual itself is kept (NCP).
 template <int LANES>
 __global__ void __launch_bounds__(256)
     k_resid_norm(int64_t m, const int64_t *__restrict__ rp, const int *__restrict__ ci,
                  const float *__restrict__ rv, const double *__restrict__ x,
-                 const double *__restrict__ b, double *__restrict__ out) {
+                 const double *__restrict__ b, double *__restrict__ out, double *__restrict__ rout) {
   double a = 0;
   for_each_segment<LANES>(m, rp, ci, rv, x, [&](int64_t i, double s, bool lead) {
     if (lead) {
       const double r = b[i] - s;
       a += r * r;
+      if (rout) rout[i] = r;
     }
   });
   a = block_sum<256>(a);
@@ -168,8 +171,14 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
   for (int64_t l = 1; l < nK; ++l)
     AIRT_REQUIRE(K[l] > K[l - 1], "Elements of K must be strictly increasing.");
   AIRT_REQUIRE(o.kmax == K[nK - 1] && o.kmax >= 0, "kmax must equal K(end)");
-  AIRT_REQUIRE(o.stoprule == AIRT_STOP_NONE || o.stoprule == AIRT_STOP_DP,
-               "ART supports the NONE and DP stopping rules");
+  AIRT_REQUIRE(o.stoprule == AIRT_STOP_NONE || o.stoprule == AIRT_STOP_DP || o.stoprule == AIRT_STOP_NCP,
+               "ART supports the NONE, DP and NCP stopping rules");
+  const bool ncp = o.stoprule == AIRT_STOP_NCP;
+  if (ncp) {
+    AIRT_REQUIRE(o.ncp_rows >= 2 && o.ncp_cols >= 1 && (int64_t)o.ncp_rows * o.ncp_cols == m,
+                 "NCP: res_dims must multiply to the number of rows of A");
+    AIRT_REQUIRE(o.ncp_smooth >= 1, "NCP: ncp_smooth must be positive");
+  }
   AIRT_REQUIRE(o.damp >= 0, "Damping must be positive");
   AIRT_REQUIRE(m < (int64_t)INT32_MAX, "too many rows for ART");
   const int64_t kmax = o.kmax;
@@ -264,19 +273,43 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
   a.ubv = P.ubv.p;
 
   const int L = lanes_for(P.nnz, m);
+  // NCP: the residual, the periodogram distances per column, and the
+  // ncp_smooth history (check_inputs.m:209, +inf initially)
+  DevBuf<double> r64, tw, pk, ccol;
+  const int q = ncp ? o.ncp_rows / 2 : 0;
+  std::vector<double> dk(ncp ? o.ncp_smooth : 0, INFINITY), hcol(ncp ? o.ncp_cols : 0);
+  if (ncp) {
+    r64.ensure(m);
+    const std::vector<double> t = ncp_twiddles(o.ncp_rows);
+    tw.upload(t.data(), t.size(), s);
+    pk.ensure((size_t)o.ncp_cols * q);
+    ccol.ensure(o.ncp_cols);
+  }
+  double ncc = 0.0;
   auto resid = [&]() -> double {
     AIRT_CHECK_CUDA(cudaMemsetAsync(red.p, 0, sizeof(double), s));
     const unsigned g = grid_for(m * L, 256);
     switch (L) {
-      case 32: k_resid_norm<32><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p); break;
-      case 16: k_resid_norm<16><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p); break;
-      case 8: k_resid_norm<8><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p); break;
-      default: k_resid_norm<4><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p); break;
+      case 32: k_resid_norm<32><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p, ncp ? r64.p : nullptr); break;
+      case 16: k_resid_norm<16><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p, ncp ? r64.p : nullptr); break;
+      case 8: k_resid_norm<8><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p, ncp ? r64.p : nullptr); break;
+      default: k_resid_norm<4><<<g, 256, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, P.x64.p, d_b, red.p, ncp ? r64.p : nullptr); break;
     }
     AIRT_LAUNCH_CHECK();
+    if (ncp) {
+      k_ncp_power<<<dim3(o.ncp_cols, (q + 255) / 256), 256, 0, s>>>(o.ncp_rows, q, r64.p, tw.p, pk.p, nullptr);
+      k_ncp_col<<<o.ncp_cols, 256, 0, s>>>(q, pk.p, ccol.p, nullptr);
+      AIRT_LAUNCH_CHECK();
+      AIRT_CHECK_CUDA(cudaMemcpyAsync(hcol.data(), ccol.p, o.ncp_cols * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
     double h = 0;
     AIRT_CHECK_CUDA(cudaMemcpyAsync(&h, red.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    if (ncp) {
+      double sum = 0.0;
+      for (double v : hcol) sum += v;
+      ncc = sum / o.ncp_cols;
+    }
     return std::sqrt(h);
   };
 
@@ -290,6 +323,17 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
       if (nrk <= o.taudelta || k >= kmax) {
         stop = true;
         stoprule = (k != kmax) ? 2 : 0;
+      }
+    } else if (ncp) {  // check_stoprules.m:124-149 on the ncc of this residual
+      double mx = -INFINITY, mxn = ncc;
+      for (double v : dk) mx = std::fmax(mx, v);
+      for (size_t i = 1; i < dk.size(); ++i) mxn = std::fmax(mxn, dk[i]);
+      if (mx < mxn || k >= kmax) {
+        stop = true;
+        stoprule = (k != kmax) ? 1 : 0;
+      } else {
+        dk.erase(dk.begin());
+        dk.push_back(ncc);
       }
     } else if (k >= kmax) {
       stop = true;

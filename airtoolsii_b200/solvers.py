@@ -101,9 +101,6 @@ def _parse(A, b, K, x0, options, caller):
             raise ValueError("NCP stopping rule only implemented for 1D and 2D residuals, the size "
                              "of which should be given using options.stoprule.res_dims.")
         smooth = int(sr.get("ncp_smooth", 2))
-        if caller != "sirt":
-            raise NotImplementedError("the NCP stopping rule is available for SIRT methods; "
-                                      "ART on the GPU takes 'DP' or 'none'")
         ncp = (rows, cols, smooth)
     elif "ncp_smooth" in sr:
         warnings.warn("options.stoprule.ncp_smooth given but only used by NCP stopping rule, "
@@ -398,6 +395,8 @@ def art(art_method, A, b, K, x0=None, options=None):
     o.damp = c["damp"]
     o.stoprule = _lib.STOP[c["stype"]]
     o.taudelta = c["taudelta"]
+    if c["ncp"] is not None:
+        o.ncp_rows, o.ncp_cols, o.ncp_smooth = c["ncp"]
     _bound_fields(o, c["bounds"])
     o.kmax = kmax
     X = np.zeros((n, Kint.size), dtype=np.float64, order="F")

@@ -94,12 +94,13 @@ typedef struct {
                                  one entry per step of a sweep (the values of
                                  the art.m:273-275 handle), or NULL           */
     double damp;              /* art.m:206                                      */
-    int stoprule;             /* AIRT_STOP_NONE or AIRT_STOP_DP                 */
+    int stoprule;             /* AIRT_STOP_NONE, AIRT_STOP_DP or AIRT_STOP_NCP  */
     double taudelta;
     int lb_kind, ub_kind;
     double lb, ub;
     const double *lbv, *ubv;
     int64_t kmax;             /* sweeps (already halved for symkaczmarz)        */
+    int ncp_rows, ncp_cols, ncp_smooth; /* NCP, as in airt_sirt_opts           */
 } airt_art_opts;
 
 typedef struct {

@@ -245,6 +245,22 @@ def test_sirt_ncp_stop(c1, method, dims, smooth):
     assert relerr(X, Xo) <= RTOL
 
 
+@pytest.mark.parametrize("method,smooth", [("kaczmarz", 2), ("symkaczmarz", 2), ("kaczmarz", 3)])
+def test_art_ncp_stop(c1, method, smooth):
+    """NCP for ART (art.m calls check_stoprules after every sweep): same stop
+    sweep and saved iterates as the oracle."""
+    A, A_ref, b, _, _ = c1
+    opts = {"stoprule": {"type": "NCP", "res_dims": [91, 180], "ncp_smooth": smooth}}
+    K = list(range(1, 31)) if method == "kaczmarz" else list(range(2, 31, 2))
+    Xo, io = O.art(method, A_ref, b, K, None, opts)
+    X, info = getattr(airt, method)(A, b, K, None, opts)
+    assert io["stoprule"] == 1
+    assert info["stoprule"] == 1 and info["finaliter"] == io["finaliter"]
+    assert X.shape == Xo.shape
+    for k in range(X.shape[1]):
+        assert relerr(X[:, k], Xo[:, k]) <= RTOL
+
+
 def test_sirt_ncp_reaches_kmax(c1):
     """NCP with kmax below its stop: stoprule 0 at kmax, as the reference."""
     A, A_ref, b, _, _ = c1
