@@ -770,3 +770,138 @@ def art(method, A, b, K, x0=None, options=None, stream=None):
     info["itersaved"] = np.concatenate([K[K < info["finaliter"]], [info["finaliter"]]])
     info["timetaken"] = time.perf_counter() - t0
     return X, info
+
+
+# ---------------------------------------------------------------- training
+def _run(method, A, b, K, x0, options):
+    if method in ("landweber", "cimmino", "cav", "drop", "sart"):
+        X, info, _ = sirt(method, A, b, K, x0, options)
+    else:
+        X, info = art(method, A, b, K, x0, options)
+    return X, info
+
+
+def train_relaxpar(A, b, x_ex, method, kmax, options=None):
+    """train/train_relaxpar.m:75-270, branch for branch."""
+    if options is not None:
+        options = dict(options)
+        options["stoprule"] = {"type": "none"}
+        options.pop("relaxpar", None)
+    else:
+        options = {}
+    fudge, stepk = 0.02, 10
+    K = list(range(1, stepk + 1))
+    k, stop, Er, x0 = 0, False, [], None
+    is_sirt = method in ("landweber", "cimmino", "cav", "drop", "sart")
+    while not stop:
+        if k + stepk > kmax:
+            K = list(range(1, kmax - k + 1))
+            k = kmax
+        else:
+            k += stepk
+        if k <= stepk:
+            if is_sirt:
+                Xnew, info = _run(method, A, b, K, x0, options)
+                options["rho"] = info["rho"]
+                relaxparmax = 2 / info["rho"]
+            else:
+                options["relaxpar"] = 0.25
+                Xnew, _ = _run(method, A, b, K, x0, options)
+                relaxparmax = 2
+        else:
+            Xnew, _ = _run(method, A, b, K, x0, options)
+        Er.extend(np.sqrt(np.sum((Xnew - x_ex[:, None]) ** 2, axis=0)))
+        kopt = int(np.argmin(Er)) + 1
+        minE = Er[kopt - 1]
+        if kopt == k and k < kmax:
+            x0 = Xnew[:, -1]
+        else:
+            stop = True
+    meub = (1 + fudge) * minE
+
+    def ev(p):
+        options["relaxpar"] = p
+        xnew, _ = _run(method, A, b, list(range(1, kopt + 1)), None, options)
+        ee = np.sqrt(np.sum((xnew - x_ex[:, None]) ** 2, axis=0))
+        kk = int(np.sum((ee[:-1] > meub) & (np.diff(ee) < 0))) + 1
+        return kk, ee[kk - 1]
+
+    r = (3 - np.sqrt(5)) / 2
+    alpha, beta = 0.0, relaxparmax
+    alphap, betap = alpha + r * (beta - alpha), alpha + (1 - r) * (beta - alpha)
+    k_alphap, err_alphap = ev(alphap)
+    k_betap, err_betap = ev(betap)
+
+    def up():
+        nonlocal alpha, alphap, betap, k_alphap, err_alphap, k_betap, err_betap
+        z = alphap + (1 - r) * abs(beta - alphap)
+        alpha, alphap, betap = alphap, betap, z
+        k_alphap, err_alphap = k_betap, err_betap
+        k_betap, err_betap = ev(betap)
+
+    def down():
+        nonlocal beta, alphap, betap, k_alphap, err_alphap, k_betap, err_betap
+        z = alpha + r * abs(betap - alpha)
+        beta, betap, alphap = betap, alphap, z
+        k_betap, err_betap = k_alphap, err_alphap
+        k_alphap, err_alphap = ev(alphap)
+
+    while abs(alphap - betap) > relaxparmax * 0.01:
+        if is_sirt:
+            if err_alphap > meub:
+                up()
+            elif err_betap > meub:
+                down()
+            elif k_alphap >= k_betap:
+                up()
+            else:
+                down()
+        else:
+            if err_betap > meub:
+                down()
+            elif err_alphap > meub:
+                up()
+            elif k_alphap >= k_betap:
+                up()
+            else:
+                down()
+    return (alphap + betap) / 2
+
+
+def train_dpme(A, b_exact, x_exact, method, type_, delta, E, kmax, options=None):
+    """train/train_dpme.m:66-136 with the noise matrix E (m x s) given."""
+    options = dict(options or {})
+    options["stoprule"] = {"type": "none"}
+    A = sp.csr_matrix(A)
+    e = delta * E / np.sqrt(np.sum(E * E, axis=0))[None, :]
+    B = b_exact[:, None] + e
+    kstep = kmax if kmax < 10 else 10
+    taus = []
+    for i in range(E.shape[1]):
+        bi = B[:, i]
+        X = np.zeros((x_exact.size, 1))
+        x0 = None
+        k = kstep
+        K = list(range(1, k + 1))
+        Ek = []
+        while True:
+            Xny, _ = _run(method, A, bi, K, x0, options)
+            Ek.extend(np.sqrt(np.sum((Xny - x_exact[:, None]) ** 2, axis=0)))
+            X = np.hstack([X, Xny])
+            I = int(np.argmin(Ek)) + 1
+            if I != k or k >= kmax:
+                kopt = I
+                break
+            if k + kstep > kmax:
+                K = list(range(1, kmax - k + 1))
+                k = kmax
+            else:
+                k += kstep
+            x0 = Xny[:, -1]
+        rk = bi - A @ X[:, kopt - 1]
+        if type_.upper().startswith("DP"):
+            taus.append(np.linalg.norm(rk) / delta)
+        else:
+            rkm1 = bi - A @ X[:, kopt - 2]
+            taus.append(0.5 * (rkm1 @ (rkm1 + rk)) / (delta * np.linalg.norm(rkm1)))
+    return float(np.mean(taus))
