@@ -154,6 +154,25 @@ def fan_tables(N, theta=None, p=None, R=None, dw=None, sd=None):
     return theta, int(p), Rv, dwv, sdv, cosd(theta), sind(theta), cosd(omega), sind(omega)
 
 
+def fancurved_tables(N, theta=None, p=None, R=None, d=None):
+    """fancurvedtomo.m:102-140,161-175: (theta, p, R, d, cos_t, sin_t,
+    cos_w, sin_w) with R multiplied by N; the arc detector's rays leave the
+    source at omega = linspace(-d/2, d/2, p) degrees about the central ray
+    (default d = 2*atand(1/(2R-1)), R = 2)."""
+    Rn = 2.0 if R is None else float(R)
+    if d is None:
+        d = 2.0 * float(atand(1.0 / (2.0 * Rn - 1.0)))
+    if p is None:
+        p = int(_mround(math.sqrt(2.0) * N))
+    theta = np.arange(0.0, 359.0, 2.0) if theta is None else np.asarray(theta, float).ravel()
+    if Rn < math.sqrt(2.0) / 2.0:
+        raise ValueError("R must be greater than half squareroot 2")
+    if d < 0 or d > 180:
+        raise ValueError("The angle of the source must be in the interval [0 180]")
+    omega = _linspace(-d / 2.0, d / 2.0, int(p))
+    return theta, int(p), Rn * N, float(d), cosd(theta), sind(theta), cosd(omega), sind(omega)
+
+
 def parallel_operator(N, cos_t, sin_t, offsets, matrix_free=False) -> AirtOperator:
     ct = np.ascontiguousarray(cos_t, np.float64)
     st = np.ascontiguousarray(sin_t, np.float64)
@@ -185,6 +204,18 @@ def paralleltomo(N, theta=None, p=None, d=None, isDisp=0, isMatrix=1):
     x = phantomgallery("shepplogan", N).ravel(order="F")
     b = A(x, "notransp")
     return A, b, x, theta, p, d
+
+
+def fancurvedtomo(N, theta=None, p=None, R=None, d=None, isDisp=0, isMatrix=1):
+    """[A,b,x,theta,p,R,d] = fancurvedtomo(N,theta,p,R,d,isDisp,isMatrix)
+    (testprobs/fancurvedtomo.m:1): fan beam onto an arc detector; the same
+    ray trace as fanlineartomo (no boundary exclusion).  R is returned in
+    units of N, d in degrees."""
+    theta, p, Rv, d, ct, st, cw, sw = fancurved_tables(N, theta, p, R, d)
+    A = fan_operator(N, ct, st, cw, sw, Rv, matrix_free=not isMatrix)
+    x = phantomgallery("shepplogan", N).ravel(order="F")
+    b = A(x, "notransp")
+    return A, b, x, theta, p, Rv / N, d
 
 
 def fanlineartomo(N, theta=None, p=None, R=None, dw=None, sd=None, isDisp=0, isMatrix=1):

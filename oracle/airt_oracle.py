@@ -192,6 +192,24 @@ def fan_geometry(N: int, theta=None, p=None, R=2.0, dw=2.5, sd=3.0):
             cosd(omega), sind(omega))
 
 
+def fancurved_geometry(N: int, theta=None, p=None, R=2.0, d=None):
+    """Defaults and tables of fancurvedtomo.m:102-140, 161-175: an arc
+    detector, ray angles omega = linspace(-d/2, d/2, p) degrees about the
+    central ray.  Returns (theta, p, Rabs, d, cos_t, sin_t, cos_w, sin_w)."""
+    if d is None:
+        d = 2.0 * float(atand(1.0 / (2.0 * R - 1.0)))
+    if p is None:
+        p = int(mround(math.sqrt(2.0) * N))
+    theta = (np.arange(0.0, 359.0, 2.0) if theta is None
+             else np.asarray(theta, float).ravel())
+    if R < math.sqrt(2.0) / 2.0:
+        raise ValueError("R must be greater than half squareroot 2")
+    if d < 0 or d > 180:
+        raise ValueError("The angle of the source must be in the interval [0 180]")
+    omega = linspace(-d / 2.0, d / 2.0, p)
+    return (theta, int(p), R * N, float(d), cosd(theta), sind(theta), cosd(omega), sind(omega))
+
+
 def fan_rays(N, R, cos_t, sin_t, cos_w, sin_w):
     """Yield (row, x0theta, y0theta, a, b) per ray, fanlineartomo.m:230-257.
 

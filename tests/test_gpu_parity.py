@@ -74,6 +74,23 @@ def test_fan_matrix_vs_c_oracle():
     same_matrix(A, Rm)
 
 
+@pytest.mark.parametrize("N,theta,p,R,d", [(40, np.arange(0.0, 360.0, 4.0), None, None, None),
+                                          (33, np.arange(0.0, 360.0, 7.5), 45, 1.5, 60.0)])
+def test_fancurved_matrix_vs_c_oracle(N, theta, p, R, d):
+    """fancurvedtomo (arc detector): bit-exact against the C tracer fed with
+    the oracle's fancurvedtomo.m tables; matrix-free products agree."""
+    th, pp, Rabs, dd, ct, st, cw, sw = O.fancurved_geometry(N, theta, p, 2.0 if R is None else R, d)
+    rows, cols, vals = cbind.trace_coo(N, list(O.fan_rays(N, Rabs, ct, st, cw, sw)), False)
+    Rm = O.coo_to_csc(rows, cols, vals, len(th) * pp, N * N)
+    A, b, x, th2, p2, R2, d2 = airt.fancurvedtomo(N, theta, p, R, d)
+    assert p2 == pp and abs(d2 - dd) == 0 and R2 == Rabs / N
+    same_matrix(A, Rm)
+    Amf, *_ = airt.fancurvedtomo(N, theta, p, R, d, 0, 0)
+    v = np.random.default_rng(N).random(N * N)
+    y = Amf(v, "notransp")
+    assert np.linalg.norm(y - Rm @ v) <= 1e-6 * np.linalg.norm(Rm @ v)
+
+
 def test_c2_matrix_bit_exact_sampled_angles():
     """N=512, p=724 on 24 of the 360 half-degree angles (full-size rays)."""
     theta = (np.arange(360) * 0.5)[::15]
