@@ -105,6 +105,7 @@ __device__ __forceinline__ Ray batch_ray(const InstGeom &gk, const double *cos_t
   g.sin_t = sin_t + gk.ang0;
   g.offsets = offs + gk.off0;
   g.cos_w = g.sin_w = nullptr;
+  g.src_x = g.src_y = g.rcv_x = g.rcv_y = nullptr;
   return ray_of(g, local);
 }
 

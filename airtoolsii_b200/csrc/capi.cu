@@ -192,6 +192,38 @@ int airt_problem_fan(int N, int nA, const double *cos_t, const double *sin_t, in
   return make_geometry(GEO_FAN, N, nA, cos_t, sin_t, p, nullptr, cos_w, sin_w, R, matrix_free, out);
 }
 
+int airt_problem_seismic(int N, int s, const double *src_x, const double *src_y, int p,
+                         const double *rcv_x, const double *rcv_y, int matrix_free,
+                         airt_problem **out) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(out, "null pointer argument");
+  AIRT_REQUIRE((src_x && src_y) || s == 0, "null pointer argument");
+  AIRT_REQUIRE((rcv_x && rcv_y) || p == 0, "null pointer argument");
+  AIRT_REQUIRE(N >= 1 && N <= 46340 && s >= 0 && p >= 0, "geometry size out of range");
+  AIRT_REQUIRE((int64_t)s * p < INT32_MAX, "too many rays");
+  Problem *P = new_problem();
+  try {
+    P->geo_kind = GEO_SEISMIC;
+    P->N = N;
+    P->nA = s;
+    P->p = p;
+    P->m = (int64_t)s * p;
+    P->n = (int64_t)N * N;
+    P->matrix_free = matrix_free != 0;
+    P->src_x.upload(src_x, s, P->stream);
+    P->src_y.upload(src_y, s, P->stream);
+    P->rcv_x.upload(rcv_x, p, P->stream);
+    P->rcv_y.upload(rcv_y, p, P->stream);
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
+    if (!P->matrix_free) generate_matrix(*P);
+  } catch (...) {
+    free_problem(P);
+    throw;
+  }
+  *out = reinterpret_cast<airt_problem *>(P);
+  AIRT_API_END
+}
+
 int airt_problem_size(const airt_problem *h, int64_t *m, int64_t *n, int64_t *nnz) {
   AIRT_API_BEGIN
   AIRT_REQUIRE(h, "null problem handle");

@@ -90,10 +90,11 @@ struct DevBuf {
 };
 
 // ---------------------------------------------------------------- geometry
-enum GeoKind { GEO_NONE = 0, GEO_PARALLEL = 1, GEO_FAN = 2 };
+enum GeoKind { GEO_NONE = 0, GEO_PARALLEL = 1, GEO_FAN = 2, GEO_SEISMIC = 3 };
 
-// Per-ray parameters of both geometries, prepared on the device:
-// ray r = angle*p + j starts at (x0t, y0t) with direction (a, b).
+// Per-ray parameters of the geometries, prepared on the device: ray
+// r = i*p + j (i = angle or source, j = detector or receiver) starts at
+// (x0t, y0t) with direction (a, b).
 struct RayGeom {
   int kind;
   int N, nA, p;
@@ -101,6 +102,8 @@ struct RayGeom {
   const double *cos_t, *sin_t;  // nA
   const double *offsets;         // p (parallel)
   const double *cos_w, *sin_w;  // p (fan)
+  const double *src_x, *src_y;  // nA sources (seismic)
+  const double *rcv_x, *rcv_y;  // p receivers (seismic)
 };
 
 // ---------------------------------------------------------------- SIRT state
@@ -141,6 +144,7 @@ struct Problem {
   int N = 0, nA = 0, p = 0;
   double R = 0;
   DevBuf<double> cos_t, sin_t, offsets, cos_w, sin_w;
+  DevBuf<double> src_x, src_y, rcv_x, rcv_y;  // seismic: nA sources, p receivers
 
   // stored matrix: CSR over rays (rows) and CSC over pixels (columns)
   DevBuf<int64_t> rp, cp;
@@ -191,6 +195,10 @@ struct Problem {
     g.offsets = offsets.p;
     g.cos_w = cos_w.p;
     g.sin_w = sin_w.p;
+    g.src_x = src_x.p;
+    g.src_y = src_y.p;
+    g.rcv_x = rcv_x.p;
+    g.rcv_y = rcv_y.p;
     return g;
   }
 };

@@ -1,11 +1,11 @@
 // GPU system-matrix generation and matrix-free projectors for the
-// paralleltomo / fanlineartomo geometries.
+// paralleltomo / fanlineartomo / fancurvedtomo / seismictomo geometries.
 //
 //  * generate_matrix: two passes over the rays (count, then fill) with an
 //    exclusive scan in between give the CSR over rays; the CSC follows by a
 //    stable transposition.  Row entries keep the ray order of the trace.
-//    Replaces testprobs/paralleltomo.m:112-301 and fanlineartomo.m:141-358
-//    (isMatrix = 1).
+//    Replaces testprobs/paralleltomo.m:112-301, fanlineartomo.m:141-358 and
+//    seismictomo.m:96-287 (isMatrix = 1).
 //  * apply_matrix_free: forward projection (one thread per ray, FP64 sum in
 //    ray order) and back projection (one thread per ray, FP64 atomic scatter)
 //    that re-trace every ray, as the isMatrix = 0 handles of

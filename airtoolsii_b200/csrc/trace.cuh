@@ -1,17 +1,18 @@
-// Device ray tracer of the paralleltomo / fanlineartomo line model.
+// Device ray tracer of the paralleltomo / fanlineartomo / fancurvedtomo /
+// seismictomo line model.
 //
 // One ray is one row of A.  The reference (testprobs/paralleltomo.m:207-263,
-// testprobs/fanlineartomo.m:271-318) computes the crossings with all x = const
-// and y = const grid lines, sorts them by the line parameter t (stable, NaN
-// last), keeps the points inside the square, drops a point whose successor is
-// within 1e-10 in both coordinates, and turns consecutive points into
-// (pixel, length) pairs.  Both crossing sequences are monotone in t, so the
-// sort is replaced here by a two-way merge that takes the x-crossing first on
-// equal t -- the same order the stable sort gives for every point that
-// survives the box filter (non-finite t values never survive it).  All FP64
-// arithmetic uses explicit round-to-nearest intrinsics, so no multiply-add is
-// contracted and the points, lengths and pixel indices are bit-identical to
-// the FP64 CPU restatement.
+// testprobs/fanlineartomo.m:271-318, testprobs/seismictomo.m:194-249) computes
+// the crossings with all x = const and y = const grid lines, sorts them by the
+// line parameter t (stable, NaN last), keeps the points inside the square,
+// drops a point whose successor is within 1e-10 in both coordinates, and turns
+// consecutive points into (pixel, length) pairs.  Both crossing sequences are
+// monotone in t, so the sort is replaced here by a two-way merge that takes the
+// x-crossing first on equal t -- the same order the stable sort gives for every
+// point that survives the box filter (non-finite t values never survive it).
+// All FP64 arithmetic uses explicit round-to-nearest intrinsics, so no
+// multiply-add is contracted and the points, lengths and pixel indices are
+// bit-identical to the FP64 CPU restatement.
 #pragma once
 
 #include "common.cuh"
@@ -22,12 +23,21 @@ struct Ray {
   double x0t, y0t, a, b;
 };
 
-// Ray parameters, paralleltomo.m:195-200 / fanlineartomo.m:230-257.
+// Ray parameters, paralleltomo.m:195-200 / fanlineartomo.m:230-257 /
+// seismictomo.m:188-200.
 __device__ __forceinline__ Ray ray_of(const RayGeom &g, int64_t r) {
   const int i = (int)(r / g.p);
   const int j = (int)(r - (int64_t)i * g.p);
-  const double c = g.cos_t[i], s = g.sin_t[i];
   Ray q;
+  if (g.kind == GEO_SEISMIC) {
+    // from source i to receiver j (t = 1 at the receiver)
+    q.x0t = g.src_x[i];
+    q.y0t = g.src_y[i];
+    q.a = __dsub_rn(g.rcv_x[j], q.x0t);
+    q.b = __dsub_rn(g.rcv_y[j], q.y0t);
+    return q;
+  }
+  const double c = g.cos_t[i], s = g.sin_t[i];
   if (g.kind == GEO_PARALLEL) {
     const double x0 = g.offsets[j];
     q.x0t = __dsub_rn(__dmul_rn(c, x0), __dmul_rn(s, 0.0));

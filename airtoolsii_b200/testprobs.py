@@ -1,13 +1,16 @@
-"""Tomography test problems on the GPU: paralleltomo and fanlineartomo.
+"""Tomography test problems on the GPU: paralleltomo, fanlineartomo,
+fancurvedtomo and seismictomo.
 
 The host side prepares the per-angle and per-detector tables in FP64 exactly
 as the reference does (cosd/sind of the angles, linspace ray offsets, the
-fan's atand detector angles); libairt traces every ray on the device and
+fan's atand detector angles, the seismic source and receiver positions);
+libairt traces every ray on the device and
 either stores A (FP32 CSR + CSC, bit-exact sparsity with the FP64 trace) or
 keeps the geometry for matrix-free projection.
 
-Also here: the reference's modified Shepp-Logan phantom and the random-ellipse
-phantom family (same rasterisation grid, testprobs/phantomgallery.m:188-214).
+Also here: the reference's modified Shepp-Logan and tectonic phantoms and the
+random-ellipse phantom family (same rasterisation grid as the Shepp-Logan
+image, testprobs/phantomgallery.m:188-214).
 """
 from __future__ import annotations
 
@@ -89,10 +92,43 @@ def ellipse_image(N: int, ellipses, clip_hi=None) -> np.ndarray:
 
 
 def phantomgallery(name: str, N: int) -> np.ndarray:
-    """The 'shepplogan' image of testprobs/phantomgallery.m:155-214 (N x N)."""
-    if name != "shepplogan":
-        raise ValueError("only the 'shepplogan' phantom is provided")
-    return ellipse_image(N, [(a, b, c, d, e, f * math.pi / 180) for a, b, c, d, e, f in _SHEPP])
+    """The 'shepplogan' (testprobs/phantomgallery.m:155-214) or 'tectonic'
+    (phantomgallery.m:422-456) image, N x N."""
+    if name == "shepplogan":
+        return ellipse_image(N, [(a, b, c, d, e, f * math.pi / 180) for a, b, c, d, e, f in _SHEPP])
+    if name == "tectonic":
+        return tectonic(N)
+    raise ValueError("only the 'shepplogan' and 'tectonic' phantoms are provided")
+
+
+def tectonic(N: int) -> np.ndarray:
+    """Two plates meeting at a sloped break (phantomgallery.m:422-456): the
+    right plate at 0.75 with a stepped upper edge, the left plate at 1 whose
+    rows shift down by one every second column across the break.  Raises
+    ValueError for N whose index ranges leave the image (N < 10)."""
+    N = int(N)
+    n5, n13, n7, n20 = (int(_mround(N / k)) for k in (5, 13, 7, 20))
+    X = np.zeros((N, N))
+
+    def put(r0, r1, c0, c1, v):          # MATLAB X(r0:r1, c0:c1) = v, 1-based
+        if r0 > r1 or c0 > c1:
+            return
+        if r0 < 1 or c0 < 1 or r1 > N or c1 > N:
+            raise ValueError("tectonic phantom needs N >= 10")
+        X[r0 - 1:r1, c0 - 1:c1] = v
+
+    put(n5, n5 + n7, 5 * n13, N, 0.75)
+    i = n5
+    for j in range(1, n20 + 1, 2):      # the stepped edge of the right plate
+        i -= 1
+        put(i, i, 5 * n13 + j, N, 0.75)
+    put(n5, 2 * n5, 1, 5 * n13, 1.0)
+    lo = n5
+    for j in range(5 * n13, min(12 * n13, N) + 1):
+        if j % 2:
+            lo += 1
+        put(lo, lo + n5, j, j, 1.0)
+    return X
 
 
 def random_ellipses(N: int, count: int, seed: int, clip=(0.0, 1.0)) -> np.ndarray:
@@ -173,6 +209,41 @@ def fancurved_tables(N, theta=None, p=None, R=None, d=None):
     return theta, int(p), Rn * N, float(d), cosd(theta), sind(theta), cosd(omega), sind(omega)
 
 
+def seismic_tables(N, s=None, p=None):
+    """seismictomo.m:67-75,98-116: (s, p, src_x, src_y, rcv_x, rcv_y).  s
+    sources (default N) on the right edge at y = linspace(-N/2+Ns, N/2-Ns, s);
+    p receivers (default 2N): floor(p/2) on the left edge, then ceil(p/2) on
+    the top edge, each set at the centres of equal intervals."""
+    N = int(N)
+    if s is not None and np.size(s) > 1:
+        raise ValueError("s must be a scaler")
+    s = N if s is None else int(np.asarray(s).ravel()[0])
+    p = 2 * N if p is None else int(p)
+    h = N / 2.0
+    ns = (N / s) / 2.0 if s else math.inf
+    p1, p2 = -(-p // 2), p // 2
+    np1 = (N / p1) / 2.0 if p1 else math.inf
+    np2 = (N / p2) / 2.0 if p2 else math.inf
+    src_x = np.full(s, h)
+    src_y = _linspace(-h + ns, h - ns, s)
+    rcv_x = np.concatenate([np.full(p2, -h), _linspace(-h + np1, h - np1, p1)])
+    rcv_y = np.concatenate([_linspace(-h + np2, h - np2, p2), np.full(p1, h)])
+    return s, p, src_x, src_y, rcv_x, rcv_y
+
+
+def seismic_operator(N, src_x, src_y, rcv_x, rcv_y, matrix_free=False) -> AirtOperator:
+    sx = np.ascontiguousarray(src_x, np.float64)
+    sy = np.ascontiguousarray(src_y, np.float64)
+    rx = np.ascontiguousarray(rcv_x, np.float64)
+    ry = np.ascontiguousarray(rcv_y, np.float64)
+    if sx.size != sy.size or rx.size != ry.size:
+        raise ValueError("source and receiver tables need matching x and y lengths")
+    h = C.c_void_p()
+    check(lib().airt_problem_seismic(int(N), sx.size, dptr(sx), dptr(sy), rx.size, dptr(rx),
+                                     dptr(ry), int(bool(matrix_free)), C.byref(h)))
+    return AirtOperator(h, "seismic", dict(N=N, s=sx.size, p=rx.size))
+
+
 def parallel_operator(N, cos_t, sin_t, offsets, matrix_free=False) -> AirtOperator:
     ct = np.ascontiguousarray(cos_t, np.float64)
     st = np.ascontiguousarray(sin_t, np.float64)
@@ -216,6 +287,18 @@ def fancurvedtomo(N, theta=None, p=None, R=None, d=None, isDisp=0, isMatrix=1):
     x = phantomgallery("shepplogan", N).ravel(order="F")
     b = A(x, "notransp")
     return A, b, x, theta, p, Rv / N, d
+
+
+def seismictomo(N, s=None, p=None, isDisp=0, isMatrix=1):
+    """[A,b,x,s,p] = seismictomo(N,s,p,isDisp,isMatrix)
+    (testprobs/seismictomo.m:1): straight rays from s sources on the right
+    edge to p receivers on the left and top edges (row i*p + j for source i,
+    receiver j); x is the 'tectonic' phantom.  isDisp is not supported."""
+    s, p, sx, sy, rx, ry = seismic_tables(N, s, p)
+    A = seismic_operator(N, sx, sy, rx, ry, matrix_free=not isMatrix)
+    x = phantomgallery("tectonic", N).ravel(order="F")
+    b = A(x, "notransp")
+    return A, b, x, s, p
 
 
 def fanlineartomo(N, theta=None, p=None, R=None, dw=None, sd=None, isDisp=0, isMatrix=1):

@@ -12,7 +12,9 @@
  * Reference interfaces replaced (AIR Tools II V1.0, paths inside its tree):
  *   airt_problem_from_csc  -> auxil/check_inputs.m:67-71 (matrix wrapped as afun)
  *   airt_problem_parallel  -> testprobs/paralleltomo.m:112-301
- *   airt_problem_fan       -> testprobs/fanlineartomo.m:141-358
+ *   airt_problem_fan       -> testprobs/fanlineartomo.m:141-358,
+ *                             testprobs/fancurvedtomo.m:140-339
+ *   airt_problem_seismic   -> testprobs/seismictomo.m:96-287
  *   airt_apply             -> auxil/afun_matrix.m:44-53 and the isMatrix=0 handles
  *                             testprobs/paralleltomo.m:146-177,280-288
  *   airt_weights           -> auxil/get_mfun_dfun.m:43-250
@@ -135,6 +137,14 @@ int airt_problem_parallel(int N, int nA, const double *cos_t, const double *sin_
 int airt_problem_fan(int N, int nA, const double *cos_t, const double *sin_t, int p,
                      const double *cos_w, const double *sin_w, double R, int matrix_free,
                      airt_problem **out);
+
+/* seismictomo geometry (testprobs/seismictomo.m:96-287): s sources at
+ * (src_x, src_y), p receivers at (rcv_x, rcv_y); ray (i, j) runs from source i
+ * through receiver j and is row i*p + j.  The reference's defaults put the
+ * sources on the right edge and the receivers on the left and top edges. */
+int airt_problem_seismic(int N, int s, const double *src_x, const double *src_y, int p,
+                         const double *rcv_x, const double *rcv_y, int matrix_free,
+                         airt_problem **out);
 
 int airt_problem_size(const airt_problem *h, int64_t *m, int64_t *n, int64_t *nnz);
 int airt_problem_stream(const airt_problem *h, void **cuda_stream);

@@ -230,6 +230,45 @@ def fan_rays(N, R, cos_t, sin_t, cos_w, sin_w):
             yield i * p + j, x0t, y0t, a, b
 
 
+def seismic_geometry(N: int, s=None, p=None):
+    """Sources and receivers of seismictomo.m:67-75, 98-116: s (default N)
+    sources at x0 = N/2, y0 = linspace(-N/2+Ns, N/2-Ns, s), Ns = (N/s)/2;
+    p (default 2N) receivers, p2 = floor(p/2) at x = -N/2 with y =
+    linspace(-N/2+Np2, N/2-Np2, p2), then p1 = ceil(p/2) at y = N/2 with
+    x = linspace(-N/2+Np1, N/2-Np1, p1).  Returns (s, p, x0, y0, xp, yp)."""
+    s = N if s is None else int(s)
+    p = 2 * N if p is None else int(p)
+    N2 = N / 2.0
+    Ns = (N / s) / 2.0
+    x0 = N2 * np.ones(s)
+    y0 = linspace(-N2 + Ns, N2 - Ns, s)
+    p1 = int(math.ceil(p / 2.0))
+    p2 = int(math.floor(p / 2.0))
+    Np1 = (N / p1) / 2.0 if p1 > 0 else math.inf
+    Np2 = (N / p2) / 2.0 if p2 > 0 else math.inf
+    xp = np.concatenate([-N2 * np.ones(p2), linspace(-N2 + Np1, N2 - Np1, p1)])
+    yp = np.concatenate([linspace(-N2 + Np2, N2 - Np2, p2), N2 * np.ones(p1)])
+    return s, p, x0, y0, xp, yp
+
+
+def seismic_rays(x0, y0, xp, yp):
+    """Yield (row, x0(i), y0(i), a(j), b(j)) per ray, seismictomo.m:188-200:
+    a = xp - x0(i), b = yp - y0(i), row (i-1)*p + j (0-based here)."""
+    p = len(xp)
+    for i in range(len(x0)):
+        a = xp - x0[i]
+        b = yp - y0[i]
+        for j in range(p):
+            yield i * p + j, float(x0[i]), float(y0[i]), float(a[j]), float(b[j])
+
+
+def seismictomo_matrix(N, s=None, p=None) -> sp.csc_matrix:
+    """System matrix of seismictomo.m:96-287 (isMatrix=1)."""
+    s, p, x0, y0, xp, yp = seismic_geometry(N, s, p)
+    rows, cols, vals = trace_coo(N, seismic_rays(x0, y0, xp, yp), False)
+    return coo_to_csc(rows, cols, vals, s * p, N * N)
+
+
 def trace_coo(N, rays, exclude_top_right):
     """COO triplets of all rays in row order (the rows/cols/vals buffers of
     paralleltomo.m:266-278)."""
@@ -355,6 +394,40 @@ def ellipse_image(N, ellipses, clip_hi=None):
     if clip_hi is not None:
         X[X > clip_hi] = clip_hi
     return X
+
+
+def tectonic(N):
+    """phantomgallery.m:422-456, element by element with MATLAB's 1-based
+    (row, column) subscripts; returns the N x N image."""
+    x = np.zeros((N, N))
+    N5 = int(mround(N / 5))
+    N13 = int(mround(N / 13))
+    N7 = int(mround(N / 7))
+    N20 = int(mround(N / 20))
+
+    def setv(r, c, v):
+        assert 1 <= r <= N and 1 <= c <= N
+        x[r - 1, c - 1] = v
+
+    for r in range(N5, N5 + N7 + 1):               # the right plate
+        for c in range(5 * N13, N + 1):
+            setv(r, c, 0.75)
+    i = N5
+    for j in range(1, N20 + 1):                    # its sloped edge
+        if j % 2 != 0:
+            i = i - 1
+            for c in range(5 * N13 + j, N + 1):
+                setv(i, c, 0.75)
+    for r in range(N5, N5 + N5 + 1):               # the left plate
+        for c in range(1, 5 * N13 + 1):
+            setv(r, c, 1.0)
+    vector = list(range(N5, N5 + N5 + 1))          # the break
+    for j in range(5 * N13, min(12 * N13, N) + 1):
+        if j % 2 != 0:
+            vector = [v + 1 for v in vector]
+        for r in vector:
+            setv(r, j, 1.0)
+    return x
 
 
 def shepplogan(N):

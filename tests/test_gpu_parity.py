@@ -91,6 +91,29 @@ def test_fancurved_matrix_vs_c_oracle(N, theta, p, R, d):
     assert np.linalg.norm(y - Rm @ v) <= 1e-6 * np.linalg.norm(Rm @ v)
 
 
+@pytest.mark.parametrize("N,s,p", [(48, None, None), (31, 9, 40), (10, 1, 1)])
+def test_seismic_matrix_vs_c_oracle(N, s, p):
+    """seismictomo: bit-exact against the C tracer fed with the oracle's
+    source/receiver tables (horizontal rays included); b is A*x of the
+    tectonic phantom; matrix-free products agree."""
+    s_, p_, x0, y0, xp, yp = O.seismic_geometry(N, s, p)
+    rows, cols, vals = cbind.trace_coo(N, list(O.seismic_rays(x0, y0, xp, yp)), False)
+    Rm = O.coo_to_csc(rows, cols, vals, s_ * p_, N * N)
+    A, b, x, s2, p2 = airt.seismictomo(N, s, p)
+    assert (s2, p2) == (s_, p_)
+    same_matrix(A, Rm)
+    np.testing.assert_array_equal(x, O.tectonic(N).ravel(order="F"))
+    R32 = Rm.copy()
+    R32.data = R32.data.astype(np.float32).astype(np.float64)
+    np.testing.assert_allclose(b, R32 @ x, rtol=1e-12, atol=1e-12)
+    Amf, *_ = airt.seismictomo(N, s, p, 0, 0)
+    v = np.random.default_rng(N).random(N * N)
+    y = Amf(v, "notransp")
+    assert np.linalg.norm(y - Rm @ v) <= 1e-6 * np.linalg.norm(Rm @ v)
+    u = np.random.default_rng(N + 1).random(s_ * p_)
+    assert np.linalg.norm(Amf(u, "transp") - Rm.T @ u) <= 1e-6 * np.linalg.norm(Rm.T @ u)
+
+
 def test_c2_matrix_bit_exact_sampled_angles():
     """N=512, p=724 on 24 of the 360 half-degree angles (full-size rays)."""
     theta = (np.arange(360) * 0.5)[::15]

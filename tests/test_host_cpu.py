@@ -77,6 +77,21 @@ def test_shepplogan_matches_oracle():
                                       O.shepplogan(N))
 
 
+def test_seismic_tables_and_tectonic_match_oracle():
+    for N, s, p in [(64, None, None), (10, 3, 7), (33, 1, 2), (512, None, None)]:
+        a = testprobs.seismic_tables(N, s, p)
+        b = O.seismic_geometry(N, s, p)
+        assert a[:2] == b[:2]
+        for u, v in zip(a[2:], b[2:]):
+            np.testing.assert_array_equal(u, v)
+    for N in (10, 13, 64, 101, 256):
+        np.testing.assert_array_equal(testprobs.phantomgallery("tectonic", N), O.tectonic(N))
+    with pytest.raises(ValueError):
+        testprobs.tectonic(6)
+    with pytest.raises(ValueError):
+        testprobs.seismic_tables(8, [2, 3])
+
+
 def test_random_ellipses_range_and_determinism():
     x1 = testprobs.random_ellipses(48, 10, seed=5)
     x2 = testprobs.random_ellipses(48, 10, seed=5)

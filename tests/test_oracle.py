@@ -168,6 +168,32 @@ def test_c_tracer_matches_numpy_fan():
     assert (A1 != A0).nnz == 0
 
 
+@pytest.mark.parametrize("N,s,p", [(24, None, None), (17, 5, 9), (10, 1, 1)])
+def test_c_tracer_matches_numpy_seismic(N, s, p):
+    """seismictomo rays include horizontal ones (b = 0, all y-crossings at
+    t = +-inf) whenever a left-edge receiver sits level with a source."""
+    s_, p_, x0, y0, xp, yp = O.seismic_geometry(N, s, p)
+    rays = list(O.seismic_rays(x0, y0, xp, yp))
+    A1 = O.coo_to_csc(*cbind.trace_coo(N, rays, False), s_ * p_, N * N)
+    A0 = O.coo_to_csc(*O.trace_coo(N, rays, False), s_ * p_, N * N)
+    assert (A1 != A0).nnz == 0
+    assert np.array_equal(A1.indices, A0.indices)
+
+
+def test_seismic_rows_are_source_receiver_distances():
+    """Sources and receivers lie on the boundary, so the traced length of
+    every ray is the source-receiver distance."""
+    N = 16
+    s, p, x0, y0, xp, yp = O.seismic_geometry(N)
+    assert (s, p) == (16, 32)
+    rays = list(O.seismic_rays(x0, y0, xp, yp))
+    assert sum(1 for r in rays if r[4] == 0.0) == 16      # one level receiver per source
+    A = O.seismictomo_matrix(N).tocsr()
+    sums = np.asarray(A.sum(axis=1)).ravel()
+    for r, x0t, y0t, a, b in rays:
+        assert abs(sums[r] - math.hypot(a, b)) <= 1e-9
+
+
 # ---------------------------------------------------------------- invariants
 @pytest.fixture(scope="module")
 def small():
