@@ -12,11 +12,12 @@ from .unet import UNet
 from .solvers import (art, calczeta, cav, cimmino, drop, kaczmarz, landweber, randkaczmarz,
                       sart, sirt, symkaczmarz)
 from .testprobs import (add_noise, cosd, fancurvedtomo, fanlineartomo, paralleltomo, phantomgallery,
-                        random_ellipses, seismictomo, sind)
+                        random_ellipses, seismictomo, sind, sphericaltomo)
 
 _load_lib()
 
 __all__ = ["AirtError", "AirtOperator", "ParallelBatch", "UNet", "afun_matrix", "as_operator", "art", "calczeta", "cav",
            "cimmino", "drop", "kaczmarz", "landweber", "randkaczmarz", "sart", "sirt",
            "symkaczmarz", "add_noise", "cosd", "fancurvedtomo", "fanlineartomo", "paralleltomo", "seismictomo",
+           "sphericaltomo",
            "phantomgallery", "random_ellipses", "sind"]

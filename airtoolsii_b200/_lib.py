@@ -67,6 +67,8 @@ SIGNATURES = {
                                    C.c_int, C.POINTER(C.c_void_p)]),
     "airt_problem_seismic": (C.c_int, [C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_int,
                                        C.POINTER(C.c_void_p)]),
+    "airt_problem_spherical": (C.c_int, [C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _i64p, _dp,
+                                         _dp, C.c_int, C.POINTER(C.c_void_p)]),
     "airt_problem_size": (C.c_int, [C.c_void_p, _i64p, _i64p, _i64p]),
     "airt_problem_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "airt_problem_export_csc": (C.c_int, [C.c_void_p, _u64p, _u64p, _dp]),

@@ -24,7 +24,7 @@ class AirtOperator:
 
     def __init__(self, handle: C.c_void_p, kind: str, geometry: dict | None = None):
         self._h = handle
-        self.kind = kind                  # 'matrix', 'parallel', 'fan'
+        self.kind = kind                  # 'matrix', 'parallel', 'fan', 'seismic', 'spherical'
         self.geometry = geometry or {}
         m, n, nnz = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().airt_problem_size(self._h, C.byref(m), C.byref(n), C.byref(nnz)))

@@ -106,6 +106,10 @@ __device__ __forceinline__ Ray batch_ray(const InstGeom &gk, const double *cos_t
   g.offsets = offs + gk.off0;
   g.cos_w = g.sin_w = nullptr;
   g.src_x = g.src_y = g.rcv_x = g.rcv_y = nullptr;
+  g.radius = g.cscale = g.cos_k = g.sin_k = nullptr;
+  g.koff = nullptr;
+  g.dx = 0;
+  g.center = 0;
   return ray_of(g, local);
 }
 

@@ -224,6 +224,54 @@ int airt_problem_seismic(int N, int s, const double *src_x, const double *src_y,
   AIRT_API_END
 }
 
+int airt_problem_spherical(int N, int nA, const double *cos_t, const double *sin_t, int nc,
+                           const double *radius, const int64_t *nphi, const double *cos_k,
+                           const double *sin_k, int matrix_free, airt_problem **out) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(out, "null pointer argument");
+  AIRT_REQUIRE((cos_t && sin_t) || nA == 0, "null pointer argument");
+  AIRT_REQUIRE((radius && nphi) || nc == 0, "null pointer argument");
+  AIRT_REQUIRE(N >= 1 && N <= 46340 && nA >= 0 && nc >= 0, "geometry size out of range");
+  AIRT_REQUIRE((int64_t)nA * nc < INT32_MAX, "too many rows");
+  std::vector<int64_t> koff(nc + 1, 0);
+  std::vector<double> cscale(nc);
+  for (int n = 0; n < nc; ++n) {
+    AIRT_REQUIRE(nphi[n] >= 1, "nphi must be positive");
+    koff[n + 1] = koff[n] + nphi[n] + 1;  // k = (0:nPhi)*dPhi, sphericaltomo.m:203
+    // 2*pi*radii(n)/nPhi(n), sphericaltomo.m:234
+    cscale[n] = 2.0 * 3.141592653589793 * radius[n] / (double)nphi[n];
+  }
+  AIRT_REQUIRE(koff[nc] < INT32_MAX, "too many samples per angle");
+  AIRT_REQUIRE(koff[nc] == 0 || (cos_k && sin_k), "null pointer argument");
+  Problem *P = new_problem();
+  try {
+    P->geo_kind = GEO_SPHERE;
+    P->N = N;
+    P->nA = nA;
+    P->p = nc;
+    P->m = (int64_t)nA * nc;
+    P->n = (int64_t)N * N;
+    P->matrix_free = matrix_free != 0;
+    P->dx = std::sqrt(2.0) / N;           // sphericaltomo.m:122
+    P->center = (N + 1) / 2;              // ceil(N/2), sphericaltomo.m:119
+    P->koff_total = koff[nc];
+    P->cos_t.upload(cos_t, nA, P->stream);
+    P->sin_t.upload(sin_t, nA, P->stream);
+    P->radius.upload(radius, nc, P->stream);
+    P->cscale.upload(cscale.data(), nc, P->stream);
+    P->koff.upload(koff.data(), nc + 1, P->stream);
+    P->cos_k.upload(cos_k, koff[nc], P->stream);
+    P->sin_k.upload(sin_k, koff[nc], P->stream);
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
+    if (!P->matrix_free) generate_matrix(*P);
+  } catch (...) {
+    free_problem(P);
+    throw;
+  }
+  *out = reinterpret_cast<airt_problem *>(P);
+  AIRT_API_END
+}
+
 int airt_problem_size(const airt_problem *h, int64_t *m, int64_t *n, int64_t *nnz) {
   AIRT_API_BEGIN
   AIRT_REQUIRE(h, "null problem handle");

@@ -90,11 +90,13 @@ struct DevBuf {
 };
 
 // ---------------------------------------------------------------- geometry
-enum GeoKind { GEO_NONE = 0, GEO_PARALLEL = 1, GEO_FAN = 2, GEO_SEISMIC = 3 };
+enum GeoKind { GEO_NONE = 0, GEO_PARALLEL = 1, GEO_FAN = 2, GEO_SEISMIC = 3, GEO_SPHERE = 4 };
 
 // Per-ray parameters of the geometries, prepared on the device: ray
 // r = i*p + j (i = angle or source, j = detector or receiver) starts at
-// (x0t, y0t) with direction (a, b).
+// (x0t, y0t) with direction (a, b).  For GEO_SPHERE, row r = i*p + n is
+// circle n of radius radius[n] about (cos_t[i], sin_t[i]), sampled at the
+// angles whose cosines and sines are cos_k/sin_k[koff[n] .. koff[n+1]).
 struct RayGeom {
   int kind;
   int N, nA, p;
@@ -104,6 +106,11 @@ struct RayGeom {
   const double *cos_w, *sin_w;  // p (fan)
   const double *src_x, *src_y;  // nA sources (seismic)
   const double *rcv_x, *rcv_y;  // p receivers (seismic)
+  const double *radius, *cscale;  // p circles: radius, entry value per hit (sphere)
+  const int64_t *koff;            // p + 1 sample offsets (sphere)
+  const double *cos_k, *sin_k;    // koff[p] samples (sphere)
+  double dx;                      // pixel size sqrt(2)/N (sphere)
+  int center;                     // ceil(N/2) (sphere)
 };
 
 // ---------------------------------------------------------------- SIRT state
@@ -145,6 +152,11 @@ struct Problem {
   double R = 0;
   DevBuf<double> cos_t, sin_t, offsets, cos_w, sin_w;
   DevBuf<double> src_x, src_y, rcv_x, rcv_y;  // seismic: nA sources, p receivers
+  DevBuf<double> radius, cscale, cos_k, sin_k;  // sphere: p circles and their samples
+  DevBuf<int64_t> koff;
+  int64_t koff_total = 0;  // samples per angle
+  double dx = 0;
+  int center = 0;
 
   // stored matrix: CSR over rays (rows) and CSC over pixels (columns)
   DevBuf<int64_t> rp, cp;
@@ -199,6 +211,13 @@ struct Problem {
     g.src_y = src_y.p;
     g.rcv_x = rcv_x.p;
     g.rcv_y = rcv_y.p;
+    g.radius = radius.p;
+    g.cscale = cscale.p;
+    g.koff = koff.p;
+    g.cos_k = cos_k.p;
+    g.sin_k = sin_k.p;
+    g.dx = dx;
+    g.center = center;
     return g;
   }
 };
@@ -229,6 +248,11 @@ void prof_collect(Problem &P);
 
 // Kernel drivers implemented in the .cu files.
 void build_csc_from_csr(Problem &P);
+// sphericaltomo (sphere.cu): the system matrix, and the exact row/column
+// statistics of its matrix-free operator
+void generate_sphere_matrix(Problem &P);
+void sphere_stats(Problem &P, double *s2, double *s1, double *colcnt, double *cols1,
+                  const double *colw, double *s2w);
 void build_csr_from_host_csc(Problem &P, const uint64_t *jc, const uint64_t *ir, const double *pr);
 void finalize_matrix(Problem &P);
 void generate_matrix(Problem &P);

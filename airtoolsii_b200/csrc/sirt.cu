@@ -137,9 +137,8 @@ __global__ void __launch_bounds__(128)
   const int64_t nn = (int64_t)g.N * g.N;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
        r += (int64_t)gridDim.x * blockDim.x) {
-    const Ray q = ray_of(g, r);
     double acc = 0.0;
-    trace_entries(g.N, q, excl, [&](int col, double v) {
+    row_entries(g, r, excl, [&](int col, double v) {
       if (col >= 0 && col < nn) acc = fma((double)(float)v, (double)x32[col], acc);
     });
     resid_row<ME>(r, acc, o, a);

@@ -1,5 +1,6 @@
 // GPU system-matrix generation and matrix-free projectors for the
-// paralleltomo / fanlineartomo / fancurvedtomo / seismictomo geometries.
+// paralleltomo / fanlineartomo / fancurvedtomo / seismictomo geometries (and
+// the matrix-free products of sphericaltomo, whose matrix is in sphere.cu).
 //
 //  * generate_matrix: two passes over the rays (count, then fill) with an
 //    exclusive scan in between give the CSR over rays; the CSC follows by a
@@ -59,9 +60,8 @@ __global__ void k_mf_forward(RayGeom g, int64_t nrays, bool excl, const double *
   const int64_t nn = (int64_t)g.N * g.N;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
        r += (int64_t)gridDim.x * blockDim.x) {
-    const Ray q = ray_of(g, r);
     double acc = 0.0;
-    trace_entries(g.N, q, excl, [&](int col, double v) {
+    row_entries(g, r, excl, [&](int col, double v) {
       if (col >= 0 && col < nn) acc = fma((double)(float)v, x[col], acc);
     });
     y[r] = acc;
@@ -75,8 +75,7 @@ __global__ void k_mf_adjoint(RayGeom g, int64_t nrays, bool excl, const double *
        r += (int64_t)gridDim.x * blockDim.x) {
     const double ur = u[r];
     if (ur == 0.0) continue;
-    const Ray q = ray_of(g, r);
-    trace_entries(g.N, q, excl, [&](int col, double v) {
+    row_entries(g, r, excl, [&](int col, double v) {
       if (col >= 0 && col < nn) atomicAdd(y + col, (double)(float)v * ur);
     });
   }
@@ -113,6 +112,10 @@ inline bool excl_of(const Problem &P) { return P.geo_kind == GEO_PARALLEL; }
 }  // namespace
 
 void generate_matrix(Problem &P) {
+  if (P.geo_kind == GEO_SPHERE) {
+    generate_sphere_matrix(P);
+    return;
+  }
   cudaStream_t s = P.stream;
   const RayGeom g = P.geom();
   const int64_t nrays = P.m;
@@ -158,6 +161,10 @@ void apply_matrix_free(Problem &P, const double *d_in, double *d_out, int transp
 
 void row_col_stats_mf(Problem &P, double *s2, double *s1, double *colcnt, double *cols1,
                       const double *colw, double *s2w) {
+  if (P.geo_kind == GEO_SPHERE) {  // a circle's hits need merging into (pixel, count) first
+    sphere_stats(P, s2, s1, colcnt, cols1, colw, s2w);
+    return;
+  }
   cudaStream_t s = P.stream;
   if (colcnt) AIRT_CHECK_CUDA(cudaMemsetAsync(colcnt, 0, P.n * sizeof(double), s));
   if (cols1) AIRT_CHECK_CUDA(cudaMemsetAsync(cols1, 0, P.n * sizeof(double), s));
@@ -176,8 +183,7 @@ __global__ void k_mf_adjoint_f32(RayGeom g, int64_t nrays, bool excl, const floa
        r += (int64_t)gridDim.x * blockDim.x) {
     const double ur = (double)u[r];
     if (ur == 0.0) continue;
-    const Ray q = ray_of(g, r);
-    trace_entries(g.N, q, excl, [&](int col, double v) {
+    row_entries(g, r, excl, [&](int col, double v) {
       if (col >= 0 && col < nn) atomicAdd(y + col, (double)(float)v * ur);
     });
   }

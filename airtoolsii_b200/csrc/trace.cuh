@@ -168,4 +168,40 @@ __device__ __forceinline__ void trace_entries(int N, const Ray &q, bool exclude_
     if (k < cnt) emit(wc[k], wv[k]);
 }
 
+// sphericaltomo (testprobs/sphericaltomo.m:203-224): sample k of a circle of
+// radius rad about (xix, yiy) lands in the pixel (round(xx), round(yy)) of
+// xx = (xix + rad*cos(k))/dx + ceil(N/2); returns its 0-based column-major
+// index, or -1 outside the image.  round() rounds halves away from zero, as
+// MATLAB's round does; the cosines and sines come from the host tables.
+__device__ __forceinline__ int sphere_pixel(const RayGeom &g, double xix, double xiy, double rad,
+                                            int64_t k) {
+  const double xx =
+      __dadd_rn(__ddiv_rn(__dadd_rn(xix, __dmul_rn(rad, g.cos_k[k])), g.dx), (double)g.center);
+  const double yy =
+      __dadd_rn(__ddiv_rn(__dadd_rn(xiy, __dmul_rn(rad, g.sin_k[k])), g.dx), (double)g.center);
+  const double col = round(xx), row = round(yy);
+  if (!(col > 0.0 && col <= (double)g.N && row > 0.0 && row <= (double)g.N)) return -1;
+  return (g.N - (int)row) + ((int)col - 1) * g.N;
+}
+
+// The entries of row r for the linear operators (products and the SIRT
+// residual): a straight ray's merged (pixel, length) pairs, or, for a circle,
+// one (pixel, 2*pi*r/nPhi) pair per sample inside the image -- a pixel hit w
+// times appears w times, which sums to the reference's w*2*pi*r/nPhi.
+template <class Emit>
+__device__ __forceinline__ void row_entries(const RayGeom &g, int64_t r, bool exclude_top_right,
+                                            Emit &&emit) {
+  if (g.kind == GEO_SPHERE) {
+    const int i = (int)(r / g.p);
+    const int n = (int)(r - (int64_t)i * g.p);
+    const double xix = g.cos_t[i], xiy = g.sin_t[i], rad = g.radius[n], c = g.cscale[n];
+    for (int64_t k = g.koff[n]; k < g.koff[n + 1]; ++k) {
+      const int J = sphere_pixel(g, xix, xiy, rad, k);
+      if (J >= 0) emit(J, c);
+    }
+    return;
+  }
+  trace_entries(g.N, ray_of(g, r), exclude_top_right, emit);
+}
+
 }  // namespace airt

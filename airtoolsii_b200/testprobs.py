@@ -1,9 +1,10 @@
 """Tomography test problems on the GPU: paralleltomo, fanlineartomo,
-fancurvedtomo and seismictomo.
+fancurvedtomo, seismictomo and sphericaltomo.
 
 The host side prepares the per-angle and per-detector tables in FP64 exactly
 as the reference does (cosd/sind of the angles, linspace ray offsets, the
-fan's atand detector angles, the seismic source and receiver positions);
+fan's atand detector angles, the seismic source and receiver positions, the
+cosines and sines of every circle sample of sphericaltomo);
 libairt traces every ray on the device and
 either stores A (FP32 CSR + CSC, bit-exact sparsity with the FP64 trace) or
 keeps the geometry for matrix-free projection.
@@ -244,6 +245,46 @@ def seismic_operator(N, src_x, src_y, rcv_x, rcv_y, matrix_free=False) -> AirtOp
     return AirtOperator(h, "seismic", dict(N=N, s=sx.size, p=rx.size))
 
 
+def _round_half_away(x):
+    a = np.abs(x)
+    f = np.floor(a)
+    return np.copysign(f + ((a - f) >= 0.5), x)
+
+
+def sphere_tables(N, angles=None, numCircles=None):
+    """sphericaltomo.m:64-75,115-124,203-205: (angles, numCircles, cos_t,
+    sin_t, radii, nphi, cos_k, sin_k).  Circle n of radius radii[n] =
+    linspace(0,2,numCircles+1)(n+1) is sampled at k = (0:nphi[n])*dPhi,
+    nphi = ceil((4*pi/dx)*radii), dPhi = 2*pi/nphi, dx = sqrt(2)/N; cos_k and
+    sin_k hold cos(k), sin(k) circle after circle."""
+    N = int(N)
+    angles = np.arange(0.0, 359.0, 2.0) if angles is None else np.asarray(angles, float).ravel()
+    nc = int(_round_half_away(math.sqrt(2.0) * N)) if numCircles is None else int(numCircles)
+    radii = _linspace(0.0, 2.0, nc + 1)[1:]
+    dx = math.sqrt(2.0) / N
+    nphi = np.ceil((4.0 * math.pi / dx) * radii).astype(np.int64)
+    dphi = 2.0 * math.pi / nphi
+    k = np.concatenate([np.arange(int(q) + 1, dtype=float) * d for q, d in zip(nphi, dphi)]) \
+        if nc else np.zeros(0)
+    return angles, nc, cosd(angles), sind(angles), radii, nphi, np.cos(k), np.sin(k)
+
+
+def sphere_operator(N, cos_t, sin_t, radii, nphi, cos_k, sin_k, matrix_free=False) -> AirtOperator:
+    ct = np.ascontiguousarray(cos_t, np.float64)
+    st = np.ascontiguousarray(sin_t, np.float64)
+    rd = np.ascontiguousarray(radii, np.float64)
+    nphi = np.ascontiguousarray(nphi, np.int64)
+    ck = np.ascontiguousarray(cos_k, np.float64)
+    sk = np.ascontiguousarray(sin_k, np.float64)
+    if nphi.size != rd.size or ck.size != sk.size or ck.size != int(np.sum(nphi + 1)):
+        raise ValueError("circle tables need one nphi per radius and nphi+1 samples per circle")
+    h = C.c_void_p()
+    check(lib().airt_problem_spherical(int(N), ct.size, dptr(ct), dptr(st), rd.size, dptr(rd),
+                                       nphi.ctypes.data_as(C.POINTER(C.c_int64)), dptr(ck), dptr(sk),
+                                       int(bool(matrix_free)), C.byref(h)))
+    return AirtOperator(h, "spherical", dict(N=N, nA=ct.size, nc=rd.size))
+
+
 def parallel_operator(N, cos_t, sin_t, offsets, matrix_free=False) -> AirtOperator:
     ct = np.ascontiguousarray(cos_t, np.float64)
     st = np.ascontiguousarray(sin_t, np.float64)
@@ -299,6 +340,18 @@ def seismictomo(N, s=None, p=None, isDisp=0, isMatrix=1):
     x = phantomgallery("tectonic", N).ravel(order="F")
     b = A(x, "notransp")
     return A, b, x, s, p
+
+
+def sphericaltomo(N, angles=None, numCircles=None, isDisp=0, isMatrix=1):
+    """[A,b,x,angles,numCircles] = sphericaltomo(N,angles,numCircles,isDisp,isMatrix)
+    (testprobs/sphericaltomo.m:1): spherical-means (circle) integrals about
+    centres on the unit circle at the given angles; x is the Shepp-Logan
+    phantom.  isDisp is not supported."""
+    angles, nc, ct, st, radii, nphi, ck, sk = sphere_tables(N, angles, numCircles)
+    A = sphere_operator(N, ct, st, radii, nphi, ck, sk, matrix_free=not isMatrix)
+    x = phantomgallery("shepplogan", N).ravel(order="F")
+    b = A(x, "notransp")
+    return A, b, x, angles, nc
 
 
 def fanlineartomo(N, theta=None, p=None, R=None, dw=None, sd=None, isDisp=0, isMatrix=1):

@@ -15,6 +15,7 @@
  *   airt_problem_fan       -> testprobs/fanlineartomo.m:141-358,
  *                             testprobs/fancurvedtomo.m:140-339
  *   airt_problem_seismic   -> testprobs/seismictomo.m:96-287
+ *   airt_problem_spherical -> testprobs/sphericaltomo.m:108-270
  *   airt_apply             -> auxil/afun_matrix.m:44-53 and the isMatrix=0 handles
  *                             testprobs/paralleltomo.m:146-177,280-288
  *   airt_weights           -> auxil/get_mfun_dfun.m:43-250
@@ -145,6 +146,16 @@ int airt_problem_fan(int N, int nA, const double *cos_t, const double *sin_t, in
 int airt_problem_seismic(int N, int s, const double *src_x, const double *src_y, int p,
                          const double *rcv_x, const double *rcv_y, int matrix_free,
                          airt_problem **out);
+
+/* sphericaltomo geometry (testprobs/sphericaltomo.m:108-270): nA centre
+ * angles as cosd/sind tables; nc circles of radius radius[n] (linspace(0,2,
+ * nc+1)(2:end)), each sampled at the nphi[n] + 1 angles k = (0:nphi[n]) *
+ * (2*pi/nphi[n]) whose cosines and sines the caller passes in cos_k / sin_k,
+ * circle after circle.  Row i*nc + n holds, for every pixel the samples of
+ * circle n about angle i hit w times, the value 2*pi*radius[n]/nphi[n] * w. */
+int airt_problem_spherical(int N, int nA, const double *cos_t, const double *sin_t, int nc,
+                           const double *radius, const int64_t *nphi, const double *cos_k,
+                           const double *sin_k, int matrix_free, airt_problem **out);
 
 int airt_problem_size(const airt_problem *h, int64_t *m, int64_t *n, int64_t *nnz);
 int airt_problem_stream(const airt_problem *h, void **cuda_stream);

@@ -269,6 +269,69 @@ def seismictomo_matrix(N, s=None, p=None) -> sp.csc_matrix:
     return coo_to_csc(rows, cols, vals, s * p, N * N)
 
 
+def mround_array(x) -> np.ndarray:
+    """MATLAB ``round`` on an array: nearest integer, halves away from zero
+    (x - floor(x) is exact for the magnitudes used here)."""
+    x = np.asarray(x, float)
+    a = np.abs(x)
+    f = np.floor(a)
+    r = f + ((a - f) >= 0.5)
+    return np.copysign(r, x)
+
+
+def sphere_geometry(N: int, angles=None, numCircles=None):
+    """sphericaltomo.m:64-75, 115-124: angles (default 0:2:358), numCircles
+    (default round(sqrt(2)*N)), radii = linspace(0,2,numCircles+1)(2:end),
+    centerImg = ceil(N/2), dx = sqrt(2)/N, nPhi = ceil((4*pi/dx)*radii),
+    dPhi = 2*pi./nPhi.  Returns (angles, numCircles, radii, nPhi, dPhi,
+    centerImg, dx)."""
+    angles = np.arange(0.0, 359.0, 2.0) if angles is None else np.asarray(angles, float).ravel()
+    nc = int(mround(math.sqrt(2.0) * N)) if numCircles is None else int(numCircles)
+    radii = linspace(0.0, 2.0, nc + 1)[1:]
+    center = int(math.ceil(N / 2.0))
+    dx = math.sqrt(2.0) / N
+    nphi = np.ceil((4.0 * math.pi / dx) * radii).astype(np.int64)
+    dphi = 2.0 * math.pi / nphi
+    return angles, nc, radii, nphi, dphi, center, dx
+
+
+def sphere_circle_tables(nphi, dphi):
+    """cos(k), sin(k) of k = (0:nPhi(n))*dPhi(n), sphericaltomo.m:203-205,
+    concatenated circle after circle."""
+    ks = [np.arange(int(n) + 1, dtype=float) * d for n, d in zip(nphi, dphi)]
+    k = np.concatenate(ks) if ks else np.zeros(0)
+    return np.cos(k), np.sin(k)
+
+
+def sphericaltomo_matrix(N, angles=None, numCircles=None) -> sp.csc_matrix:
+    """System matrix of sphericaltomo.m:108-270 (isMatrix=1): per circle the
+    samples' pixels, unique(J) and histc counts w, values
+    (2*pi*radii(n)/nPhi(n))*w; row (m-1)*numCircles + n."""
+    angles, nc, radii, nphi, dphi, center, dx = sphere_geometry(N, angles, numCircles)
+    ck, sk = sphere_circle_tables(nphi, dphi)
+    off = np.concatenate([[0], np.cumsum(nphi + 1)])
+    xi_c, xi_s = cosd(angles), sind(angles)
+    R, Cc, V = [], [], []
+    for m in range(len(angles)):
+        for n in range(nc):
+            c, s_ = ck[off[n]:off[n + 1]], sk[off[n]:off[n + 1]]
+            xx = (xi_c[m] + radii[n] * c) / dx + center
+            yy = (xi_s[m] + radii[n] * s_) / dx + center
+            col = mround_array(xx)
+            row = mround_array(yy)
+            keep = (col > 0) & (col <= N) & (row > 0) & (row <= N)
+            J = (N - row[keep] + 1) + (col[keep] - 1) * N
+            Ju, w = np.unique(J, return_counts=True)
+            if Ju.size:
+                R.append(np.full(Ju.size, m * nc + n, np.int64))
+                Cc.append(Ju.astype(np.int64) - 1)
+                V.append((2.0 * math.pi * radii[n] / nphi[n]) * w.astype(float))
+    if not R:
+        return sp.csc_matrix((len(angles) * nc, N * N))
+    return coo_to_csc(np.concatenate(R), np.concatenate(Cc), np.concatenate(V),
+                      len(angles) * nc, N * N)
+
+
 def trace_coo(N, rays, exclude_top_right):
     """COO triplets of all rays in row order (the rows/cols/vals buffers of
     paralleltomo.m:266-278)."""

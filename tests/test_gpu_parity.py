@@ -114,6 +114,35 @@ def test_seismic_matrix_vs_c_oracle(N, s, p):
     assert np.linalg.norm(Amf(u, "transp") - Rm.T @ u) <= 1e-6 * np.linalg.norm(Rm.T @ u)
 
 
+@pytest.mark.parametrize("N,angles,nc", [(16, None, None), (33, [0.0, 45.0, 97.5, 200.0], 7),
+                                         (40, np.arange(0.0, 360.0, 24.0), None)])
+def test_spherical_matrix_vs_oracle(N, angles, nc):
+    """sphericaltomo: bit-exact against the oracle's unique/histc restatement
+    (same circle-sample tables); matrix-free products within the FP32 entry
+    rounding, matrix-free SIRT weights equal to the stored matrix's."""
+    Ro = O.sphericaltomo_matrix(N, angles, nc)
+    A, b, x, ang, nc2 = airt.sphericaltomo(N, angles, nc)
+    assert nc2 == Ro.shape[0] // len(ang)
+    same_matrix(A, Ro)
+    R32 = Ro.copy()
+    R32.data = R32.data.astype(np.float32).astype(np.float64)
+    np.testing.assert_allclose(b, R32 @ x, rtol=1e-12, atol=1e-12)
+    Amf, *_ = airt.sphericaltomo(N, angles, nc, 0, 0)
+    assert Amf.matrix_free
+    v = np.random.default_rng(N).random(N * N)
+    assert np.linalg.norm(Amf(v, "notransp") - Ro @ v) <= 1e-6 * np.linalg.norm(Ro @ v)
+    u = np.random.default_rng(N + 1).random(Ro.shape[0])
+    assert np.linalg.norm(Amf(u, "transp") - Ro.T @ u) <= 1e-6 * np.linalg.norm(Ro.T @ u)
+    for meth in ("cimmino", "cav", "drop", "sart"):
+        Ms, Ds = A.weights(meth)
+        Mm, Dm = Amf.weights(meth)
+        np.testing.assert_allclose(Mm, Ms, rtol=1e-12)
+        np.testing.assert_allclose(Dm, Ds, rtol=1e-12)
+    Xs, info = airt.cimmino(A, b, 20)
+    Xm, _ = airt.cimmino(Amf, b, 20, None, {"rho": info["rho"]})
+    assert relerr(Xm, Xs) <= 1e-5
+
+
 def test_c2_matrix_bit_exact_sampled_angles():
     """N=512, p=724 on 24 of the 360 half-degree angles (full-size rays)."""
     theta = (np.arange(360) * 0.5)[::15]

@@ -92,6 +92,19 @@ def test_seismic_tables_and_tectonic_match_oracle():
         testprobs.seismic_tables(8, [2, 3])
 
 
+def test_sphere_tables_match_oracle():
+    for N, ang, nc in [(16, None, None), (33, [0.0, 45.0, 97.5], 7), (128, None, None)]:
+        t = testprobs.sphere_tables(N, ang, nc)
+        angles, nc_, radii, nphi, dphi, center, dx = O.sphere_geometry(N, ang, nc)
+        ck, sk = O.sphere_circle_tables(nphi, dphi)
+        assert t[1] == nc_
+        for u, v in zip(t[:1] + t[2:], (angles, O.cosd(angles), O.sind(angles), radii, nphi, ck, sk)):
+            np.testing.assert_array_equal(u, v)
+    x = np.array([-2.5, -1.5, -0.5, 0.5, 1.5, 2.4999999999999996, 0.49999999999999994, 3.0])
+    np.testing.assert_array_equal(testprobs._round_half_away(x), [-3, -2, -1, 1, 2, 2, 0, 3])
+    np.testing.assert_array_equal(O.mround_array(x), [-3, -2, -1, 1, 2, 2, 0, 3])
+
+
 def test_random_ellipses_range_and_determinism():
     x1 = testprobs.random_ellipses(48, 10, seed=5)
     x2 = testprobs.random_ellipses(48, 10, seed=5)

@@ -194,6 +194,30 @@ def test_seismic_rows_are_source_receiver_distances():
         assert abs(sums[r] - math.hypot(a, b)) <= 1e-9
 
 
+def test_sphere_rows_count_in_image_samples():
+    """Every sample of a circle that lands in the image adds 2*pi*r/nPhi to its
+    row (sphericaltomo.m:224-234): the row sum is that times the number of
+    in-image samples, counted here with scalar MATLAB rounding."""
+    N = 12
+    angles = np.array([0.0, 90.0, 225.0])
+    A = O.sphericaltomo_matrix(N, angles).tocsr()
+    ang, nc, radii, nphi, dphi, center, dx = O.sphere_geometry(N, angles)
+    ck, sk = O.sphere_circle_tables(nphi, dphi)
+    off = np.concatenate([[0], np.cumsum(nphi + 1)])
+    sums = np.asarray(A.sum(axis=1)).ravel()
+    for m, a in enumerate(ang):
+        xc, yc = O.cosd(a)[0], O.sind(a)[0]
+        for n in range(nc):
+            hits = 0
+            for k in range(off[n], off[n + 1]):
+                col = O.mround((xc + radii[n] * ck[k]) / dx + center)
+                row = O.mround((yc + radii[n] * sk[k]) / dx + center)
+                hits += (1 <= col <= N) and (1 <= row <= N)
+            want = (2 * math.pi * radii[n] / nphi[n]) * hits
+            assert abs(sums[m * nc + n] - want) <= 1e-12 * max(1.0, want)
+    assert A.nnz > 0 and np.all(A.data > 0)
+
+
 # ---------------------------------------------------------------- invariants
 @pytest.fixture(scope="module")
 def small():
