@@ -9,14 +9,14 @@ from ._lib import AirtError, lib as _load_lib
 from .afun import AirtOperator, afun_matrix, as_operator
 from .batch import ParallelBatch
 from .unet import UNet
-from .solvers import (art, calczeta, cav, cimmino, drop, kaczmarz, landweber, randkaczmarz,
-                      sart, sirt, symkaczmarz)
+from .solvers import (art, calczeta, cart, cav, cimmino, columnaction, drop, kaczmarz, landweber,
+                      randkaczmarz, sart, sirt, symkaczmarz)
 from .testprobs import (add_noise, cosd, fancurvedtomo, fanlineartomo, paralleltomo, phantomgallery,
                         random_ellipses, seismictomo, sind, sphericaltomo)
 
 _load_lib()
 
-__all__ = ["AirtError", "AirtOperator", "ParallelBatch", "UNet", "afun_matrix", "as_operator", "art", "calczeta", "cav",
+__all__ = ["AirtError", "AirtOperator", "ParallelBatch", "UNet", "afun_matrix", "as_operator", "art", "calczeta", "cart", "cav", "columnaction",
            "cimmino", "drop", "kaczmarz", "landweber", "randkaczmarz", "sart", "sirt",
            "symkaczmarz", "add_noise", "cosd", "fancurvedtomo", "fanlineartomo", "paralleltomo", "seismictomo",
            "sphericaltomo",

@@ -50,6 +50,16 @@ class ArtOpts(C.Structure):
                 ("ncp_rows", C.c_int), ("ncp_cols", C.c_int), ("ncp_smooth", C.c_int)]
 
 
+class CartOpts(C.Structure):
+    _fields_ = [("order_kind", C.c_int), ("cols", _i64p), ("ncols", C.c_int64),
+                ("relaxpar", C.c_double), ("damp", C.c_double), ("stoprule", C.c_int),
+                ("taudelta", C.c_double), ("lb_kind", C.c_int), ("ub_kind", C.c_int),
+                ("lb", C.c_double), ("ub", C.c_double), ("lbv", _dp), ("ubv", _dp),
+                ("kmax", C.c_int64), ("ncp_rows", C.c_int), ("ncp_cols", C.c_int),
+                ("ncp_smooth", C.c_int), ("thr", C.c_double), ("kbegin", C.c_int64),
+                ("nunflag", C.c_int64), ("seed", C.c_uint64)]
+
+
 class Info(C.Structure):
     _fields_ = [("stoprule", C.c_int), ("finaliter", C.c_int64), ("relaxpar", C.c_double),
                 ("nsaved", C.c_int64), ("gpu_ms", C.c_double)]
@@ -83,6 +93,8 @@ SIGNATURES = {
                                    C.c_int64, C.c_void_p, _dp, C.POINTER(Info)]),
     "airt_art": (C.c_int, [C.c_void_p, C.POINTER(ArtOpts), _dp, _dp, _i64p, C.c_int64, _dp, _dp,
                            C.POINTER(Info)]),
+    "airt_cart": (C.c_int, [C.c_void_p, C.POINTER(CartOpts), _dp, _dp, _i64p, C.c_int64, _dp, _dp,
+                            C.POINTER(Info)]),
     "airt_batch_parallel": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), _dp, _dp, _dp, C.POINTER(C.c_void_p)]),
     "airt_batch_layout": (C.c_int, [C.c_void_p, _i64p, _i64p, _i64p]),

@@ -277,7 +277,7 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
   // ncp_smooth history (check_inputs.m:209, +inf initially)
   DevBuf<double> r64, tw, pk, ccol;
   const int q = ncp ? o.ncp_rows / 2 : 0;
-  std::vector<double> dk(ncp ? o.ncp_smooth : 0, INFINITY), hcol(ncp ? o.ncp_cols : 0);
+  std::vector<double> hcol(ncp ? o.ncp_cols : 0);
   if (ncp) {
     r64.ensure(m);
     const std::vector<double> t = ncp_twiddles(o.ncp_rows);
@@ -315,36 +315,12 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
 
   std::vector<double> resn;
   resn.push_back(resid());
-  int stoprule = 0;
-  int64_t finaliter = 0;
-  bool stop = false;
-  auto judge = [&](int64_t k, double nrk) {
-    if (o.stoprule == AIRT_STOP_DP) {
-      if (nrk <= o.taudelta || k >= kmax) {
-        stop = true;
-        stoprule = (k != kmax) ? 2 : 0;
-      }
-    } else if (ncp) {  // check_stoprules.m:124-149 on the ncc of this residual
-      double mx = -INFINITY, mxn = ncc;
-      for (double v : dk) mx = std::fmax(mx, v);
-      for (size_t i = 1; i < dk.size(); ++i) mxn = std::fmax(mxn, dk[i]);
-      if (mx < mxn || k >= kmax) {
-        stop = true;
-        stoprule = (k != kmax) ? 1 : 0;
-      } else {
-        dk.erase(dk.begin());
-        dk.push_back(ncc);
-      }
-    } else if (k >= kmax) {
-      stop = true;
-    }
-    if (stop) finaliter = k;
-  };
-  judge(0, resn[0]);
+  SweepStop st(o.stoprule, o.taudelta, kmax, o.ncp_smooth);
+  st.judge(0, resn[0], ncc);
   int64_t l = 0;
   const bool bounded = o.lb_kind != AIRT_BOUND_NONE || o.ub_kind != AIRT_BOUND_NONE;
   double lam_last = o.relaxpar;
-  for (int64_t k = 1; !stop; ++k) {
+  for (int64_t k = 1; !st.stop; ++k) {
     const int64_t *ord = order.data() + (per_sweep_sched ? (k - 1) * per_sweep : 0);
     if (per_sweep_sched) build_schedule(hrp, hci, ord, per_sweep, n, S, s);
     if (k == 1 && bounded && per_sweep > 0) {
@@ -359,8 +335,8 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
     if (o.relax_table && per_sweep > 0) lam_last = o.relax_table[(k - 1) * per_sweep + per_sweep - 1];
     const double nrk = resid();
     resn.push_back(nrk);
-    judge(k, nrk);
-    if ((l < nK && k == K[l]) || stop) {
+    st.judge(k, nrk, ncc);
+    if ((l < nK && k == K[l]) || st.stop) {
       AIRT_CHECK_CUDA(cudaMemcpyAsync(d_X + l * n, P.x64.p, n * sizeof(double),
                                       cudaMemcpyDeviceToDevice, s));
       ++l;
@@ -374,8 +350,8 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
   cudaEventDestroy(t1);
   if (resn_host) std::copy(resn.begin(), resn.end(), resn_host);
   if (info) {
-    info->stoprule = stoprule;
-    info->finaliter = finaliter;
+    info->stoprule = st.stoprule;
+    info->finaliter = st.finaliter;
     info->relaxpar = lam_last;
     info->nsaved = l;
     info->gpu_ms = ms;

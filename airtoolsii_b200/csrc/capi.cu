@@ -417,6 +417,25 @@ int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const 
   AIRT_API_END
 }
 
+int airt_cart(airt_problem *h, const airt_cart_opts *opts, const double *b, const double *x0,
+              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && opts && b && X, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  cudaStream_t s = P->stream;
+  P->b64.upload(b, P->m, s);
+  if (x0) P->vin.upload(x0, P->n, s);
+  P->Xd.ensure((size_t)P->n * (nK > 0 ? nK : 1));
+  airt_info inf{};
+  run_cart(*P, *opts, P->b64.p, x0 ? P->vin.p : nullptr, K, nK, P->Xd.p, resnorms, &inf);
+  if (inf.nsaved)
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(X, P->Xd.p, (size_t)inf.nsaved * P->n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (info) *info = inf;
+  AIRT_API_END
+}
+
 // ---------------------------------------------------------------- batches
 int airt_batch_parallel(int ninst, const int *N, const int *nA, const int *p, const double *cos_t,
                         const double *sin_t, const double *offsets, airt_batch **out) {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -259,6 +260,46 @@ void generate_matrix(Problem &P);
 void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
 void compute_weights(Problem &P, int method, double *dM, double *dD);
 void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const double *d_x0,
+              const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
+// Stopping-rule state of the sweep loops of ART and CART (DP, NCP and NONE
+// branches of check_stoprules.m:54-151): judge(k, ||r_k||, ncc_k) once per
+// sweep, with the NCP history dk of check_inputs.m:209 (+inf initially).
+struct SweepStop {
+  int rule;
+  double taudelta;
+  int64_t kmax;
+  std::vector<double> dk;
+  bool stop = false;
+  int stoprule = 0;
+  int64_t finaliter = 0;
+  SweepStop(int rule_, double taudelta_, int64_t kmax_, int ncp_smooth)
+      : rule(rule_), taudelta(taudelta_), kmax(kmax_),
+        dk(rule_ == AIRT_STOP_NCP ? ncp_smooth : 0, INFINITY) {}
+  void judge(int64_t k, double nrk, double ncc) {
+    if (rule == AIRT_STOP_DP) {
+      if (nrk <= taudelta || k >= kmax) {
+        stop = true;
+        stoprule = (k != kmax) ? 2 : 0;
+      }
+    } else if (rule == AIRT_STOP_NCP) {  // check_stoprules.m:124-149
+      double mx = -INFINITY, mxn = ncc;
+      for (double v : dk) mx = std::fmax(mx, v);
+      for (size_t i = 1; i < dk.size(); ++i) mxn = std::fmax(mxn, dk[i]);
+      if (mx < mxn || k >= kmax) {
+        stop = true;
+        stoprule = (k != kmax) ? 1 : 0;
+      } else {
+        dk.erase(dk.begin());
+        dk.push_back(ncc);
+      }
+    } else if (k >= kmax) {
+      stop = true;
+    }
+    if (stop) finaliter = k;
+  }
+};
+
+void run_cart(Problem &P, const airt_cart_opts &o, const double *d_b, const double *d_x0,
               const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
 void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double *d_x0,
              const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);

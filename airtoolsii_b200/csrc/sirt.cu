@@ -742,53 +742,114 @@ __global__ void k_dot2(int64_t n, const double *__restrict__ u, const double *__
     atomicAdd(out + 1, b);
   }
 }
-__global__ void k_scale(int64_t n, const double *__restrict__ w, const double *__restrict__ nrm2,
-                        double *__restrict__ u) {
-  const double s = 1.0 / sqrt(nrm2[1]);
+// w -= a * x
+__global__ void k_axmy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ w) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    u[i] = w[i] * s;
+    w[i] -= a * x[i];
+}
+__global__ void k_scale_by(int64_t n, double c, const double *__restrict__ w,
+                           double *__restrict__ u) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    u[i] = w[i] * c;
+}
+
+// Largest eigenvalue of the symmetric tridiagonal matrix with diagonal
+// alpha[0..k) and off-diagonal beta[1..k): bisection on the Sturm count
+// (the number of eigenvalues below x is the number of negative pivots of
+// T - x*I) inside the Gershgorin interval.
+double tridiag_max_eig(const std::vector<double> &alpha, const std::vector<double> &beta) {
+  const size_t k = alpha.size();
+  double lo = INFINITY, hi = -INFINITY;
+  for (size_t i = 0; i < k; ++i) {
+    const double r = (i > 0 ? std::fabs(beta[i]) : 0.0) + (i + 1 < k ? std::fabs(beta[i + 1]) : 0.0);
+    lo = std::fmin(lo, alpha[i] - r);
+    hi = std::fmax(hi, alpha[i] + r);
+  }
+  auto below = [&](double x) {
+    size_t cnt = 0;
+    double d = 1.0;
+    for (size_t i = 0; i < k; ++i) {
+      d = alpha[i] - x - (i > 0 ? beta[i] * beta[i] / d : 0.0);
+      if (d == 0.0) d = -1e-300;
+      if (d < 0) ++cnt;
+    }
+    return cnt;
+  };
+  for (int it = 0; it < 200 && hi - lo > 1e-15 * std::fmax(std::fabs(hi), std::fabs(lo)); ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (below(mid) >= k) hi = mid;  // every eigenvalue lies below mid
+    else lo = mid;
+  }
+  return hi;
 }
 
 }  // namespace
 
-// Largest eigenvalue of D*A'*M*A by power iteration on the similar symmetric
-// operator D^(1/2)*A'*M*A*D^(1/2) (valid for nonnegative M, D), Rayleigh
-// quotient estimate; replaces eigs(...,'lm',tol=1e-4) of calc_relaxpar.m:91-103.
+// Largest eigenvalue of D*A'*M*A, through the similar symmetric operator
+// S = D^(1/2)*A'*M*A*D^(1/2) (M, D nonnegative), by the Lanczos iteration
+// from the normalised ones vector: the largest Ritz value of the
+// tridiagonal matrix, stopped once it changes by at most tol (relative)
+// after at least five steps, or on an invariant subspace.  Replaces
+// eigs(...,'lm',tol=1e-4) of calc_relaxpar.m:91-103; unlike a power
+// iteration it does not stall below rho when the top eigenvalues cluster.
 double estimate_rho(Problem &P, const double *dM, const double *dD, double tol, int maxit) {
   cudaStream_t s = P.stream;
   const int64_t m = P.m, n = P.n;
-  DevBuf<double> sd, u, t, y, w, red;
+  if (n == 0) return 0.0;
+  DevBuf<double> sd, v, vprev, t, y, w, red;
   sd.ensure(n);
-  u.ensure(n);
+  v.ensure(n);
+  vprev.ensure(n);
   t.ensure(n);
-  y.ensure(m);
+  y.ensure(std::max<int64_t>(m, 1));
   w.ensure(n);
   red.ensure(2);
-  const unsigned gn = grid_for(n, kThreads), gm = grid_for(m, kThreads);
+  const unsigned gn = grid_for(n, kThreads), gm = grid_for(std::max<int64_t>(m, 1), kThreads);
   k_sqrt_vec<<<gn, kThreads, 0, s>>>(n, dD, sd.p);
-  std::vector<double> h(n, 1.0 / std::sqrt((double)(n ? n : 1)));
-  u.upload(h.data(), n, s);
-  double lam = 0, prev = 0;
-  for (int it = 0; it < maxit; ++it) {
-    k_mul<<<gn, kThreads, 0, s>>>(n, sd.p, u.p, t.p);
-    apply_operator(P, t.p, y.p, 0);
-    k_mul<<<gm, kThreads, 0, s>>>(m, dM, y.p, y.p);
-    apply_operator(P, y.p, t.p, 1);
-    k_mul<<<gn, kThreads, 0, s>>>(n, sd.p, t.p, w.p);
+  std::vector<double> h(n, 1.0 / std::sqrt((double)n));
+  v.upload(h.data(), n, s);
+  std::vector<double> alpha, beta{0.0};
+  double theta = 0.0, prev = 0.0;
+  auto dot = [&](const double *a, const double *b) {  // a.b
     AIRT_CHECK_CUDA(cudaMemsetAsync(red.p, 0, 2 * sizeof(double), s));
-    k_dot2<<<gn, kThreads, 0, s>>>(n, u.p, w.p, red.p);
-    k_scale<<<gn, kThreads, 0, s>>>(n, w.p, red.p, u.p);
+    k_dot2<<<gn, kThreads, 0, s>>>(n, a, b, red.p);
     AIRT_LAUNCH_CHECK();
     double hr[2];
     AIRT_CHECK_CUDA(cudaMemcpyAsync(hr, red.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-    lam = hr[0];
-    if (!(hr[1] > 0)) break;
-    if (it > 0 && std::fabs(lam - prev) <= tol * std::fabs(lam)) break;
-    prev = lam;
+    return hr[0];
+  };
+  for (int it = 0; it < std::max(maxit, 1); ++it) {
+    // w = S v - beta_j v_(j-1)
+    k_mul<<<gn, kThreads, 0, s>>>(n, sd.p, v.p, t.p);
+    if (m) {
+      apply_operator(P, t.p, y.p, 0);
+      k_mul<<<gm, kThreads, 0, s>>>(m, dM, y.p, y.p);
+      apply_operator(P, y.p, t.p, 1);
+    } else {
+      AIRT_CHECK_CUDA(cudaMemsetAsync(t.p, 0, n * sizeof(double), s));
+    }
+    k_mul<<<gn, kThreads, 0, s>>>(n, sd.p, t.p, w.p);
+    if (it > 0) k_axmy<<<gn, kThreads, 0, s>>>(n, beta.back(), vprev.p, w.p);
+    AIRT_LAUNCH_CHECK();
+    const double a = dot(v.p, w.p);
+    alpha.push_back(a);
+    k_axmy<<<gn, kThreads, 0, s>>>(n, a, v.p, w.p);
+    AIRT_LAUNCH_CHECK();
+    const double b = std::sqrt(std::fmax(dot(w.p, w.p), 0.0));
+    theta = tridiag_max_eig(alpha, beta);
+    if (!(b > 1e-14 * std::fmax(std::fabs(theta), 1e-300))) break;  // invariant subspace
+    if (it >= 4 && std::fabs(theta - prev) <= tol * std::fabs(theta)) break;
+    prev = theta;
+    beta.push_back(b);
+    std::swap(vprev.p, v.p);
+    std::swap(vprev.n, v.n);
+    k_scale_by<<<gn, kThreads, 0, s>>>(n, 1.0 / b, w.p, v.p);
+    AIRT_LAUNCH_CHECK();
   }
-  return lam;
+  return theta;
 }
 
 }  // namespace airt

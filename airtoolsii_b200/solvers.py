@@ -20,7 +20,7 @@ import numpy as np
 import scipy.sparse as sp
 
 from . import _lib
-from ._lib import ArtOpts, Info, SirtOpts, check, dptr, i64ptr, lib
+from ._lib import ArtOpts, CartOpts, Info, SirtOpts, check, dptr, i64ptr, lib
 from .afun import AirtOperator, as_operator
 
 
@@ -423,6 +423,84 @@ def art(art_method, A, b, K, x0=None, options=None):
         _print_verbose(c["verbose"], kmax, resn, np.full(kmax, lam), res_info["timetaken"],
                        int(info.finaliter))
     return SolverResult(X, res_info)
+
+
+def cart(cart_method, A, b, K, x0=None, options=None):
+    """[X,info] = cart(cart_method,A,b,K,x0,options)  (cart/cart.m:1).
+
+    cart_method: 'columnaction' (None means the same) or a 0-based column
+    order.  options as for art plus THR (default 1e-4), Kbegin (10) and
+    Nunflag (round(kmax/4)); relaxpar is a scalar, default 0.25.  The
+    unflagging draws randi(Nunflag) come from a counter-based generator
+    seeded with options['seed'] (default 0), keyed by sweep and column.
+    """
+    t_total = time.perf_counter()
+    if cart_method is None:
+        cart_method = "columnaction"
+    c = _parse(A, b, K, x0, options, "cart")
+    op: AirtOperator = c["op"]
+    n, K, kmax = c["n"], c["K"], c["kmax"]
+    opts = c["options"]
+    relin = opts.get("relaxpar")
+    if relin is None:
+        lam = 0.25
+    elif (np.isscalar(relin) or np.size(relin) == 1) and not callable(relin):
+        lam = float(np.asarray(relin).item())
+        if lam <= 0 or lam >= 2:
+            warnings.warn("The relaxpar value is outside the interval (0,2)")
+    else:
+        raise ValueError("For CART methods the relaxpar must be a scalar.")
+    o = CartOpts()
+    cols = None
+    if isinstance(cart_method, str):
+        if cart_method.lower() != "columnaction":
+            raise ValueError("Unknown CART method specified")
+        o.order_kind = 0
+    else:
+        o.order_kind = 2
+        cols = np.ascontiguousarray(np.asarray(cart_method, dtype=np.int64).ravel())
+        o.cols = i64ptr(cols)
+        o.ncols = cols.size
+    o.relaxpar = lam
+    o.damp = c["damp"]
+    o.stoprule = _lib.STOP[c["stype"]]
+    o.taudelta = c["taudelta"]
+    if c["ncp"] is not None:
+        o.ncp_rows, o.ncp_cols, o.ncp_smooth = c["ncp"]
+    _bound_fields(o, c["bounds"])
+    o.kmax = kmax
+    o.thr = float(opts.get("THR", 1e-4))
+    o.kbegin = int(opts.get("Kbegin", 10))
+    o.nunflag = int(opts["Nunflag"]) if "Nunflag" in opts else int(_mround(kmax / 4.0))
+    o.seed = int(opts.get("seed", 0)) & 0xFFFFFFFFFFFFFFFF
+    X = np.zeros((n, K.size), dtype=np.float64, order="F")
+    resn = np.zeros(kmax + 1)
+    info = Info()
+    check(lib().airt_cart(op.handle, C.byref(o), dptr(c["b"]), dptr(c["x0"]), i64ptr(K), K.size,
+                          X.ctypes.data_as(_lib._dp), dptr(resn), C.byref(info)))
+    fin = int(info.finaliter)
+    X = X[:, :int(info.nsaved)]
+    res_info = {
+        "stoprule": int(info.stoprule),
+        "finaliter": fin,
+        "relaxpar": lam,
+        "itersaved": np.concatenate([K[K < fin], [fin]]),
+        "timetaken": time.perf_counter() - t_total,
+        "gpu_ms": float(info.gpu_ms),
+        "resnorms": resn[:fin + 1],
+    }
+    if c["verbose"]:
+        _print_verbose(c["verbose"], kmax, resn, np.full(kmax, lam), res_info["timetaken"], fin)
+    return SolverResult(X, res_info)
+
+
+def columnaction(A, b, K, x0=None, options=None):
+    """cart/columnaction.m: cart('columnaction', ...)."""
+    return cart("columnaction", A, b, K, x0, options)
+
+
+def _mround(x: float) -> float:
+    return math.copysign(math.floor(abs(x) + 0.5), x)
 
 
 def _randk_stream(normAi, damp, kmax, seed):

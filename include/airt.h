@@ -21,6 +21,7 @@
  *   airt_weights           -> auxil/get_mfun_dfun.m:43-250
  *   airt_rho               -> auxil/calc_relaxpar.m:91-103 (eigs of D*A'*M*A)
  *   airt_sirt              -> sirt/sirt.m:147-261 with auxil/check_stoprules.m:54-94,153-161
+ *   airt_cart              -> cart/cart.m:139-320 (cart/columnaction.m)
  *   airt_art               -> art/art.m:138-309
  */
 #ifndef AIRT_H
@@ -107,6 +108,26 @@ typedef struct {
 } airt_art_opts;
 
 typedef struct {
+    int order_kind;           /* 0 columnaction (every nonzero column, in order),
+                                 2 caller column list                          */
+    const int64_t *cols;      /* order_kind 2: 0-based columns, ncols of them  */
+    int64_t ncols;
+    double relaxpar;          /* scalar relaxpar (default 0.25, calc_relaxpar.m) */
+    double damp;              /* cart.m: normAj + damp*max(normAj)             */
+    int stoprule;             /* AIRT_STOP_NONE, AIRT_STOP_DP or AIRT_STOP_NCP  */
+    double taudelta;
+    int lb_kind, ub_kind;
+    double lb, ub;
+    const double *lbv, *ubv;
+    int64_t kmax;
+    int ncp_rows, ncp_cols, ncp_smooth;
+    double thr;               /* flagging threshold THR (check_inputs.m, 1e-4)  */
+    int64_t kbegin;           /* first sweep that may flag (Kbegin, 10)          */
+    int64_t nunflag;          /* unflagging parameter (Nunflag, round(kmax/4))   */
+    uint64_t seed;            /* seed of the unflagging draws                    */
+} airt_cart_opts;
+
+typedef struct {
     int stoprule;       /* 0 max iterations, 1 NCP, 2 DP, 3 ME (check_stoprules.m:27-31) */
     int64_t finaliter;  /* iterations performed                                 */
     double relaxpar;    /* relaxpar of the final iteration                      */
@@ -174,8 +195,10 @@ int airt_apply_device(airt_problem *h, const double *d_in, double *d_out, int tr
 /* Diagonals of M (m) and D (n) of a built-in method (get_mfun_dfun.m). */
 int airt_weights(airt_problem *h, int method, double *M, double *D);
 
-/* rho = largest eigenvalue of D*A'*M*A (power iteration in FP64 to the given
- * relative tolerance; maxit bounds the operator applications). */
+/* rho = largest eigenvalue of D*A'*M*A (FP64 Lanczos iteration on
+ * D^(1/2)*A'*M*A*D^(1/2) from the ones vector, stopped when the largest Ritz
+ * value changes by at most the given relative tolerance; maxit bounds the
+ * operator applications). */
 int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *Dcustom,
              double tol, int maxit, double *rho);
 
@@ -193,6 +216,14 @@ int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *
 /* ART (Kaczmarz) sweeps, art.m:138-309.  Same K / X / info conventions. */
 int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const double *x0,
              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
+
+/* CART column-action sweeps, cart/cart.m:139-320 (cart/columnaction.m).  Same K /
+ * X / info conventions as airt_art.  The residual is updated column by column
+ * as in the reference.  Each unflagging decision draws randi(nunflag) from a
+ * counter-based generator keyed by (seed, sweep, column), because MATLAB's
+ * randi stream cannot be reproduced. */
+int airt_cart(airt_problem *h, const airt_cart_opts *opts, const double *b, const double *x0,
+              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
 
 /* ---- batches of independent problems --------------------------------------- */
 /* No counterpart in the reference (one problem per sirt/art call, sirt/sirt.m:1).

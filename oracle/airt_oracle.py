@@ -926,6 +926,110 @@ def art(method, A, b, K, x0=None, options=None, stream=None):
     return X, info
 
 
+_M64 = (1 << 64) - 1
+
+
+def _splitmix64(z: int) -> int:
+    z = (z + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def cart_randi(seed: int, k: int, j: int, N: int) -> int:
+    """The unflagging draw randi(N) of sweep k at 0-based column j: MATLAB's
+    randi stream cannot be reproduced, so every draw is a counter-based
+    splitmix64 hash of (seed, k, j) mapped to 1 + floor(u*N)."""
+    key = ((k << 32) | (j & 0xFFFFFFFF)) & _M64
+    z = _splitmix64((seed & _M64) ^ _splitmix64(key))
+    u = float(z >> 11) * 2.0 ** -53
+    return 1 + min(int(math.floor(u * N)), N - 1)
+
+
+def cart(method, A, b, K, x0=None, options=None):
+    """cart/cart.m:109-320 (columnaction) in FP64, column by column, with
+    mm = max(abs(xk)) scanned in full before every column as in the
+    reference.  Returns (X, info)."""
+    t0 = time.perf_counter()
+    options = dict(options or {})
+    if method is None:
+        method = "columnaction"
+    c = _parse_common(A, b, K, x0, options, "cart")
+    A, m, n, b, K, kmax = c["A"], c["m"], c["n"], c["b"], c["K"], c["kmax"]
+    THR = float(options.get("THR", 1e-4))
+    Kbegin = int(options.get("Kbegin", 10))
+    Nunflag = int(options["Nunflag"]) if "Nunflag" in options else int(mround(kmax / 4))
+    seed = int(options.get("seed", 0))
+    X = np.zeros((n, K.size))
+    rk = b - A @ c["x0"]
+    k = 0
+    xk = c["x0"].copy()
+    l = 0
+    rkm1, dk = c["rkm1"], c["dk"]
+    relin = c["relaxpar"]
+    stop, info, rkm1, dk = check_stoprules(c["stype"], rk, relin, c["taudelta"], k, kmax,
+                                           rkm1, dk, c["res_dims"])
+    if relin is not None and (callable(relin) or np.size(relin) != 1):
+        raise ValueError("For CART methods the relaxpar must be a scalar.")
+    relaxpar = 0.25 if relin is None else float(relin)
+    Acsc = sp.csc_matrix(A)
+    normAj = np.asarray(Acsc.multiply(Acsc).sum(axis=0)).ravel()
+    if isinstance(method, str):
+        if method.lower() != "columnaction":
+            raise ValueError("Unknown CART method specified")
+        J = np.flatnonzero(normAj > 0)
+    else:
+        J = np.asarray(method, dtype=np.int64).ravel()
+        J = J[normAj[J] > 0]
+    normAj = normAj + c["damp"] * np.max(normAj)
+    F = np.ones(n, dtype=bool)
+    Nflag = np.zeros(n, dtype=np.int64)
+    lb, ub = c["lb"], c["ub"]
+    indptr, indices, data = Acsc.indptr, Acsc.indices, Acsc.data
+    while not stop:
+        k += 1
+        for j in J:
+            mm = np.max(np.abs(xk)) if n else 0.0
+            if F[j]:
+                s_, e_ = indptr[j], indptr[j + 1]
+                rows = indices[s_:e_]
+                aj = data[s_:e_]
+                delta = float(aj @ rk[rows]) / normAj[j]
+                od = relaxpar * delta
+                xkj = xk[j]
+                if lb is not None:
+                    lbj = lb[0] if lb.size == 1 else lb[j]
+                    if od < lbj - xkj:
+                        od = lbj - xkj
+                if ub is not None:
+                    ubj = ub[0] if ub.size == 1 else ub[j]
+                    if od > ubj - xkj:
+                        od = ubj - xkj
+                xk[j] = xkj + od
+                if k >= Kbegin and abs(od) < THR * mm:
+                    F[j] = False
+                    Nflag[j] = 1
+                rk[rows] = rk[rows] - od * aj
+            else:
+                if Nunflag < 1:
+                    raise ValueError("randi: Nunflag must be a positive integer")
+                if Nflag[j] < cart_randi(seed, k, int(j), Nunflag):
+                    Nflag[j] += 1
+                else:
+                    F[j] = True
+        stop, info, rkm1, dk = check_stoprules(c["stype"], rk, relaxpar, c["taudelta"], k, kmax,
+                                               rkm1, dk, c["res_dims"])
+        if (l < K.size and k == K[l]) or stop:
+            X[:, l] = xk
+            l += 1
+    X = X[:, :l]
+    if not info:
+        info = {"stoprule": 0, "finaliter": 0, "relaxpar": relaxpar}
+    info["itersaved"] = np.concatenate([K[K < info["finaliter"]], [info["finaliter"]]])
+    info["timetaken"] = time.perf_counter() - t0
+    return X, info
+
+
 # ---------------------------------------------------------------- training
 def _run(method, A, b, K, x0, options):
     if method in ("landweber", "cimmino", "cav", "drop", "sart"):

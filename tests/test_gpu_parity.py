@@ -497,3 +497,86 @@ def test_art_c3_sized_iterate_by_iterate(c3art, method):
     for j in range(len(K)):
         x = cbind.kaczmarz(Rm, b, nrm, order, 1.0, 0.0, None, 1, x0=x)
         assert relerr(X[:, j], x) <= RTOL, (method, K[j], relerr(X[:, j], x))
+
+
+# ------------------------------------------------------------ CART
+def _f32(A):
+    """A with its values rounded to FP32, as the GPU stores them: the CART
+    oracle runs on it so that both sides take the same flagging decisions."""
+    R = sp.csc_matrix(A, copy=True)
+    R.data = R.data.astype(np.float32).astype(np.float64)
+    return R
+
+
+CART_TOL = 1e-9
+
+
+@pytest.mark.parametrize("opts", [
+    {},
+    {"lbound": 0.0, "ubound": 1.0, "relaxpar": 0.5, "Kbegin": 2, "Nunflag": 2, "THR": 5e-3},
+    {"damp": 0.1, "relaxpar": 1.2, "Kbegin": 1, "Nunflag": 3, "THR": 2e-2, "seed": 7},
+])
+def test_cart_vs_oracle(small, opts):
+    """cart.m columnaction: saved iterates, finaliter and itersaved against
+    the oracle, with flagging and unflagging active in the last two cases."""
+    A, A_ref, b = small
+    K = [1, 3, 8, 15]
+    Xo, io = O.cart("columnaction", _f32(A_ref), b, K, None, opts)
+    X, info = airt.columnaction(A, b, K, None, opts)
+    assert X.shape == Xo.shape
+    assert relerr(X, Xo) <= CART_TOL
+    assert info["finaliter"] == io["finaliter"] == 15
+    assert list(info["itersaved"]) == list(io["itersaved"])
+    assert info["relaxpar"] == opts.get("relaxpar", 0.25)
+
+
+def test_cart_running_max_rescans(small):
+    """x0 above the upper bound: the clipped steps keep lowering the entry
+    that holds max(abs(x)), and with THR = 0.05 from the first sweep on the
+    flag of every column depends on that maximum before its step."""
+    A, A_ref, b = small
+    x0 = np.random.default_rng(5).uniform(0.0, 3.0, A.n)
+    opts = {"lbound": 0.0, "ubound": 1.0, "Kbegin": 1, "THR": 0.05, "Nunflag": 2, "seed": 3}
+    K = list(range(1, 7))
+    Xo, _ = O.cart("columnaction", _f32(A_ref), b, K, x0, opts)
+    X, _ = airt.columnaction(A, b, K, x0, opts)
+    for j in range(len(K)):
+        assert relerr(X[:, j], Xo[:, j]) <= CART_TOL, (K[j], relerr(X[:, j], Xo[:, j]))
+
+
+def test_cart_custom_order_and_stop_rules(small, c1):
+    A, A_ref, b = small
+    n = A.n
+    order = np.concatenate([np.arange(n)[::-1], np.arange(12), [5, 5, 7]])
+    opts = {"Kbegin": 2, "Nunflag": 2, "THR": 1e-2}
+    Xo, io = O.cart(order, _f32(A_ref), b, [2, 6], None, opts)
+    X, info = airt.cart(order, A, b, [2, 6], None, opts)
+    assert relerr(X, Xo) <= CART_TOL
+    # DP: stop at the sweep whose residual first falls below taudelta
+    Ac, Ac_ref, bc, enorm, _ = c1
+    tau = 1.02 * enorm
+    dp = {"stoprule": {"type": "DP", "taudelta": tau}}
+    Xo, io = O.cart(None, _f32(Ac_ref), bc, 60, None, dp)
+    X, info = airt.cart(None, Ac, bc, 60, None, dp)
+    assert info["finaliter"] == io["finaliter"] and info["stoprule"] == io["stoprule"]
+    assert relerr(X, Xo) <= CART_TOL
+    assert info["resnorms"][-1] <= tau < info["resnorms"][-2] or info["finaliter"] == 60
+    # NCP on the projections (res_dims = [rays, angles])
+    ncp = {"stoprule": {"type": "NCP", "res_dims": [91, 180]}}
+    Xo, io = O.cart("columnaction", _f32(Ac_ref), bc, 40, None, ncp)
+    X, info = airt.columnaction(Ac, bc, 40, None, ncp)
+    assert info["finaliter"] == io["finaliter"] and info["stoprule"] == io["stoprule"]
+    assert relerr(X, Xo) <= CART_TOL
+
+
+def test_cart_input_errors(small):
+    A, A_ref, b = small
+    with pytest.raises(ValueError):
+        airt.cart("rowaction", A, b, 2)
+    with pytest.raises(ValueError):
+        airt.columnaction(A, b, 2, None, {"relaxpar": lambda k: 0.5})
+    with pytest.raises(ValueError):
+        airt.columnaction(A, b, 2, None, {"stoprule": {"type": "ME", "taudelta": 1.0}})
+    Amf, *_ = airt.paralleltomo(16, np.arange(0.0, 180.0, 6.0), None, None, 0, 0)
+    with pytest.raises(airt.AirtError):
+        airt.columnaction(Amf, Amf(np.ones(256), "notransp"), 2)

@@ -218,6 +218,29 @@ def test_sphere_rows_count_in_image_samples():
     assert A.nnz > 0 and np.all(A.data > 0)
 
 
+def test_cart_diagonal_known_answer():
+    """For a diagonal A, one columnaction sweep with relaxpar 1 solves A x = b
+    exactly (each column's step is b_j/a_jj), and the box clips it."""
+    d = np.array([2.0, 0.5, 4.0, 1.0, 8.0])
+    b = np.array([1.0, -3.0, 2.0, 5.0, 0.25])
+    A = sp.diags(d).tocsc()
+    X, info = O.cart("columnaction", A, b, [1, 2], None, {"relaxpar": 1.0})
+    np.testing.assert_array_equal(X[:, 0], b / d)
+    np.testing.assert_array_equal(X[:, 1], b / d)
+    assert info["finaliter"] == 2
+    X, _ = O.cart("columnaction", A, b, [1], None, {"relaxpar": 1.0, "lbound": 0.0, "ubound": 2.0})
+    np.testing.assert_array_equal(X[:, 0], np.clip(b / d, 0.0, 2.0))
+
+
+def test_cart_randi_draws():
+    draws = [O.cart_randi(11, k, j, 4) for k in range(1, 50) for j in range(40)]
+    assert min(draws) == 1 and max(draws) == 4
+    assert draws == [O.cart_randi(11, k, j, 4) for k in range(1, 50) for j in range(40)]
+    counts = np.bincount(draws)[1:]
+    assert np.all(np.abs(counts / len(draws) - 0.25) < 0.03)
+    assert O.cart_randi(11, 1, 0, 1) == 1
+
+
 # ---------------------------------------------------------------- invariants
 @pytest.fixture(scope="module")
 def small():
