@@ -8,6 +8,7 @@ sm_100a); the package raises on import if the library is missing.
 from ._lib import AirtError, lib as _load_lib
 from .afun import AirtOperator, afun_matrix, as_operator
 from .batch import ParallelBatch
+from .analytic import fbp
 from .unet import UNet
 from .solvers import (art, calczeta, cart, cav, cimmino, columnaction, drop, kaczmarz, landweber,
                       randkaczmarz, sart, sirt, symkaczmarz)
@@ -16,7 +17,7 @@ from .testprobs import (add_noise, cosd, fancurvedtomo, fanlineartomo, parallelt
 
 _load_lib()
 
-__all__ = ["AirtError", "AirtOperator", "ParallelBatch", "UNet", "afun_matrix", "as_operator", "art", "calczeta", "cart", "cav", "columnaction",
+__all__ = ["AirtError", "AirtOperator", "ParallelBatch", "UNet", "afun_matrix", "as_operator", "art", "calczeta", "cart", "cav", "columnaction", "fbp",
            "cimmino", "drop", "kaczmarz", "landweber", "randkaczmarz", "sart", "sirt",
            "symkaczmarz", "add_noise", "cosd", "fancurvedtomo", "fanlineartomo", "paralleltomo", "seismictomo",
            "sphericaltomo",

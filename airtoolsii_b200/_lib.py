@@ -95,6 +95,7 @@ SIGNATURES = {
                            C.POINTER(Info)]),
     "airt_cart": (C.c_int, [C.c_void_p, C.POINTER(CartOpts), _dp, _dp, _i64p, C.c_int64, _dp, _dp,
                             C.POINTER(Info)]),
+    "airt_fbp": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, C.c_int, _dp]),
     "airt_batch_parallel": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), _dp, _dp, _dp, C.POINTER(C.c_void_p)]),
     "airt_batch_layout": (C.c_int, [C.c_void_p, _i64p, _i64p, _i64p]),
@@ -109,6 +110,8 @@ SIGNATURES = {
     "airt_batch_nnz": (C.c_int, [C.c_void_p, _i64p]),
     "airt_batch_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "airt_batch_backproject": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]),
+    "airt_batch_fbp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p,
+                                 _dp]),
     "airt_batch_kaczmarz": (C.c_int, [C.c_void_p, _dp, C.c_int64, C.c_double, C.c_int,
                                       C.c_double, C.c_int, C.c_double, _dp, _dp]),
     "airt_batch_destroy": (C.c_int, [C.c_void_p]),

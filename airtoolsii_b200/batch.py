@@ -10,6 +10,7 @@ principle threshold per instance; every instance stops on its own.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -38,6 +39,8 @@ def _batch_signatures():
         "airt_batch_nnz": (C.c_int, [C.c_void_p, i64p]),
         "airt_batch_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
         "airt_batch_backproject": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _lib._dp]),
+        "airt_batch_fbp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, _lib._dp, C.c_int, _lib._dp,
+                                     C.c_void_p, _lib._dp]),
         "airt_batch_kaczmarz": (C.c_int, [C.c_void_p, _lib._dp, C.c_int64, C.c_double, C.c_int,
                                           C.c_double, C.c_int, C.c_double, _lib._dp, _lib._dp]),
         "airt_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -197,6 +200,22 @@ class ParallelBatch:
         ms = C.c_double()
         check(self._L.airt_batch_backproject(self._h, _lib.METHODS[method], C.c_void_p(d_b),
                                              C.c_void_p(d_x), C.byref(ms)))
+        return float(ms.value)
+
+    def fbp_device(self, d_b, d_x, filter="ram-lak") -> float:
+        """Filtered back projection of every instance (auxil/fbp.m:40-79) on
+        device vectors; all instances need the same number of rays.  Returns
+        the device time in ms."""
+        from .analytic import fbp_kernel
+        if len(set(self.ps)) != 1:
+            raise ValueError("batch fbp needs the same number of rays in every instance")
+        nr = self.ps[0]
+        h = fbp_kernel(nr, filter)
+        scale = np.concatenate([np.full(na, math.pi / (2.0 * na)) for na in self.nAs])
+        ms = C.c_double()
+        check(self._L.airt_batch_fbp(self._h, C.c_void_p(d_b), int(nr), dptr(h), int(h.size),
+                                     dptr(np.ascontiguousarray(scale)), C.c_void_p(d_x),
+                                     C.byref(ms)))
         return float(ms.value)
 
     def kaczmarz(self, b, sweeps, relaxpar=1.0, lbound=None, ubound=None):

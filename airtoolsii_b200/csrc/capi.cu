@@ -539,6 +539,62 @@ int airt_batch_backproject(airt_batch *h, int method, const double *d_b, double 
   AIRT_API_END
 }
 
+int airt_fbp(airt_problem *h, const double *b, int na, const double *kernel, int order,
+                        double *x) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && b && kernel && x, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  AIRT_REQUIRE(na >= 1 && P->m % na == 0, "fbp: the number of angles must divide the rows of A");
+  const int64_t nr64 = P->m / na;
+  AIRT_REQUIRE(nr64 >= 1 && nr64 < INT32_MAX, "fbp: projection length out of range");
+  const int nr = (int)nr64;
+  cudaStream_t s = P->stream;
+  DevBuf<double> hk, filt;
+  hk.upload(kernel, order, s);
+  P->b64.upload(b, P->m, s);
+  filt.ensure(P->m);
+  const double scale = 3.141592653589793 / (2.0 * na);  // fbp.m:79
+  fbp_filter(P->b64.p, filt.p, nr, na, hk.p, order, nullptr, scale, s);
+  P->vout.ensure(P->n);
+  apply_operator(*P, filt.p, P->vout.p, 1);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P->vout.p, P->n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  AIRT_API_END
+}
+
+int airt_batch_fbp(airt_batch *h, const double *d_b, int nr, const double *kernel,
+                              int order, const double *col_scale, double *d_x, double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && d_b && kernel && col_scale && d_x, "null pointer argument");
+  Batch &B = *reinterpret_cast<Batch *>(h);
+  Problem &P = batch_problem(B);
+  const int K = batch_ninst(B);
+  const int64_t *roff = batch_row_off(B);
+  for (int k = 0; k < K; ++k)
+    AIRT_REQUIRE(nr >= 1 && (roff[k + 1] - roff[k]) % nr == 0,
+                 "batch fbp: every instance needs projections of nr rays");
+  const int64_t ncols = P.m / nr;
+  cudaStream_t s = P.stream;
+  cudaEvent_t t0, t1;
+  AIRT_CHECK_CUDA(cudaEventCreate(&t0));
+  AIRT_CHECK_CUDA(cudaEventCreate(&t1));
+  DevBuf<double> hk, sc, filt;
+  hk.upload(kernel, order, s);
+  sc.upload(col_scale, ncols, s);
+  filt.ensure(std::max<int64_t>(P.m, 1));
+  AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
+  fbp_filter(d_b, filt.p, nr, ncols, hk.p, order, sc.p, 1.0, s);
+  apply_operator(P, filt.p, d_x, 1);
+  AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (gpu_ms) *gpu_ms = ms;
+  AIRT_API_END
+}
+
 int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double relaxpar,
                         int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms) {
   AIRT_API_BEGIN

@@ -323,6 +323,10 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
 void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int lbk, double lb,
                     int ubk, double ub, double *d_x, double *gpu_ms);
 void batch_backproject(Batch &B, int method, const double *d_b, double *d_x, double *gpu_ms);
+// fbp.cu: out = col_scale (or scale) * the circular convolution of every
+// nr-sample column of in with the order-entry kernel h, cropped to nr
+void fbp_filter(const double *d_in, double *d_out, int nr, int64_t ncols, const double *d_h,
+                int order, const double *d_col_scale, double scale, cudaStream_t s);
 
 // Exclusive scan of counts[0..n) into offs[0..n] (offs[n] = total), device.
 void exclusive_scan_i64(const int64_t *counts, int64_t *offs, int64_t n, cudaStream_t s);

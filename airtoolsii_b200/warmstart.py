@@ -215,11 +215,14 @@ class WarmStart:
                     net_wall_s=t_net, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
                     plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0))
 
-    def time_to_dp(self, data, batch, kmax=2000):
+    def time_to_dp(self, data, batch, kmax=2000, fbp_filter="hamming"):
         """Time to the DP stop for all instances of `data`, `batch` at a time
-        (a multiple of batch instances), plain vs warm start.
+        (a multiple of batch instances): plain, fbp warm start and learned
+        warm start.
 
         plain: batched cimmino from zero, batch after batch.
+        fbp: per batch, the filtered back projection (auxil/fbp.m, filter
+        `fbp_filter`) as x0, then batched cimmino from it.
         warm: per batch, the back-projection u, the network's x0 and batched
         cimmino from x0, in that order on the solver's stream.  (Running the
         next batch's network on its own stream during a solve was measured
@@ -241,6 +244,8 @@ class WarmStart:
         xw = [torch.empty_like(xp[0]) for _ in range(nb)]
         u = [torch.empty_like(xp[0]) for _ in range(nb)]
         x0 = [torch.empty_like(xp[0]) for _ in range(nb)]
+        xf = [torch.empty_like(xp[0]) for _ in range(nb)]
+        xf0 = [torch.empty_like(xp[0]) for _ in range(nb)]
         rho = np.full(batch, self.rho)
         tds = [data["taudelta"][sl] for sl in sels]
         stream = Bt.stream_ptr()
@@ -250,6 +255,14 @@ class WarmStart:
                              rho=rho) for i in range(nb)]
         torch.cuda.synchronize()
         wall_plain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        iF = []
+        for i in range(nb):
+            Bt.fbp_device(d_b[i].data_ptr(), xf0[i].data_ptr(), fbp_filter)
+            iF.append(Bt.sirt_device(self.method, d_b[i].data_ptr(), xf[i].data_ptr(), kmax,
+                                     taudelta=tds[i], rho=rho, d_x0=xf0[i].data_ptr()))
+        torch.cuda.synchronize()
+        wall_fbp = time.perf_counter() - t0
         t0 = time.perf_counter()
         iw = []
         for i in range(nb):
@@ -267,11 +280,15 @@ class WarmStart:
                 out.append((torch.linalg.norm(xs[i] - ref, dim=1) / torch.linalg.norm(ref, dim=1)).cpu().numpy())
             return np.concatenate(out)
         return dict(instances=nb * batch, batch=batch, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
+                    fbp_wall_s=wall_fbp, fbp_filter=fbp_filter,
                     plain_iters=np.concatenate([r["finaliter"] for r in ip]),
                     warm_iters=np.concatenate([r["finaliter"] for r in iw]),
+                    fbp_iters=np.concatenate([r["finaliter"] for r in iF]),
                     plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0),
+                    fbp_relerr=err(xf), fbp_x0_relerr=err(xf0),
                     plain_solver_gpu_ms=sum(r["gpu_ms"] for r in ip),
-                    warm_solver_gpu_ms=sum(r["gpu_ms"] for r in iw))
+                    warm_solver_gpu_ms=sum(r["gpu_ms"] for r in iw),
+                    fbp_solver_gpu_ms=sum(r["gpu_ms"] for r in iF))
 
 
 # ---------------------------------------------------------------- training CLI

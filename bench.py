@@ -261,7 +261,9 @@ def warm_leg(a):
     the solutions resident on the device; times are host wall clocks around
     each synchronised pipeline, after one untimed pass.  The network was
     trained on 20000 other seeds (seeds 1000..20999)
-    by this project's kernels (airtoolsii_b200/warmstart.py, train_c5)."""
+    by this project's kernels (airtoolsii_b200/warmstart.py, train_c5).
+    fbp_baseline: the same solves started from the filtered back projection
+    (auxil/fbp.m, hamming filter) instead of the network's x0."""
     import torch
     from airtoolsii_b200 import warmstart as W
     ws = W.c5_warmstart()
@@ -273,7 +275,8 @@ def warm_leg(a):
     r = ws.time_to_dp(te, a.warm_batch)
     done = r["instances"]
     cat = {k: np.asarray(r[k], dtype=float) for k in
-           ("plain_iters", "warm_iters", "plain_relerr", "warm_relerr", "x0_relerr")}
+           ("plain_iters", "warm_iters", "plain_relerr", "warm_relerr", "x0_relerr",
+            "fbp_iters", "fbp_relerr", "fbp_x0_relerr")}
     tot = {"plain_wall_s": r["plain_wall_s"], "warm_wall_s": r["warm_wall_s"],
            "plain_gpu_ms": r["plain_solver_gpu_ms"], "warm_gpu_ms": r["warm_solver_gpu_ms"]}
     return {
@@ -293,6 +296,12 @@ def warm_leg(a):
         "warm_relerr_mean": round(float(cat["warm_relerr"].mean()), 5),
         "x0_relerr_mean": round(float(cat["x0_relerr"].mean()), 5),
         "warm_not_worse_frac": round(float(np.mean(cat["warm_relerr"] <= cat["plain_relerr"] * 1.0001)), 4),
+        "fbp_baseline": {"filter": r["fbp_filter"], "fbp_s": round(r["fbp_wall_s"], 4),
+                         "speedup": round(tot["plain_wall_s"] / r["fbp_wall_s"], 3),
+                         "solver_gpu_ms": round(r["fbp_solver_gpu_ms"], 2),
+                         "iters_mean": round(float(cat["fbp_iters"].mean()), 3),
+                         "relerr_mean": round(float(cat["fbp_relerr"].mean()), 5),
+                         "x0_relerr_mean": round(float(cat["fbp_x0_relerr"].mean()), 5)},
     }
 
 

@@ -22,6 +22,7 @@
  *   airt_rho               -> auxil/calc_relaxpar.m:91-103 (eigs of D*A'*M*A)
  *   airt_sirt              -> sirt/sirt.m:147-261 with auxil/check_stoprules.m:54-94,153-161
  *   airt_cart              -> cart/cart.m:139-320 (cart/columnaction.m)
+ *   airt_fbp               -> auxil/fbp.m:40-79
  *   airt_art               -> art/art.m:138-309
  */
 #ifndef AIRT_H
@@ -225,6 +226,13 @@ int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const 
 int airt_cart(airt_problem *h, const airt_cart_opts *opts, const double *b, const double *x0,
               const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);
 
+/* Filtered back projection, auxil/fbp.m:40-79: b is the nr x na sinogram
+ * (nr = rows/na); every column is circularly convolved with `kernel`
+ * (order >= 2*nr - 1 entries: real(ifft) of fbp.m's zero-padded filter,
+ * computed by the caller) and cropped to nr samples; x = A'*(that) *
+ * pi/(2*na).  The 'none' filter is airt_apply with transp = 1. */
+int airt_fbp(airt_problem *h, const double *b, int na, const double *kernel, int order, double *x);
+
 /* ---- batches of independent problems --------------------------------------- */
 /* No counterpart in the reference (one problem per sirt/art call, sirt/sirt.m:1).
  * ninst paralleltomo instances (N[k], nA[k] angles, p[k] rays); cos_t/sin_t
@@ -259,6 +267,11 @@ int airt_batch_apply(airt_batch *h, const double *d_in, double *d_out, int trans
  * vectors): the first iterate of sirt (sirt/sirt.m:229) from x0 = 0
  * with relaxpar 1 and no bounds, computed with one transpose pass. */
 int airt_batch_backproject(airt_batch *h, int method, const double *d_b, double *d_x, double *gpu_ms);
+/* fbp of every instance at once (auxil/fbp.m:40-79): all instances have
+ * projections of nr rays; d_b holds rows/nr such columns, col_scale (host,
+ * one entry per column) the pi/(2*na_k) of the column's instance. */
+int airt_batch_fbp(airt_batch *h, const double *d_b, int nr, const double *kernel, int order,
+                   const double *col_scale, double *d_x, double *gpu_ms);
 /* Kaczmarz sweeps in the kaczmarz row order, one CTA per instance, x0 = 0. */
 int airt_batch_kaczmarz(airt_batch *h, const double *b, int64_t sweeps, double relaxpar,
                         int lb_kind, double lb, int ub_kind, double ub, double *x, double *gpu_ms);

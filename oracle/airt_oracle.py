@@ -1030,6 +1030,53 @@ def cart(method, A, b, K, x0=None, options=None):
     return X, info
 
 
+def _nextpow2(x):
+    x = abs(float(x))
+    if x == 0:
+        return 0
+    return int(math.ceil(math.log2(x)))
+
+
+def fbp(A, b, theta, filter="ram-lak"):
+    """auxil/fbp.m:40-79 in FP64: the sinogram reshaped to nr x na, each
+    column zero-padded to order = max(64, 2^nextpow2(2*nr)) samples,
+    FFT, times the filter, inverse FFT, real part, cropped to nr rows, then
+    x = A'*b(:)*pi/(2*na)."""
+    filter = filter.lower()
+    A = sp.csr_matrix(A)
+    if filter == "none":
+        return A.T @ np.asarray(b, float)
+    m = A.shape[0]
+    na = len(np.atleast_1d(theta))
+    nr = m // na
+    B = np.asarray(b, float).reshape(nr, na, order="F")
+    order = max(64, 2 ** _nextpow2(2 * nr))
+    n = np.arange(order / 2 + 1)
+    f = n / np.max(n)
+    f[0] = 0.4 / order
+    f[-1] = 1 - f[0]
+    w = 2 * math.pi * n / order
+    if filter == "ram-lak":
+        pass
+    elif filter == "shepp-logan":
+        f[1:] = f[1:] * (np.sin(w[1:] / 2) / (w[1:] / 2))
+    elif filter == "cosine":
+        f[1:] = f[1:] * np.cos(w[1:] / 2)
+    elif filter == "hamming":
+        f[1:] = f[1:] * (0.54 + 0.46 * np.cos(w[1:]))
+    elif filter == "hann":
+        f[1:] = f[1:] * (1 + np.cos(w[1:])) / 2
+    else:
+        raise ValueError("Iinvalid filter")
+    f = np.concatenate([f, f[-2:0:-1]])
+    Bp = np.zeros((order, na))
+    Bp[:nr] = B
+    Bf = np.fft.fft(Bp, axis=0)
+    Bf = Bf * f[:, None]
+    Bf = np.real(np.fft.ifft(Bf, axis=0))[:nr]
+    return (A.T @ Bf.ravel(order="F")) * math.pi / (2 * na)
+
+
 # ---------------------------------------------------------------- training
 def _run(method, A, b, K, x0, options):
     if method in ("landweber", "cimmino", "cav", "drop", "sart"):

@@ -105,6 +105,26 @@ def test_sphere_tables_match_oracle():
     np.testing.assert_array_equal(O.mround_array(x), [-3, -2, -1, 1, 2, 2, 0, 3])
 
 
+def test_fbp_kernel_is_the_filtered_impulse_response():
+    """Circular convolution with fbp_kernel equals fbp.m's zero-pad / fft /
+    filter / ifft / crop of one projection, for every filter."""
+    from airtoolsii_b200 import analytic as F
+    rng = np.random.default_rng(4)
+    for nr in (17, 91, 130):
+        col = rng.standard_normal(nr)
+        for name in ("ram-lak", "shepp-logan", "cosine", "hamming", "hann"):
+            h = F.fbp_kernel(nr, name)
+            order = h.size
+            assert order == max(64, 2 ** int(np.ceil(np.log2(2 * nr))))
+            direct = np.array([sum(h[(i - j) % order] * col[j] for j in range(nr)) for i in range(nr)])
+            pad = np.zeros(order)
+            pad[:nr] = col
+            ref = np.real(np.fft.ifft(np.fft.fft(pad) * F.fbp_filter(nr, name)))[:nr]
+            np.testing.assert_allclose(direct, ref, rtol=1e-12, atol=1e-12)
+    with pytest.raises(ValueError):
+        F.fbp_filter(10, "bogus")
+
+
 def test_random_ellipses_range_and_determinism():
     x1 = testprobs.random_ellipses(48, 10, seed=5)
     x2 = testprobs.random_ellipses(48, 10, seed=5)
