@@ -549,14 +549,13 @@ int airt_fbp(airt_problem *h, const double *b, int na, const double *kernel, int
   AIRT_REQUIRE(nr64 >= 1 && nr64 < INT32_MAX, "fbp: projection length out of range");
   const int nr = (int)nr64;
   cudaStream_t s = P->stream;
-  DevBuf<double> hk, filt;
-  hk.upload(kernel, order, s);
+  P->fbp_h.upload(kernel, order, s);
   P->b64.upload(b, P->m, s);
-  filt.ensure(P->m);
+  P->fbp_tmp.ensure(P->m);
   const double scale = 3.141592653589793 / (2.0 * na);  // fbp.m:79
-  fbp_filter(P->b64.p, filt.p, nr, na, hk.p, order, nullptr, scale, s);
+  fbp_filter(P->b64.p, P->fbp_tmp.p, nr, na, P->fbp_h.p, order, nullptr, scale, s);
   P->vout.ensure(P->n);
-  apply_operator(*P, filt.p, P->vout.p, 1);
+  apply_operator(*P, P->fbp_tmp.p, P->vout.p, 1);
   AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P->vout.p, P->n * sizeof(double), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   AIRT_API_END
@@ -578,13 +577,12 @@ int airt_batch_fbp(airt_batch *h, const double *d_b, int nr, const double *kerne
   cudaEvent_t t0, t1;
   AIRT_CHECK_CUDA(cudaEventCreate(&t0));
   AIRT_CHECK_CUDA(cudaEventCreate(&t1));
-  DevBuf<double> hk, sc, filt;
-  hk.upload(kernel, order, s);
-  sc.upload(col_scale, ncols, s);
-  filt.ensure(std::max<int64_t>(P.m, 1));
+  P.fbp_h.upload(kernel, order, s);
+  P.fbp_scale.upload(col_scale, ncols, s);
+  P.fbp_tmp.ensure(std::max<int64_t>(P.m, 1));
   AIRT_CHECK_CUDA(cudaEventRecord(t0, s));
-  fbp_filter(d_b, filt.p, nr, ncols, hk.p, order, sc.p, 1.0, s);
-  apply_operator(P, filt.p, d_x, 1);
+  fbp_filter(d_b, P.fbp_tmp.p, nr, ncols, P.fbp_h.p, order, P.fbp_scale.p, 1.0, s);
+  apply_operator(P, P.fbp_tmp.p, d_x, 1);
   AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   float ms = 0;

@@ -182,6 +182,8 @@ struct Problem {
   DevBuf<double> x64, r64, rprev, g64, b64, M, D, lbv, ubv, vin, vout, table, resn, lamh, Xd;
   // NCP stopping rule: DFT twiddles (cos, sin pairs), power spectra, column distances, history
   DevBuf<double> ncp_tw, ncp_pk, ncp_col, ncp_dk;
+  // fbp: filter kernel, per-column scales, filtered sinogram (kept between calls)
+  DevBuf<double> fbp_h, fbp_scale, fbp_tmp;
   int ncp_len = 0;  // column length the twiddles were made for
   DevBuf<float> x32, mr32;
   DevBuf<SirtState> state;

@@ -257,8 +257,11 @@ class WarmStart:
         wall_plain = time.perf_counter() - t0
         t0 = time.perf_counter()
         iF = []
+        wall_filter = 0.0
         for i in range(nb):
-            Bt.fbp_device(d_b[i].data_ptr(), xf0[i].data_ptr(), fbp_filter)
+            t1 = time.perf_counter()
+            Bt.fbp_device(d_b[i].data_ptr(), xf0[i].data_ptr(), fbp_filter)  # returns synchronised
+            wall_filter += time.perf_counter() - t1
             iF.append(Bt.sirt_device(self.method, d_b[i].data_ptr(), xf[i].data_ptr(), kmax,
                                      taudelta=tds[i], rho=rho, d_x0=xf0[i].data_ptr()))
         torch.cuda.synchronize()
@@ -280,7 +283,7 @@ class WarmStart:
                 out.append((torch.linalg.norm(xs[i] - ref, dim=1) / torch.linalg.norm(ref, dim=1)).cpu().numpy())
             return np.concatenate(out)
         return dict(instances=nb * batch, batch=batch, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
-                    fbp_wall_s=wall_fbp, fbp_filter=fbp_filter,
+                    fbp_wall_s=wall_fbp, fbp_filter_wall_s=wall_filter, fbp_filter=fbp_filter,
                     plain_iters=np.concatenate([r["finaliter"] for r in ip]),
                     warm_iters=np.concatenate([r["finaliter"] for r in iw]),
                     fbp_iters=np.concatenate([r["finaliter"] for r in iF]),
