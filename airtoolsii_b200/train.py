@@ -1,8 +1,8 @@
 """Training of the relaxation parameter and of the DP/ME factor tau
 (train/train_relaxpar.m, train/train_dpme.m) on the GPU solvers.
 
-Both are host loops of solves; every solve runs through libairt (sirt / art
-of solvers.py).  train_dpme's noise matrix comes from the caller (or a
+Both are host loops of solves; every solve runs through libairt (sirt, art
+and cart/columnaction of solvers.py).  train_dpme's noise matrix comes from the caller (or a
 seeded NumPy generator): MATLAB's randn stream cannot be reproduced.
 """
 from __future__ import annotations
@@ -15,12 +15,13 @@ from . import solvers
 
 SIRT_METHODS = ("landweber", "cimmino", "cav", "drop", "sart")
 ART_METHODS = ("kaczmarz", "symkaczmarz", "randkaczmarz")
+CART_METHODS = ("columnaction",)
 
 
 def _solve(method, A, b, K, x0, options):
     if method in SIRT_METHODS:
         X, info = solvers.sirt(method, A, b, K, x0, options)
-    elif method in ART_METHODS:
+    elif method in ART_METHODS or method in CART_METHODS:
         X, info = getattr(solvers, method)(A, b, K, x0, options)
     else:
         raise ValueError(f"Unknown method {method}")
@@ -63,7 +64,7 @@ def train_relaxpar(A, b, x_ex, method: str, kmax: int, options=None) -> float:
                 Xnew, info = _solve(method, A, b, K, x0, options)
                 options["rho"] = info["rho"]
                 relaxparmax = 2.0 / info["rho"]
-            elif method in ART_METHODS:
+            elif method in ART_METHODS or method in CART_METHODS:  # train_relaxpar.m:90
                 options["relaxpar"] = 0.25
                 Xnew, _ = _solve(method, A, b, K, x0, options)
                 relaxparmax = 2.0

@@ -1081,6 +1081,8 @@ def fbp(A, b, theta, filter="ram-lak"):
 def _run(method, A, b, K, x0, options):
     if method in ("landweber", "cimmino", "cav", "drop", "sart"):
         X, info, _ = sirt(method, A, b, K, x0, options)
+    elif method == "columnaction":
+        X, info = cart(method, A, b, K, x0, options)
     else:
         X, info = art(method, A, b, K, x0, options)
     return X, info

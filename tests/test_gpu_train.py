@@ -35,6 +35,19 @@ def test_train_relaxpar(prob, method):
     assert abs(r_gpu - r_ref) <= 1e-9 * r_ref
 
 
+def test_train_relaxpar_columnaction(prob):
+    """train_relaxpar.m:90 runs CART through the ART branch (relaxpar 0.25 to
+    find kopt, golden section on (0, 2)); the oracle uses the FP32-rounded
+    matrix so that both take the same flagging decisions."""
+    A, A_ref, x, _, b, _ = prob
+    R = A_ref.copy().tocsc()
+    R.data = R.data.astype(np.float32).astype(np.float64)
+    r_gpu = T.train_relaxpar(A, b, x, "columnaction", 30, {})
+    r_ref = O.train_relaxpar(R, b, x, "columnaction", 30, {})
+    assert 0 < r_ref < 2
+    assert abs(r_gpu - r_ref) <= 1e-9 * r_ref
+
+
 @pytest.mark.parametrize("rule", ["DP", "ME"])
 def test_train_dpme(prob, rule):
     A, A_ref, x, b_ex, _, en = prob
