@@ -620,3 +620,20 @@ def test_fbp_matrix_free_and_batch():
     for k, th in enumerate(thetas):
         Ak, *_ = airt.paralleltomo(48, th)
         assert relerr(got[k], airt.fbp(Ak, bs[k], th, "hamming")) <= 1e-10
+
+
+def test_cart_residual_in_global_memory():
+    """N=128, 180 angles: a residual of 32,580 rows does not fit in shared
+    memory, so the sweep runs on the 256-thread CTA kernel; flagging and
+    unflagging active."""
+    theta = np.arange(0.0, 180.0, 1.0)
+    A_ref = O.paralleltomo_matrix(128, theta)
+    A, *_ = airt.paralleltomo(128, theta)
+    assert A.m == 32580
+    x = airt.random_ellipses(128, 8, seed=5)
+    b = A_ref @ x
+    opts = {"lbound": 0.0, "Kbegin": 2, "Nunflag": 2, "THR": 1e-2}
+    Xo, io = O.cart("columnaction", _f32(A_ref), b, [2, 4], None, opts)
+    X, info = airt.columnaction(A, b, [2, 4], None, opts)
+    assert relerr(X, Xo) <= CART_TOL
+    assert info["finaliter"] == io["finaliter"] == 4
