@@ -42,6 +42,25 @@ def test_golden_parallel_matrix():
     np.testing.assert_allclose(b, R @ g["x"], rtol=1e-6)
 
 
+def test_golden_widened_rows():
+    """libairt against widened_N16.npz: seismictomo and sphericaltomo matrices
+    bit-exact, CART columnaction iterates (1e-9) and fbp (1e-10)."""
+    g = np.load(os.path.join(GOLD, "paralleltomo_N16_30ang.npz"))
+    w = np.load(os.path.join(GOLD, "widened_N16.npz"))
+    As, *_ = airt.seismictomo(12, 6, 10)
+    same_matrix(As, sp.csc_matrix((w["seis_data"], w["seis_indices"], w["seis_indptr"]),
+                                  shape=tuple(w["seis_shape"])))
+    Aq, *_ = airt.sphericaltomo(10, np.arange(0.0, 360.0, 30.0), 8)
+    same_matrix(Aq, sp.csc_matrix((w["sph_data"], w["sph_indices"], w["sph_indptr"]),
+                                  shape=tuple(w["sph_shape"])))
+    A = airt.afun_matrix(sp.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=tuple(g["shape"])))
+    opts = {"lbound": 0.0, "Kbegin": 2, "Nunflag": 2, "THR": 1e-2, "seed": 5}
+    X, info = airt.columnaction(A, g["b"], [2, 6], None, opts)
+    assert relerr(X, w["cart_X"]) <= 1e-9 and info["finaliter"] == int(w["cart_finaliter"])
+    assert relerr(airt.fbp(A, g["b"], g["theta"], "hamming"), w["fbp_hamming"]) <= 1e-10
+    assert relerr(airt.fbp(A, g["b"], g["theta"], "ram-lak"), w["fbp_ramlak"]) <= 1e-10
+
+
 def test_golden_fan_matrix():
     g = np.load(os.path.join(GOLD, "fanlineartomo_N12_30ang.npz"))
     A, *_ = airt.fanlineartomo(12, np.arange(0.0, 360.0, 12.0), 17)

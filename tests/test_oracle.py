@@ -37,6 +37,27 @@ def test_golden_fanlineartomo_matrix():
     assert np.array_equal(F.data, g["data"])
 
 
+def test_golden_widened():
+    """widened_N16.npz: seismictomo and sphericaltomo matrices, CART and fbp
+    on the N=16 problem (FP32-rounded values) reproduce exactly."""
+    g = _load("paralleltomo_N16_30ang.npz")
+    w = _load("widened_N16.npz")
+    S = O.seismictomo_matrix(12, 6, 10)
+    Q = O.sphericaltomo_matrix(10, np.arange(0.0, 360.0, 30.0), 8)
+    for M, k in ((S, "seis"), (Q, "sph")):
+        assert np.array_equal(M.indptr, w[k + "_indptr"])
+        assert np.array_equal(M.indices, w[k + "_indices"])
+        assert np.array_equal(M.data, w[k + "_data"])
+    R = sp.csc_matrix((g["data"].astype(np.float32).astype(np.float64), g["indices"], g["indptr"]),
+                      shape=tuple(g["shape"]))
+    opts = {"lbound": 0.0, "Kbegin": 2, "Nunflag": 2, "THR": 1e-2, "seed": 5}
+    Xc, ic = O.cart("columnaction", R, g["b"], [2, 6], None, opts)
+    np.testing.assert_allclose(Xc, w["cart_X"], rtol=1e-12, atol=1e-13)
+    assert ic["finaliter"] == int(w["cart_finaliter"])
+    np.testing.assert_allclose(O.fbp(R, g["b"], g["theta"], "hamming"), w["fbp_hamming"], rtol=1e-12)
+    np.testing.assert_allclose(O.fbp(R, g["b"], g["theta"], "ram-lak"), w["fbp_ramlak"], rtol=1e-12)
+
+
 def test_golden_solvers():
     g = _load("paralleltomo_N16_30ang.npz")
     s = _load("solvers_N16_30ang.npz")
