@@ -248,6 +248,65 @@ def extra_legs(A_c2, b_c2, wl):
     _, ik = B.kaczmarz(np.concatenate(bs), 5)
     c4["kaczmarz_5_sweeps_ms"] = round(ik["gpu_ms"], 2)
     out["c4_batch"] = c4
+    out["widened"] = widened_legs(A_c2, b_c2, wl)
+    return out
+
+
+def widened_legs(A_c2, b_c2, wl):
+    """The rows beyond the SIRT/ART core, each timed once after an untimed
+    pass; a leg that fails reports its error instead of stopping the bench.
+
+    * CART columnaction: paralleltomo N=256, 60 angles (0:3:177 deg), 10
+      sweeps (residual in shared memory), and N=256, 180 angles, 3 sweeps
+      (residual in global memory); device time per sweep and per column.
+    * fbp (hamming) of the C2 sinogram (N=512, 360 angles x 724 rays) on the
+      stored C2 matrix: wall time and relative error against the phantom.
+    * Matrix generation for seismictomo N=256 (256 sources, 512 receivers)
+      and sphericaltomo N=256 (180 centres x 362 circles): wall time and nnz."""
+    import airtoolsii_b200 as airt
+    out = {}
+
+    def leg(name, fn):
+        try:
+            out[name] = fn()
+        except Exception as e:  # noqa: BLE001 -- recorded, not fatal
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+
+    def cart(na, sweeps):
+        A, b, x, *_ = airt.paralleltomo(256, np.arange(na) * (180.0 / na))
+        airt.columnaction(A, b, 1)
+        X, info = airt.columnaction(A, b, sweeps)
+        ms = info["gpu_ms"] / sweeps
+        return {"workload": f"paralleltomo N=256, {na} angles, columnaction {sweeps} sweeps",
+                "ms_per_sweep": round(ms, 3), "us_per_column": round(1e3 * ms / A.n, 4),
+                "relerr": round(float(np.linalg.norm(X[:, -1] - x) / np.linalg.norm(x)), 5)}
+
+    leg("cart_n256_a60", lambda: cart(60, 10))
+    leg("cart_n256_a180", lambda: cart(180, 3))
+
+    def fbp():
+        theta = np.arange(wl["nA"]) * wl["step"]
+        x = airt.random_ellipses(wl["N"], wl["ellipses"], seed=100)
+        airt.fbp(A_c2, b_c2, theta, "hamming")
+        t0 = _sync_s()
+        xf = airt.fbp(A_c2, b_c2, theta, "hamming")
+        t1 = _sync_s()
+        return {"workload": f"fbp (hamming), paralleltomo N={wl['N']}, {wl['nA']} angles x {wl['p']} rays",
+                "wall_ms": round(1e3 * (t1 - t0), 3),
+                "relerr": round(float(np.linalg.norm(xf - x) / np.linalg.norm(x)), 5)}
+
+    leg("fbp_c2", fbp)
+
+    def build(fn, label):
+        t0 = _sync_s()
+        A, *_ = fn()
+        t1 = _sync_s()
+        return {"workload": label, "build_s": round(t1 - t0, 3), "rows": A.m, "nnz": A.nnz}
+
+    leg("seismictomo_n256", lambda: build(lambda: airt.seismictomo(256),
+                                          "seismictomo N=256, 256 sources x 512 receivers"))
+    leg("sphericaltomo_n256", lambda: build(lambda: airt.sphericaltomo(256),
+                                            "sphericaltomo N=256, 180 centres x 362 circles"))
     return out
 
 
