@@ -48,6 +48,11 @@ __device__ __forceinline__ double clampv(double v, int64_t j, const KaczArgs &a)
   return v;
 }
 
+// Entries per lane whose gathered x is kept in registers across a row step:
+// for rows of up to 32 * kKaczCache entries the update reuses the value of x
+// the dot product read (the column indices and values it re-reads are in L1).
+constexpr int kKaczCache = 8;
+
 __global__ void __launch_bounds__(1024)
     k_kacz_levels(int nlev, const int *__restrict__ lev_ptr, const int *__restrict__ steps,
                   const int *__restrict__ step_pos, KaczArgs a) {
@@ -58,12 +63,33 @@ __global__ void __launch_bounds__(1024)
     for (int q = lev_ptr[L] + warp; q < q1; q += nw) {
       const int row = steps[q];
       const int64_t s0 = a.rp[row], s1 = a.rp[row + 1];
+      const int64_t e0 = s0 + lane;
+      // the gathers of the cached part are all issued before the first FMA;
+      // the FMAs run in the order of the plain strided loop
+      double cx[kKaczCache];
+#pragma unroll
+      for (int u = 0; u < kKaczCache; ++u)
+        cx[u] = e0 + 32 * u < s1 ? a.x[a.ci[e0 + 32 * u]] : 0.0;
       double acc = 0.0;
-      for (int64_t e = s0 + lane; e < s1; e += 32) acc = fma((double)a.rv[e], a.x[a.ci[e]], acc);
+#pragma unroll
+      for (int u = 0; u < kKaczCache; ++u)
+        if (e0 + 32 * u < s1) acc = fma((double)a.rv[e0 + 32 * u], cx[u], acc);
+      for (int64_t e = e0 + 32 * kKaczCache; e < s1; e += 32)
+        acc = fma((double)a.rv[e], a.x[a.ci[e]], acc);
       acc = warp_sum(acc);
       const double lam = a.lam_tab ? a.lam_tab[step_pos[q]] : a.lam;
       const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(a.b[row], acc)), a.nrm[row]);
-      for (int64_t e = s0 + lane; e < s1; e += 32) {
+      // no other step of this level touches these pixels, so the gathered x
+      // is still the current value
+#pragma unroll
+      for (int u = 0; u < kKaczCache; ++u)
+        if (e0 + 32 * u < s1) {
+          const int j = a.ci[e0 + 32 * u];
+          double v = __dadd_rn(cx[u], __dmul_rn(c, (double)a.rv[e0 + 32 * u]));
+          if (clamp) v = clampv(v, j, a);
+          a.x[j] = v;
+        }
+      for (int64_t e = e0 + 32 * kKaczCache; e < s1; e += 32) {
         const int j = a.ci[e];
         double v = __dadd_rn(a.x[j], __dmul_rn(c, (double)a.rv[e]));
         if (clamp) v = clampv(v, j, a);
