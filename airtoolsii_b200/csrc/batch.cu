@@ -885,6 +885,8 @@ __global__ void k_level_fill(int64_t m, const int64_t *__restrict__ roff, const 
   }
 }
 
+constexpr int kBatchKaczCache = 6;  // gathered x values a lane keeps for the update
+
 // Kaczmarz sweeps of one instance per CTA over its level schedule: the steps
 // of a level touch disjoint pixels and run one per warp (fixed lane order and
 // shuffle tree); a block barrier separates levels, so every pixel sees the
@@ -905,11 +907,31 @@ __global__ void __launch_bounds__(512)
       for (int q = lp[L] + warp; q < q1; q += nw) {
         const int row = steps[q];
         const int64_t s0 = rp[row], s1 = rp[row + 1];
+        const int64_t e0 = s0 + lane;
+        // the first kBatchKaczCache gathers per lane are issued together and
+        // kept for the update (no other step of the level touches these
+        // pixels); the FMAs keep the order of the plain strided loop
+        double cx[kBatchKaczCache];
+#pragma unroll
+        for (int u = 0; u < kBatchKaczCache; ++u)
+          cx[u] = e0 + 32 * u < s1 ? x[ci[e0 + 32 * u]] : 0.0;
         double acc = 0.0;
-        for (int64_t e = s0 + lane; e < s1; e += 32) acc = fma((double)rv[e], x[ci[e]], acc);
+#pragma unroll
+        for (int u = 0; u < kBatchKaczCache; ++u)
+          if (e0 + 32 * u < s1) acc = fma((double)rv[e0 + 32 * u], cx[u], acc);
+        for (int64_t e = e0 + 32 * kBatchKaczCache; e < s1; e += 32)
+          acc = fma((double)rv[e], x[ci[e]], acc);
         acc = warp_sum(acc);
         const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(b[row], acc)), nrm[row]);
-        for (int64_t e = s0 + lane; e < s1; e += 32) {
+#pragma unroll
+        for (int u = 0; u < kBatchKaczCache; ++u)
+          if (e0 + 32 * u < s1) {
+            double v = __dadd_rn(cx[u], __dmul_rn(c, (double)rv[e0 + 32 * u]));
+            if (lbk) v = fmax(v, lb);
+            if (ubk) v = fmin(v, ub);
+            x[ci[e0 + 32 * u]] = v;
+          }
+        for (int64_t e = e0 + 32 * kBatchKaczCache; e < s1; e += 32) {
           const int j = ci[e];
           double v = __dadd_rn(x[j], __dmul_rn(c, (double)rv[e]));
           if (lbk) v = fmax(v, lb);
