@@ -159,3 +159,25 @@ def test_randk_stream_matches_oracle_stream():
         ri, ii = O.art_sweep_rows(I, normAi, True, st, normAi.size)
         np.testing.assert_array_equal(rows[k], ri)
         np.testing.assert_array_equal(lam_rows[k], ii)
+
+
+def test_bench_reference_arm_json_contract():
+    """bench.py --impl reference (the CPU restatement timed on the host) prints
+    one JSON line with the contract's keys, on the small workload."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                          "--small", "--steps", "1", "--warmup", "3"],
+                         capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+                "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0 and line["warmup"] >= 3
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] in ("port", "reference") and line["cpu_baseline"]["cores"] >= 1
+    assert "workload" in line["config"]
