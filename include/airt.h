@@ -8,6 +8,9 @@
  * keeps FP32 CSR/CSC matrices and FP64 vectors in HBM, and owns device memory
  * until airt_destroy().  Functions ending in _device take device pointers and
  * run on the problem's CUDA stream (airt_problem_stream) without host copies.
+ * A handle keeps work buffers between calls, so calls on the same handle must
+ * not overlap (one host thread at a time per handle); distinct handles are
+ * independent.  airt_last_error() is per host thread.
  *
  * Reference interfaces replaced (AIR Tools II V1.0, paths inside its tree):
  *   airt_problem_from_csc  -> auxil/check_inputs.m:67-71 (matrix wrapped as afun)
