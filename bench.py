@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--method", default="cimmino")
     ap.add_argument("--iters", type=int, default=200)
     ap.add_argument("--small", action="store_true", help="N=256 problem (profiling captures)")
+    ap.add_argument("--tiny", action="store_true",
+                    help="N=48 problem (checks of the output line's contract, not a measurement)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start time-to-DP leg")
     ap.add_argument("--no-extra", action="store_true", help="skip the C2-methods / C3 / C4 legs")
@@ -57,7 +59,9 @@ def parse():
     return ap.parse_args()
 
 
-def workload(small: bool):
+def workload(small: bool, tiny: bool = False):
+    if tiny:
+        return dict(N=48, nA=60, p=68, step=3.0, ellipses=10, eta=0.01)
     if small:
         return dict(N=256, nA=360, p=362, step=0.5, ellipses=30, eta=0.005)
     return dict(N=512, nA=360, p=724, step=0.5, ellipses=30, eta=0.005)
@@ -396,13 +400,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    wl = workload(a.small)
+    wl = workload(a.small, a.tiny)
     cfg = {"workload": f"paralleltomo N={wl['N']}, {wl['nA']} angles x {wl['p']} rays, "
                        f"{a.method} {a.iters} iterations, box [0,1], FP32 CSR+CSC",
            "N": wl["N"], "angles": wl["nA"], "rays": wl["p"], "method": a.method,
            "iterations": a.iters, "phantom": f"{wl['ellipses']} random ellipses",
-           "noise": wl["eta"], "l2": "inputs larger than L2 (A ~1.9 GB)" if not a.small else
-           "inputs larger than L2 (A ~0.25 GB)", "parallelism": f"replicas x{a.gpus}"}
+           "noise": wl["eta"], "l2": ("contract-check case, fits in L2" if a.tiny else
+                                      "inputs larger than L2 (A ~0.25 GB)" if a.small else
+                                      "inputs larger than L2 (A ~1.9 GB)"),
+           "parallelism": f"replicas x{a.gpus}"}
     metric = "SIRT SpMV HBM GB/s (CSR+CSC byte model, plain GPU SIRT)"
 
     if a.impl == "reference":
@@ -591,12 +597,11 @@ def reference_arm(a, wl, cfg, metric):
     del rows, cols, vals
     m, n = A.shape
     nnz = A.nnz
-    from airtoolsii_b200.testprobs import add_noise, random_ellipses  # data generator only
-    x = random_ellipses(wl["N"], wl["ellipses"], seed=100)
-    b, _ = add_noise(A @ x, wl["eta"], seed=200)
+    x = O.random_ellipses(wl["N"], wl["ellipses"], seed=100)
+    b, _ = O.add_noise(A @ x, wl["eta"], seed=200)
     M, D, _, _ = O.get_mfun_dfun(a.method, A)
     lam = 1.0
-    sample = 2 if not a.small else 10
+    sample = 10 if (a.small or a.tiny) else 2
     prep = cbind.PreparedSirt(A, b, M, D)
     for _ in range(max(a.warmup, 3)):
         prep.run(lam, 0.0, 1.0, 1)

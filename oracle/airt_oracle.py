@@ -499,6 +499,33 @@ def shepplogan(N):
     return ellipse_image(N, e).ravel(order="F")
 
 
+def random_ellipses(N, count, seed):
+    """Seeded random-ellipse phantom as x(:), drawn in the same order from the
+    same NumPy generator as the product's data generator: centres
+    U[-0.6,0.6]^2, semi-axes U[0.05,0.4], rotation U[0,pi), intensity
+    U[0.1,1], additive on the phantomgallery.m:188-190 grid, clipped to
+    [0,1].  The CPU benchmark arm draws its inputs here so that it loads no
+    part of the product."""
+    rng = np.random.default_rng(seed)
+    ell = []
+    for _ in range(count):
+        cx, cy = rng.uniform(-0.6, 0.6, 2)
+        a, b = rng.uniform(0.05, 0.4, 2)
+        phi = rng.uniform(0.0, math.pi)
+        amp = rng.uniform(0.1, 1.0)
+        ell.append((amp, a, b, cx, cy, phi))
+    return ellipse_image(N, ell, clip_hi=1.0).ravel(order="F")
+
+
+def add_noise(b, eta, seed):
+    """b + e, e Gaussian from a seeded NumPy generator scaled to
+    ||e|| = eta*||b|| (demos/demo_stoprules.m:43-46); returns (b + e, ||e||)."""
+    rng = np.random.default_rng(seed)
+    e = rng.standard_normal(b.size)
+    e = eta * np.linalg.norm(b) * e / np.linalg.norm(e)
+    return b + e, float(np.linalg.norm(e))
+
+
 # ---------------------------------------------------------------------------
 # Solver auxiliaries
 # ---------------------------------------------------------------------------

@@ -163,16 +163,24 @@ def test_randk_stream_matches_oracle_stream():
 
 def test_bench_reference_arm_json_contract():
     """bench.py --impl reference (the CPU restatement timed on the host) prints
-    one JSON line with the contract's keys, on the small workload."""
+    one JSON line with the contract's keys (N=48 contract-check case), and the
+    process that runs it imports no part of the product: neither the
+    airtoolsii_b200 package nor a mapping of libairt.so."""
     import json
     import subprocess
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
-                          "--small", "--steps", "1", "--warmup", "3"],
-                         capture_output=True, text=True, timeout=600, cwd=root)
+    probe = ("import sys, runpy\n"
+             "sys.argv = ['bench.py', '--impl', 'reference', '--tiny', '--steps', '1', '--warmup', '3']\n"
+             "runpy.run_path('bench.py', run_name='__main__')\n"
+             "maps = open('/proc/self/maps').read()\n"
+             "print('PRODUCT_LOADED', int('airtoolsii_b200' in sys.modules or 'libairt' in maps))\n")
+    out = subprocess.run([sys.executable, "-c", probe], capture_output=True, text=True,
+                         timeout=300, cwd=root)
     assert out.returncode == 0, out.stderr[-2000:]
-    line = json.loads(out.stdout.strip().splitlines()[-1])
+    lines = out.stdout.strip().splitlines()
+    assert lines[-1] == "PRODUCT_LOADED 0", lines[-1]
+    line = json.loads(lines[-2])
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
                 "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
                 "cpu_baseline", "e2e"):
@@ -181,3 +189,15 @@ def test_bench_reference_arm_json_contract():
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] in ("port", "reference") and line["cpu_baseline"]["cores"] >= 1
     assert "workload" in line["config"]
+
+
+def test_oracle_data_generators_match_product():
+    """The CPU benchmark arm draws phantom and noise from the oracle's copies of
+    the generators; they give the same arrays as the product's for a seed."""
+    x1 = testprobs.random_ellipses(40, 12, seed=77)
+    x2 = O.random_ellipses(40, 12, seed=77)
+    np.testing.assert_array_equal(x1, x2)
+    b1, e1 = testprobs.add_noise(x1 * 3.0, 0.02, seed=78)
+    b2, e2 = O.add_noise(x2 * 3.0, 0.02, seed=78)
+    np.testing.assert_array_equal(b1, b2)
+    assert e1 == e2
