@@ -70,6 +70,21 @@ __global__ void k_csc64_to_f32(int64_t nnz, const uint64_t *__restrict__ ir, con
   }
 }
 
+// MATLAB's canonical sparse form: row indices strictly increasing within
+// each column (no duplicates).  One thread per column; sets *bad = 2.
+__global__ void k_check_col_sorted(int64_t n, const uint64_t *__restrict__ jc,
+                                   const uint64_t *__restrict__ ir, int *bad) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t q1 = jc[j + 1];
+    for (uint64_t q = jc[j] + 1; q < q1; ++q)
+      if (ir[q] <= ir[q - 1]) {
+        atomicExch(bad, 2);
+        break;
+      }
+  }
+}
+
 __global__ void k_u64_to_i64(int64_t n, const uint64_t *__restrict__ a, int64_t *__restrict__ b) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
        q += (int64_t)gridDim.x * blockDim.x)
@@ -187,11 +202,16 @@ void build_csr_from_host_csc(Problem &P, const uint64_t *jc, const uint64_t *ir,
     k_csc64_to_f32<<<grid_for(P.nnz, 256), 256, 0, s>>>(P.nnz, dir.p, dpr.p, P.ri.p, P.cv.p, P.m,
                                                          bad.p);
     AIRT_LAUNCH_CHECK();
+    k_check_col_sorted<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, djc.p, dir.p, bad.p);
+    AIRT_LAUNCH_CHECK();
   }
   int hbad = 0;
   AIRT_CHECK_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-  AIRT_REQUIRE(!hbad, "row index out of range in the CSC input");
+  AIRT_REQUIRE(hbad != 1, "row index out of range in the CSC input");
+  AIRT_REQUIRE(hbad != 2,
+               "row indices of a CSC column are not strictly increasing (the matrix must be in "
+               "MATLAB's canonical sparse form: sorted, no duplicate entries)");
   transpose(P.n, P.m, P.nnz, P.cp.p, P.ri.p, P.cv.p, P.rp, P.ci, P.rv, s);
 }
 

@@ -145,8 +145,9 @@ int airt_version(void);
 
 /* ---- problem construction ------------------------------------------------- */
 /* MATLAB sparse layout (mxGetJc / mxGetIr / mxGetPr): jc n+1 column starts,
- * ir nnz row indices, pr nnz values.  Replaces the matrix branch of
- * auxil/check_inputs.m:67-71 and auxil/afun_matrix.m:44-53. */
+ * ir nnz row indices, pr nnz values, in MATLAB's canonical form (row indices
+ * strictly increasing within each column: AIRT_ERR_ARG otherwise).  Replaces
+ * the matrix branch of auxil/check_inputs.m:67-71 and auxil/afun_matrix.m:44-53. */
 int airt_problem_from_csc(int64_t m, int64_t n, const uint64_t *jc, const uint64_t *ir,
                           const double *pr, airt_problem **out);
 
@@ -325,10 +326,14 @@ int airt_phantom_ellipses(int N, int nimg, int nell, const double *params, doubl
  * GPU memory budget through its own pool, or code that must not call
  * cudaMalloc/cudaFree because they synchronise the device.  It allocates
  * nothing; its scratch is a static 4 MiB + 256 B device array, so n is limited
- * to 1,048,576 unknowns (AIRT_ERR_ARG beyond).  The first call on a device
- * looks the array up and should come before any stream capture; calls that
- * overlap on the GPU race on the shared scratch.  Runs on cuda_stream (NULL =
- * legacy default stream). */
+ * to 1,048,576 unknowns (AIRT_ERR_ARG beyond).  The array's address belongs
+ * to a CUDA context: the first call in each context (the first call on a
+ * device, and again after cudaDeviceReset or in a context the caller made
+ * current) looks it up and should come before any stream capture.  Calls that
+ * overlap on the GPU race on the shared scratch, so order them.  Every d_ci
+ * entry must lie in [0, n) and d_rp must be nondecreasing with d_rp[m] the
+ * number of entries; an index outside [0, n) is skipped and the call writes
+ * NaN to d_resnorm.  Runs on cuda_stream (NULL = legacy default stream). */
 int airt_residual_noalloc(int64_t m, int64_t n, const int64_t *d_rp, const int *d_ci,
                           const float *d_rv, const double *d_x, const double *d_b, double *d_r,
                           double *d_resnorm, void *cuda_stream);

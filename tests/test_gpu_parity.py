@@ -187,6 +187,26 @@ def test_csc_upload_roundtrip_and_apply():
     assert list(op(None, "size")) == [300, 200]
 
 
+def test_csc_with_unsorted_or_duplicate_rows_is_rejected():
+    """airt_problem_from_csc takes MATLAB's canonical sparse form only: a
+    column whose row indices repeat or decrease is an argument error."""
+    import ctypes as C
+    from airtoolsii_b200 import _lib
+    L = _lib.lib()
+    h = C.c_void_p()
+    jc = np.array([0, 2, 3], np.uint64)
+    pr = np.array([1.0, 2.0, 3.0])
+    for ir in (np.array([1, 1, 0], np.uint64), np.array([2, 0, 1], np.uint64)):
+        st = L.airt_problem_from_csc(3, 2, _lib.u64ptr(jc), _lib.u64ptr(ir), _lib.dptr(pr),
+                                     C.byref(h))
+        assert st == _lib.AIRT_ERR_ARG
+        assert b"strictly increasing" in L.airt_last_error()
+    ir = np.array([0, 2, 1], np.uint64)
+    assert L.airt_problem_from_csc(3, 2, _lib.u64ptr(jc), _lib.u64ptr(ir), _lib.dptr(pr),
+                                   C.byref(h)) == _lib.AIRT_OK
+    L.airt_destroy(h)
+
+
 def test_empty_and_degenerate_matrices():
     op = airt.afun_matrix(sp.csc_matrix((5, 4)))
     assert op.nnz == 0
