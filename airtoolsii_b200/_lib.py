@@ -38,7 +38,7 @@ class SirtOpts(C.Structure):
                 ("taudelta", C.c_double), ("lb_kind", C.c_int), ("ub_kind", C.c_int),
                 ("lb", C.c_double), ("ub", C.c_double), ("lbv", _dp), ("ubv", _dp),
                 ("kmax", C.c_int64), ("ncp_rows", C.c_int), ("ncp_cols", C.c_int),
-                ("ncp_smooth", C.c_int)]
+                ("ncp_smooth", C.c_int), ("M_full", C.c_int), ("D_full", C.c_int)]
 
 
 class ArtOpts(C.Structure):
@@ -87,6 +87,8 @@ SIGNATURES = {
     "airt_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "airt_weights": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "airt_rho": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.c_double, C.c_int, _dp]),
+    "airt_rho_custom": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, C.c_int, C.c_double, C.c_int,
+                                  _dp]),
     "airt_sirt": (C.c_int, [C.c_void_p, C.POINTER(SirtOpts), _dp, _dp, _i64p, C.c_int64, _dp,
                             _dp, C.POINTER(Info)]),
     "airt_sirt_device": (C.c_int, [C.c_void_p, C.POINTER(SirtOpts), C.c_void_p, C.c_void_p, _i64p,

@@ -369,6 +369,34 @@ int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *D
   AIRT_API_END
 }
 
+int airt_rho_custom(airt_problem *h, const double *M, int M_full, const double *D, int D_full,
+                    double tol, int maxit, double *rho) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && rho, "null pointer argument");
+  AIRT_REQUIRE(maxit > 0 && tol >= 0, "invalid tolerance or iteration limit");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  const bool mf = M && M_full, df = D && D_full;
+  AIRT_REQUIRE(!mf || (double)P->m * (double)P->m <= 4e9, "a full custom M does not fit the device");
+  AIRT_REQUIRE(!df || (double)P->n * (double)P->n <= 4e9, "a full custom D does not fit the device");
+  const double *dM = nullptr, *dD = nullptr;
+  if (mf) {
+    P->Mfull.upload(M, (size_t)P->m * P->m, P->stream);
+    dM = P->Mfull.p;
+  } else if (M) {
+    P->M.upload(M, P->m, P->stream);
+    dM = P->M.p;
+  }
+  if (df) {
+    P->Dfull.upload(D, (size_t)P->n * P->n, P->stream);
+    dD = P->Dfull.p;
+  } else if (D) {
+    P->D.upload(D, P->n, P->stream);
+    dD = P->D.p;
+  }
+  *rho = estimate_rho_custom(*P, dM, mf, dD, df, tol, maxit);
+  AIRT_API_END
+}
+
 int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *d_b,
                      const double *d_x0, const int64_t *K, int64_t nK, double *d_X,
                      double *resnorms, airt_info *info) {

@@ -180,6 +180,9 @@ struct Problem {
 
   // solver work vectors
   DevBuf<double> x64, r64, rprev, g64, b64, M, D, lbv, ubv, vin, vout, table, resn, lamh, Xd;
+  // custom SIRT weights given as full matrices (get_mfun_dfun.m:252-307, flag 2):
+  // column-major m x m / n x n, and the column sums of D (line search)
+  DevBuf<double> Mfull, Dfull, Dcol, dscratch;
   // NCP stopping rule: DFT twiddles (cos, sin pairs), power spectra, column distances, history
   DevBuf<double> ncp_tw, ncp_pk, ncp_col, ncp_dk;
   // fbp: filter kernel, per-column scales, filtered sinogram (kept between calls)
@@ -306,6 +309,10 @@ void run_cart(Problem &P, const airt_cart_opts &o, const double *d_b, const doub
 void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double *d_x0,
              const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
 double estimate_rho(Problem &P, const double *dM, const double *dD, double tol, int maxit);
+// Custom weights: dM / dD are device diagonals, or full column-major matrices
+// when mfull / dfull; nullptr is the identity.
+double estimate_rho_custom(Problem &P, const double *dM, bool mfull, const double *dD, bool dfull,
+                           double tol, int maxit);
 void export_csc(Problem &P, uint64_t *jc, uint64_t *ir, double *pr);
 void row_sums_sq(Problem &P, double *out);
 

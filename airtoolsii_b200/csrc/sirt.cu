@@ -280,6 +280,96 @@ __global__ void __launch_bounds__(kThreads) k_dg2(int64_t n, const double *__res
   if (threadIdx.x == 0) atomicAdd(&st->acc[4], a);
 }
 
+// ---- custom weights given as full matrices (get_mfun_dfun.m:252-307,
+// Mflag/Dflag = 2): M*r and D*g are dense FP64 products over the caller's
+// column-major matrix.  A block of 256 threads owns 32 consecutive rows;
+// thread (row lane l, phase c) sums columns j = c, c+8, ... of its row (the
+// 32 lanes of a warp read 256 contiguous bytes of one column and share the
+// broadcast v[j]), and the 8 phase sums are added in a fixed order, so the
+// product repeats bit for bit.
+constexpr int kGemvRows = 32, kGemvPhases = 8;
+
+__device__ __forceinline__ double dense_row(int64_t k, const double *__restrict__ W,
+                                            const double *__restrict__ v, int64_t row,
+                                            double (*part)[kGemvRows]) {
+  const int l = threadIdx.x % kGemvRows, c = threadIdx.x / kGemvRows;
+  double a0 = 0.0, a1 = 0.0;
+  if (row < k) {
+    const double *__restrict__ w = W + row;
+    int64_t j = c;
+    for (; j + kGemvPhases < k; j += 2 * kGemvPhases) {
+      a0 = fma(w[j * k], v[j], a0);
+      a1 = fma(w[(j + kGemvPhases) * k], v[j + kGemvPhases], a1);
+    }
+    if (j < k) a0 = fma(w[j * k], v[j], a0);
+  }
+  part[c][l] = a0 + a1;
+  __syncthreads();
+  double y = 0.0;
+  if (c == 0)
+    for (int q = 0; q < kGemvPhases; ++q) y += part[q][l];
+  return y;  // valid on the phase-0 threads (threadIdx.x < 32)
+}
+
+// y = W*v (rho estimation).
+__global__ void __launch_bounds__(256) k_dense_apply(int64_t k, const double *__restrict__ W,
+                                                     const double *__restrict__ v,
+                                                     double *__restrict__ y) {
+  __shared__ double part[kGemvPhases][kGemvRows];
+  const int64_t row = blockIdx.x * (int64_t)kGemvRows + threadIdx.x % kGemvRows;
+  const double r = dense_row(k, W, v, row, part);
+  if (threadIdx.x < kGemvRows && row < k) y[row] = r;
+}
+
+// M*r with M full (r = the residual kept by the forward pass): the FP32 copy
+// for the transpose gather, and r'*M*r into acc[1] (sirt.m:221).
+__global__ void __launch_bounds__(256) k_dense_M(int64_t m, const double *__restrict__ Mf,
+                                                 const double *__restrict__ r,
+                                                 float *__restrict__ mr32, SirtState *st) {
+  if (stopped(st)) return;
+  __shared__ double part[kGemvPhases][kGemvRows];
+  const int64_t row = blockIdx.x * (int64_t)kGemvRows + threadIdx.x % kGemvRows;
+  const double y = dense_row(m, Mf, r, row, part);
+  if (threadIdx.x < kGemvRows) {
+    double a = 0.0;
+    if (row < m) {
+      mr32[row] = (float)y;
+      a = r[row] * y;
+    }
+    a = group_sum<32>(a);
+    if (threadIdx.x == 0) atomicAdd(&st->acc[1], a);
+  }
+}
+
+// x += lam * (D*g) with D full (sirt.m:229), then the box projection, the
+// FP32 copy and the save of x; LINE takes the line-search relaxpar.
+template <bool LINE>
+__global__ void __launch_bounds__(256) k_dense_D_update(const double *__restrict__ Df,
+                                                        const double *__restrict__ g, UpdArgs u) {
+  if (stopped(u.st)) return;
+  __shared__ double part[kGemvPhases][kGemvRows];
+  const int it = u.st->iter;
+  const int slot = u.save_slot[it];
+  const double lam = LINE ? u.st->rmr_prev / u.st->acc[4] : u.st->lam_cur;
+  const int64_t row = blockIdx.x * (int64_t)kGemvRows + threadIdx.x % kGemvRows;
+  const double y = dense_row(u.n, Df, g, row, part);
+  if (LINE && blockIdx.x == 0 && threadIdx.x == 0) u.st->lam_cur = lam;
+  if (threadIdx.x < kGemvRows && row < u.n) update_x_pre(row, y, lam, u, slot, u.x64[row], 1.0);
+}
+
+// Column sums of a full column-major D: sum(D*(g.^2)) = sum_j colsum_j g_j^2
+// (the line-search denominator of sirt.m:220).
+__global__ void k_colsum(int64_t k, const double *__restrict__ W, double *__restrict__ out) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < k;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int64_t i = 0; i < k; ++i) a += W[i + j * k];
+    out[j] = a;
+  }
+}
+
+inline unsigned dense_grid(int64_t k) { return (unsigned)((k + kGemvRows - 1) / kGemvRows); }
+
 // Stopping rule of check_stoprules.m on the sums of the residual just
 // computed, then the relaxpar of the next iteration (sirt.m:216-226).
 __global__ void k_sirt_ctrl(SirtState *st, const SirtParams *p) {
@@ -438,12 +528,25 @@ void launch_bwd_t(Problem &P, const UpdArgs &u) {
   }
 }
 
-void launch_bwd(Problem &P, const UpdArgs &u, int relax_kind) {
+void launch_bwd(Problem &P, const UpdArgs &u, int relax_kind, const double *Dfull) {
   cudaStream_t s = P.stream;
   cudaEvent_t e0 = nullptr;
   prof_begin(P, 1, &e0);
   const unsigned ge = grid_for(P.n, kThreads);
-  if (P.matrix_free) {
+  const bool line = relax_kind == AIRT_RELAX_LINE;
+  if (Dfull) {
+    // g = A'*(M.*r) kept in g64 with sum(colsum(D).*g.^2), then the dense update
+    UpdArgs ul = u;
+    ul.D = P.Dcol.p;
+    if (P.matrix_free) {
+      mf_backproject_f32(P, P.mr32.p, P.g64.p, &P.state.p->stop);
+      if (line) k_dg2<<<ge, kThreads, 0, s>>>(P.n, P.Dcol.p, P.g64.p, P.state.p);
+    } else {
+      launch_bwd_t<1>(P, ul);
+    }
+    if (line) k_dense_D_update<true><<<dense_grid(P.n), 256, 0, s>>>(Dfull, P.g64.p, u);
+    else k_dense_D_update<false><<<dense_grid(P.n), 256, 0, s>>>(Dfull, P.g64.p, u);
+  } else if (P.matrix_free) {
     mf_backproject_f32(P, P.mr32.p, P.g64.p, &P.state.p->stop);
     if (relax_kind == AIRT_RELAX_LINE) {
       k_dg2<<<ge, kThreads, 0, s>>>(P.n, P.D.p, P.g64.p, P.state.p);
@@ -487,8 +590,9 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   AIRT_REQUIRE(o.relax_kind != AIRT_RELAX_TABLE || o.relax_table || o.kmax == 0,
                "relax_table required");
   const int64_t kmax = o.kmax;
-  // NCP needs the residual itself: the ME variant of the forward kernel keeps it
-  const bool me = o.stoprule == AIRT_STOP_ME || ncp;
+  // NCP and a full custom M need the residual itself: the ME variant of the
+  // forward kernel keeps it
+  const bool me = o.stoprule == AIRT_STOP_ME || ncp || (o.method == AIRT_CUSTOM && o.M && o.M_full);
 
   cudaEvent_t t0, t1;
   AIRT_CHECK_CUDA(cudaEventCreate(&t0));
@@ -501,17 +605,40 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   // weights (get_mfun_dfun.m)
   P.M.ensure(m);
   P.D.ensure(n);
+  const bool mfull = o.method == AIRT_CUSTOM && o.M && o.M_full;
+  const bool dfull = o.method == AIRT_CUSTOM && o.D && o.D_full;
   if (o.method == AIRT_CUSTOM) {
-    std::vector<double> ones;
-    if (o.M) P.M.upload(o.M, m, s);
-    else {
-      ones.assign(m, 1.0);
-      P.M.upload(ones.data(), m, s);
+    AIRT_REQUIRE(!mfull || (double)m * (double)m <= 4e9,
+                 "a full custom M of %lld x %lld does not fit the device", (long long)m,
+                 (long long)m);
+    AIRT_REQUIRE(!dfull || (double)n * (double)n <= 4e9,
+                 "a full custom D of %lld x %lld does not fit the device", (long long)n,
+                 (long long)n);
+    std::vector<double> fill;
+    if (mfull) {
+      // the forward pass keeps r and adds nothing to r'*M*r (M diagonal 0);
+      // k_dense_M forms M*r and r'*M*r
+      P.Mfull.upload(o.M, (size_t)m * m, s);
+      fill.assign(m, 0.0);
+      P.M.upload(fill.data(), m, s);
+    } else if (o.M) {
+      P.M.upload(o.M, m, s);
+    } else {
+      fill.assign(m, 1.0);
+      P.M.upload(fill.data(), m, s);
     }
-    if (o.D) P.D.upload(o.D, n, s);
-    else {
-      ones.assign(n, 1.0);
-      P.D.upload(ones.data(), n, s);
+    if (dfull) {
+      P.Dfull.upload(o.D, (size_t)n * n, s);
+      P.Dcol.ensure(n);
+      k_colsum<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, P.Dfull.p, P.Dcol.p);
+      AIRT_LAUNCH_CHECK();
+      fill.assign(n, 1.0);
+      P.D.upload(fill.data(), n, s);
+    } else if (o.D) {
+      P.D.upload(o.D, n, s);
+    } else {
+      fill.assign(n, 1.0);
+      P.D.upload(fill.data(), n, s);
     }
     AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   } else {
@@ -523,7 +650,7 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   P.x32.ensure(n);
   P.mr32.ensure(m);
   if (me) P.rprev.ensure(m);
-  if (o.relax_kind == AIRT_RELAX_LINE || P.matrix_free) P.g64.ensure(n);
+  if (o.relax_kind == AIRT_RELAX_LINE || P.matrix_free || dfull) P.g64.ensure(n);
   if (d_x0)
     k_copy<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, d_x0, P.x64.p);
   else
@@ -598,8 +725,13 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
   ua.g64 = P.g64.p;
 
   // forward pass, and with NCP the periodogram of the new residual
+  const double *Dfull = dfull ? P.Dfull.p : nullptr;
   auto fwd = [&]() {
     launch_fwd(P, fo, me);
+    if (mfull) {
+      k_dense_M<<<dense_grid(m), 256, 0, s>>>(m, P.Mfull.p, P.rprev.p, P.mr32.p, P.state.p);
+      AIRT_LAUNCH_CHECK();
+    }
     if (ncp) {
       k_ncp_power<<<dim3(o.ncp_cols, (ncp_q + 255) / 256), 256, 0, s>>>(o.ncp_rows, ncp_q, P.rprev.p,
                                                                       P.ncp_tw.p, P.ncp_pk.p, &P.state.p->stop);
@@ -634,7 +766,7 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
     cudaGraph_t g = nullptr;
     AIRT_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int64_t j = 0; j < chunk; ++j) {
-      launch_bwd(P, ua, o.relax_kind);
+      launch_bwd(P, ua, o.relax_kind, Dfull);
       fwd();
       k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
     }
@@ -651,7 +783,7 @@ void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const doub
       AIRT_CHECK_CUDA(cudaGraphLaunch(chunk_graph, s));
     } else {
       for (int64_t j = 0; j < cnt; ++j) {
-        launch_bwd(P, ua, o.relax_kind);
+        launch_bwd(P, ua, o.relax_kind, Dfull);
         fwd();
         k_sirt_ctrl<<<1, 32, 0, s>>>(P.state.p, P.params.p);
       }
@@ -847,6 +979,69 @@ double estimate_rho(Problem &P, const double *dM, const double *dD, double tol, 
     std::swap(vprev.p, v.p);
     std::swap(vprev.n, v.n);
     k_scale_by<<<gn, kThreads, 0, s>>>(n, 1.0 / b, w.p, v.p);
+    AIRT_LAUNCH_CHECK();
+  }
+  return theta;
+}
+
+// Dominant eigenvalue of T = D*A'*M*A for custom weights that may be full
+// matrices (T is then not similar to a symmetric operator built from
+// diagonal square roots, so the Lanczos form above does not apply): the
+// power iteration v <- T v / ||T v|| from the normalised ones vector with the
+// Rayleigh quotient v'*T*v as the estimate, stopped once it changes by at
+// most tol (relative) after at least five steps, or after maxit steps.
+// Replaces eigs(atma,n,1,'lm') of calc_relaxpar.m:91-103 for these weights.
+double estimate_rho_custom(Problem &P, const double *dM, bool mfull, const double *dD, bool dfull,
+                           double tol, int maxit) {
+  cudaStream_t s = P.stream;
+  const int64_t m = P.m, n = P.n;
+  if (n == 0) return 0.0;
+  DevBuf<double> v, t, y, y2, w, red;
+  v.ensure(n);
+  t.ensure(n);
+  y.ensure(std::max<int64_t>(m, 1));
+  y2.ensure(std::max<int64_t>(m, 1));
+  w.ensure(n);
+  red.ensure(2);
+  const unsigned gn = grid_for(n, kThreads), gm = grid_for(std::max<int64_t>(m, 1), kThreads);
+  std::vector<double> h(n, 1.0 / std::sqrt((double)n));
+  v.upload(h.data(), n, s);
+  double theta = 0.0, prev = 0.0;
+  for (int it = 0; it < std::max(maxit, 1); ++it) {
+    if (m) {
+      apply_operator(P, v.p, y.p, 0);
+      const double *my = y.p;
+      if (dM && mfull) {
+        k_dense_apply<<<dense_grid(m), 256, 0, s>>>(m, dM, y.p, y2.p);
+        my = y2.p;
+      } else if (dM) {
+        k_mul<<<gm, kThreads, 0, s>>>(m, dM, y.p, y.p);
+      }
+      apply_operator(P, my, t.p, 1);
+    } else {
+      AIRT_CHECK_CUDA(cudaMemsetAsync(t.p, 0, n * sizeof(double), s));
+    }
+    const double *tw = t.p;
+    if (dD && dfull) {
+      k_dense_apply<<<dense_grid(n), 256, 0, s>>>(n, dD, t.p, w.p);
+      tw = w.p;
+    } else if (dD) {
+      k_mul<<<gn, kThreads, 0, s>>>(n, dD, t.p, w.p);
+      tw = w.p;
+    }
+    AIRT_LAUNCH_CHECK();
+    AIRT_CHECK_CUDA(cudaMemsetAsync(red.p, 0, 2 * sizeof(double), s));
+    k_dot2<<<gn, kThreads, 0, s>>>(n, v.p, tw, red.p);  // v'Tv, ||Tv||^2
+    AIRT_LAUNCH_CHECK();
+    double hr[2];
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hr, red.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    theta = hr[0];
+    const double nrm = std::sqrt(std::fmax(hr[1], 0.0));
+    if (!(nrm > 0.0)) break;
+    if (it >= 4 && std::fabs(theta - prev) <= tol * std::fabs(theta)) break;
+    prev = theta;
+    k_scale_by<<<gn, kThreads, 0, s>>>(n, 1.0 / nrm, tw, v.p);
     AIRT_LAUNCH_CHECK();
   }
   return theta;

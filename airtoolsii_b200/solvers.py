@@ -176,43 +176,63 @@ def _relax_sirt(relaxparinput, rho, kmax):
 
 
 def _method_code(sirt_method, m, n):
-    """Built-in name -> code, or a custom struct {M, D} -> diagonal vectors."""
+    """get_mfun_dfun.m dispatch: (code, M, D, name, M_full, D_full).  A custom
+    struct's M and D become diagonals when they are vectors or diagonal
+    matrices (Mflag/Dflag 1, get_mfun_dfun.m:256-271) and stay full
+    column-major matrices otherwise (flag 2, applied as dense products on the
+    device)."""
     if sirt_method is None:
         sirt_method = "sart"
     if isinstance(sirt_method, str):
         if sirt_method not in _lib.METHODS:
             raise ValueError("SIRT method not defined.")
-        return _lib.METHODS[sirt_method], None, None, sirt_method
+        return _lib.METHODS[sirt_method], None, None, sirt_method, False, False
     if isinstance(sirt_method, dict):
-        out = []
+        out, full = [], []
         for key, size in (("M", m), ("D", n)):
             W = sirt_method.get(key)
             if W is None or np.size(W) == 0:
                 out.append(None)
+                full.append(False)
                 continue
             if sp.issparse(W):
                 W = sp.csr_matrix(W, dtype=np.float64)
-                dg = W.diagonal()
                 if min(W.shape) == 1:
                     W = W.toarray()
-                elif (W - sp.diags(dg, shape=W.shape)).count_nonzero() == 0:
-                    W = np.ascontiguousarray(dg)
+                elif (W - sp.diags(W.diagonal(), shape=W.shape)).count_nonzero() == 0:
+                    W = np.ascontiguousarray(W.diagonal())
                 else:
-                    raise NotImplementedError(
-                        "non-diagonal custom M/D are not supported on the GPU path")
+                    W = W.toarray()
+            if not np.issubdtype(np.asarray(W).dtype, np.number):
+                raise ValueError(f"{key} must be given as an array, either of dimension 0, 1 or 2.")
             W = np.asarray(W, dtype=np.float64)
-            if W.ndim == 1 or min(W.shape) == 1:
-                v = W.ravel()
+            if W.ndim > 2:
+                raise ValueError(f"{key} must be given as an array, either of dimension 0, 1 or 2.")
+            if W.ndim <= 1 or min(W.shape) == 1:
+                v, f = W.ravel(), False
             elif np.count_nonzero(W - np.diag(np.diag(W))) == 0:
-                v = np.diag(W).copy()
+                v, f = np.diag(W).copy(), False
             else:
-                raise NotImplementedError("non-diagonal custom M/D are not supported on the GPU path")
-            if v.size != size:
+                if W.shape != (size, size):
+                    raise ValueError(f"custom {key} has the wrong size")
+                v, f = np.asfortranarray(W), True
+            if not f and v.size != size:
                 raise ValueError(f"custom {key} has the wrong size")
-            out.append(np.ascontiguousarray(v))
-        return _lib.AIRT_CUSTOM, out[0], out[1], "custom"
+            out.append(v if f else np.ascontiguousarray(v))
+            full.append(f)
+        return _lib.AIRT_CUSTOM, out[0], out[1], "custom", full[0], full[1]
     raise ValueError("First input must be a string with the SIRT method name or a struct "
                      "with fields M and D characterizing a custom method.")
+
+
+def _fptr(a):
+    """Pointer to a 1-D array or to a Fortran-ordered (column-major) matrix."""
+    if a is None:
+        return None
+    if a.ndim == 2:
+        assert a.flags.f_contiguous and a.dtype == np.float64
+        return a.ctypes.data_as(_lib._dp)
+    return dptr(a)
 
 
 def _print_verbose(verbose, kmax, resn, lams, total_s, k_final):
@@ -234,7 +254,7 @@ def sirt(sirt_method, A, b, K, x0=None, options=None):
     c = _parse(A, b, K, x0, options, "sirt")
     op: AirtOperator = c["op"]
     m, n, K, kmax = c["m"], c["n"], c["K"], c["kmax"]
-    code, Mv, Dv, name = _method_code(sirt_method, m, n)
+    code, Mv, Dv, name, Mfull, Dfull = _method_code(sirt_method, m, n)
     opts = c["options"]
     rho = opts.get("rho", float("nan"))
     rho = float("nan") if rho is None else float(rho)
@@ -242,13 +262,18 @@ def sirt(sirt_method, A, b, K, x0=None, options=None):
         rho = 1.0                                   # sirt.m:166-168
     if math.isnan(rho):
         r = C.c_double()
-        check(lib().airt_rho(op.handle, code, dptr(Mv), dptr(Dv), 1e-7, 200, C.byref(r)))
+        if Mfull or Dfull:
+            check(lib().airt_rho_custom(op.handle, _fptr(Mv), int(Mfull), _fptr(Dv), int(Dfull),
+                                        1e-7, 1000, C.byref(r)))
+        else:
+            check(lib().airt_rho(op.handle, code, dptr(Mv), dptr(Dv), 1e-7, 200, C.byref(r)))
         rho = float(r.value)
     kind, lam, table = _relax_sirt(opts.get("relaxpar"), rho, kmax)
 
     o = SirtOpts()
     o.method = code
-    o.M, o.D = dptr(Mv), dptr(Dv)
+    o.M, o.D = _fptr(Mv), _fptr(Dv)
+    o.M_full, o.D_full = int(Mfull), int(Dfull)
     o.relax_kind, o.relaxpar = kind, (lam if kind == _lib.RELAX_CONST else 0.0)
     o.relax_table = dptr(table)
     o.stoprule = _lib.STOP[c["stype"]]

@@ -23,6 +23,7 @@
  *                             testprobs/paralleltomo.m:146-177,280-288
  *   airt_weights           -> auxil/get_mfun_dfun.m:43-250
  *   airt_rho               -> auxil/calc_relaxpar.m:91-103 (eigs of D*A'*M*A)
+ *   airt_rho_custom        -> the same, custom weights of get_mfun_dfun.m:252-307
  *   airt_sirt              -> sirt/sirt.m:147-261 with auxil/check_stoprules.m:54-94,153-161
  *   airt_cart              -> cart/cart.m:139-320 (cart/columnaction.m)
  *   airt_fbp               -> auxil/fbp.m:40-79
@@ -88,6 +89,10 @@ typedef struct {
        the residual is reshaped column-major to ncp_rows x ncp_cols (ncp_cols = 1
        for a 1D res_dims) and ncp_smooth values are compared.                    */
     int ncp_rows, ncp_cols, ncp_smooth;
+    /* AIRT_CUSTOM only: M (D) points to a full column-major m x m (n x n)
+       matrix instead of a diagonal, the Mflag/Dflag = 2 case of
+       auxil/get_mfun_dfun.m:252-307 (M*r and D*g are dense products).      */
+    int M_full, D_full;
 } airt_sirt_opts;
 
 typedef struct {
@@ -206,6 +211,15 @@ int airt_weights(airt_problem *h, int method, double *M, double *D);
  * operator applications). */
 int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *Dcustom,
              double tol, int maxit, double *rho);
+/* rho for a custom method whose M and/or D may be full matrices (M_full /
+ * D_full as in airt_sirt_opts; a NULL M or D is the identity): the
+ * dominant eigenvalue of D*A'*M*A by a power iteration on that operator
+ * (the general operator of calc_relaxpar.m:91-103's eigs; the symmetric
+ * Lanczos form of airt_rho needs diagonal weights), stopped when the
+ * Rayleigh quotient changes by at most tol (relative) after at least five
+ * steps, or after maxit steps. */
+int airt_rho_custom(airt_problem *h, const double *M, int M_full, const double *D, int D_full,
+                    double tol, int maxit, double *rho);
 
 /* ---- solvers ---------------------------------------------------------------- */
 /* SIRT loop.  K: nK strictly increasing 1-based iteration numbers (K(end) =
