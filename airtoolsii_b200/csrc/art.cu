@@ -10,6 +10,16 @@
 // separates levels.  Each pixel therefore sees the same update sequence, and
 // each dot product reads the same values, as in the sequential sweep.
 //
+// The sweep runs as one cooperative launch over all SMs with one warp per
+// step: the steps, sorted by level, are dealt round-robin to every warp of
+// the grid, and a step waits only for its predecessors -- the last earlier
+// step that touched each of its pixels -- through per-step completion
+// stamps in global memory (release store after the step's x writes, acquire
+// loads before its gathers).  The chain of levels is the critical path; no
+// grid-wide barrier separates levels.  Each wait is bounded: on expiry the
+// kernel raises an error flag, every warp leaves, and the host reports
+// AIRT_ERR_TIMEOUT.
+//
 // The whole-vector box projection after every row (art.m:279-284) is
 // equivalent to clamping x0 once right after the first row step and the
 // row's support after every later step: once x is feasible only the updated
@@ -48,55 +58,103 @@ __device__ __forceinline__ double clampv(double v, int64_t j, const KaczArgs &a)
   return v;
 }
 
-// Entries per lane whose gathered x is kept in registers across a row step:
-// for rows of up to 32 * kKaczCache entries the update reuses the value of x
-// the dot product read (the column indices and values it re-reads are in L1).
-constexpr int kKaczCache = 8;
+// Test hook: a cycle budget for the bounded waits of the sweep kernel and
+// an injected stall (the first step waits for a stamp that no step writes),
+// so that a test can make a wait run out.  Defaults: ~2 s, no stall.
+long long g_kacz_wait_budget = 4000000000ll;
+int g_kacz_inject_stall = 0;
 
-__global__ void __launch_bounds__(1024)
-    k_kacz_levels(int nlev, const int *__restrict__ lev_ptr, const int *__restrict__ steps,
-                  const int *__restrict__ step_pos, KaczArgs a) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+constexpr int kDagCache = 16;  // entries per lane kept in registers (rows <= 512)
+constexpr int kDagThreads = 256;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// One Kaczmarz sweep in the level-sorted step order: warp w of the grid
+// (consecutive warps on different SMs) runs steps w, w+W, w+2W, ... ; step q
+// waits until done[pred] >= stamp for each of its predecessors
+// preds[pred_ptr[q] .. pred_ptr[q+1]) (indices into the same order), then
+// computes exactly what the sequential sweep computes for its row and
+// publishes done[q] = stamp.  The row's indices, values, b and the norm are
+// loaded before the wait; x is read through L2 (other SMs wrote it).
+__global__ void __launch_bounds__(kDagThreads, 1)
+    k_kacz_dag(int nsteps, const int *__restrict__ steps, const int *__restrict__ step_pos,
+               const int *__restrict__ pred_ptr, const int *__restrict__ preds, unsigned stamp,
+               unsigned *__restrict__ done, int *__restrict__ err, long long budget, int stall,
+               KaczArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int W = gridDim.x * (blockDim.x >> 5);
+  const int w = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
   const bool clamp = a.lbk != AIRT_BOUND_NONE || a.ubk != AIRT_BOUND_NONE;
-  for (int L = 0; L < nlev; ++L) {
-    const int q1 = lev_ptr[L + 1];
-    for (int q = lev_ptr[L] + warp; q < q1; q += nw) {
-      const int row = steps[q];
-      const int64_t s0 = a.rp[row], s1 = a.rp[row + 1];
-      const int64_t e0 = s0 + lane;
-      // the gathers of the cached part are all issued before the first FMA;
-      // the FMAs run in the order of the plain strided loop
-      double cx[kKaczCache];
+  for (int q = w; q < nsteps; q += W) {
+    const int row = __ldg(steps + q);
+    const int64_t s0 = __ldg(a.rp + row), s1 = __ldg(a.rp + row + 1);
+    const int64_t e0 = s0 + lane;
+    int cj[kDagCache];
+    float cv[kDagCache];
 #pragma unroll
-      for (int u = 0; u < kKaczCache; ++u)
-        cx[u] = e0 + 32 * u < s1 ? a.x[a.ci[e0 + 32 * u]] : 0.0;
-      double acc = 0.0;
-#pragma unroll
-      for (int u = 0; u < kKaczCache; ++u)
-        if (e0 + 32 * u < s1) acc = fma((double)a.rv[e0 + 32 * u], cx[u], acc);
-      for (int64_t e = e0 + 32 * kKaczCache; e < s1; e += 32)
-        acc = fma((double)a.rv[e], a.x[a.ci[e]], acc);
-      acc = warp_sum(acc);
-      const double lam = a.lam_tab ? a.lam_tab[step_pos[q]] : a.lam;
-      const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(a.b[row], acc)), a.nrm[row]);
-      // no other step of this level touches these pixels, so the gathered x
-      // is still the current value
-#pragma unroll
-      for (int u = 0; u < kKaczCache; ++u)
-        if (e0 + 32 * u < s1) {
-          const int j = a.ci[e0 + 32 * u];
-          double v = __dadd_rn(cx[u], __dmul_rn(c, (double)a.rv[e0 + 32 * u]));
-          if (clamp) v = clampv(v, j, a);
-          a.x[j] = v;
+    for (int u = 0; u < kDagCache; ++u) {
+      const int64_t e = e0 + 32 * u;
+      cj[u] = e < s1 ? __ldg(a.ci + e) : -1;
+      cv[u] = e < s1 ? __ldg(a.rv + e) : 0.f;
+    }
+    const double bi = __ldg(a.b + row), ni = __ldg(a.nrm + row);
+    const double lam = a.lam_tab ? __ldg(a.lam_tab + __ldg(step_pos + q)) : a.lam;
+    // wait for the predecessors (each lane polls its share of them)
+    const int p0 = __ldg(pred_ptr + q), p1 = __ldg(pred_ptr + q + 1);
+    bool ok = true;
+    const long long t0 = clock64();
+    for (int pi = p0 + lane; ok && pi < p1 + (stall && q == 0 ? 1 : 0); pi += 32) {
+      const unsigned *f = pi < p1 ? done + __ldg(preds + pi) : done + q;  // stall: own stamp
+      const unsigned want = pi < p1 ? stamp : stamp + 1u;
+      while (ld_acquire_u32(f) < want) {
+        if (*(volatile int *)err) {
+          ok = false;
+          break;
         }
-      for (int64_t e = e0 + 32 * kKaczCache; e < s1; e += 32) {
-        const int j = a.ci[e];
-        double v = __dadd_rn(a.x[j], __dmul_rn(c, (double)a.rv[e]));
-        if (clamp) v = clampv(v, j, a);
-        a.x[j] = v;
+        if (clock64() - t0 > budget) {
+          atomicExch(err, 1);
+          ok = false;
+          break;
+        }
       }
     }
-    __syncthreads();
+    if (!__all_sync(0xffffffffu, ok)) return;
+    // gathers (through L2) and the dot product in the order of the plain
+    // strided loop
+    double cx[kDagCache];
+#pragma unroll
+    for (int u = 0; u < kDagCache; ++u) cx[u] = cj[u] >= 0 ? __ldcg(a.x + cj[u]) : 0.0;
+    double acc = 0.0;
+#pragma unroll
+    for (int u = 0; u < kDagCache; ++u)
+      if (cj[u] >= 0) acc = fma((double)cv[u], cx[u], acc);
+    for (int64_t e = e0 + 32 * kDagCache; e < s1; e += 32)
+      acc = fma((double)__ldg(a.rv + e), __ldcg(a.x + __ldg(a.ci + e)), acc);
+    acc = warp_sum(acc);
+    const double c = __ddiv_rn(__dmul_rn(lam, __dsub_rn(bi, acc)), ni);
+#pragma unroll
+    for (int u = 0; u < kDagCache; ++u)
+      if (cj[u] >= 0) {
+        double v = __dadd_rn(cx[u], __dmul_rn(c, (double)cv[u]));
+        if (clamp) v = clampv(v, cj[u], a);
+        __stcg(a.x + cj[u], v);
+      }
+    for (int64_t e = e0 + 32 * kDagCache; e < s1; e += 32) {
+      const int j = __ldg(a.ci + e);
+      double v = __dadd_rn(__ldcg(a.x + j), __dmul_rn(c, (double)__ldg(a.rv + e)));
+      if (clamp) v = clampv(v, j, a);
+      __stcg(a.x + j, v);
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release_u32(done + q, stamp);
   }
 }
 
@@ -154,36 +212,62 @@ __global__ void k_copy_d(int64_t n, const double *__restrict__ a, double *__rest
 
 struct Schedule {
   int nlev = 0;
-  DevBuf<int> lev_ptr, steps, pos;
+  int64_t nsteps = 0;
+  DevBuf<int> steps, pos, pred_ptr, preds;
 };
 
-// Level schedule of a row order (see the file comment).
+// Level schedule of a row order (see the file comment): steps sorted by
+// level (stable), each with the distinct last earlier writers of its pixels
+// as predecessors, given as indices into the sorted order.
 void build_schedule(const std::vector<int64_t> &hrp, const std::vector<int> &hci,
                     const int64_t *order, int64_t nsteps, int64_t n, Schedule &S,
                     cudaStream_t s) {
-  std::vector<int> level(nsteps), last(n, -1);
+  std::vector<int> level(nsteps), last(n, -1), seen(nsteps, -1);
+  std::vector<int64_t> tptr(nsteps + 1, 0);
+  std::vector<int> tpred;
   int maxlev = -1;
   for (int64_t t = 0; t < nsteps; ++t) {
     const int64_t row = order[t];
     int L = 0;
-    for (int64_t e = hrp[row]; e < hrp[row + 1]; ++e) L = std::max(L, last[hci[e]] + 1);
+    for (int64_t e = hrp[row]; e < hrp[row + 1]; ++e) {
+      const int w = last[hci[e]];
+      if (w >= 0 && seen[w] != (int)t) {
+        seen[w] = (int)t;
+        tpred.push_back(w);
+        L = std::max(L, level[w] + 1);
+      }
+    }
+    tptr[t + 1] = (int64_t)tpred.size();
     level[t] = L;
-    for (int64_t e = hrp[row]; e < hrp[row + 1]; ++e) last[hci[e]] = L;
+    for (int64_t e = hrp[row]; e < hrp[row + 1]; ++e) last[hci[e]] = (int)t;
     maxlev = std::max(maxlev, L);
   }
   S.nlev = maxlev + 1;
-  std::vector<int> ptr(S.nlev + 1, 0), steps(nsteps), pos(nsteps);
+  S.nsteps = nsteps;
+  std::vector<int> ptr(S.nlev + 1, 0), steps(nsteps), pos(nsteps), qof(nsteps);
   for (int64_t t = 0; t < nsteps; ++t) ++ptr[level[t] + 1];
   for (int L = 0; L < S.nlev; ++L) ptr[L + 1] += ptr[L];
-  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
   for (int64_t t = 0; t < nsteps; ++t) {
-    const int q = fill[level[t]]++;
+    const int q = ptr[level[t]]++;
     steps[q] = (int)order[t];
     pos[q] = (int)t;
+    qof[t] = q;
   }
-  S.lev_ptr.upload(ptr.data(), ptr.size(), s);
+  std::vector<int> pptr(nsteps + 1, 0), preds(tpred.size());
+  for (int64_t q = 0; q < nsteps; ++q) {
+    const int t = pos[q];
+    pptr[q + 1] = pptr[q] + (int)(tptr[t + 1] - tptr[t]);
+  }
+  for (int64_t q = 0; q < nsteps; ++q) {
+    const int t = pos[q];
+    int o = pptr[q];
+    for (int64_t k = tptr[t]; k < tptr[t + 1]; ++k) preds[o++] = qof[tpred[k]];
+  }
   S.steps.upload(steps.data(), nsteps, s);
   S.pos.upload(pos.data(), nsteps, s);
+  S.pred_ptr.upload(pptr.data(), nsteps + 1, s);
+  if (preds.empty()) S.preds.ensure(1);
+  else S.preds.upload(preds.data(), preds.size(), s);
 }
 
 }  // namespace
@@ -278,6 +362,19 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
     AIRT_CHECK_CUDA(cudaMemsetAsync(P.x64.p, 0, n * sizeof(double), s));
   if (o.lb_kind == AIRT_BOUND_VECTOR) P.lbv.upload(o.lbv, n, s);
   if (o.ub_kind == AIRT_BOUND_VECTOR) P.ubv.upload(o.ubv, n, s);
+  // sweep kernel: completion stamps of the steps, error flag, grid size
+  DevBuf<unsigned> done;
+  done.ensure(std::max<int64_t>(per_sweep, 1));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(done.p, 0, std::max<int64_t>(per_sweep, 1) * sizeof(unsigned), s));
+  P.err.ensure(1);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.err.p, 0, sizeof(int), s));
+  int occ = 0;
+  AIRT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_kacz_dag, kDagThreads, 0));
+  AIRT_REQUIRE(occ >= 1, "the Kaczmarz sweep kernel cannot be resident");
+  const int dag_grid = num_sms();
+  const long long budget = g_kacz_wait_budget;
+  const int stall = g_kacz_inject_stall;
+  int herr = 0;
   DevBuf<double> tab, red, keep;
   if (o.relax_table && kmax > 0) tab.upload(o.relax_table, kmax * per_sweep, s);
   red.ensure(1);
@@ -356,10 +453,24 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
       k_preclamp<<<1, 1024, 0, s>>>(n, (int)r0, keep.p, a);
     }
     a.lam_tab = tab.p ? tab.p + (k - 1) * per_sweep : nullptr;
-    if (S.nlev > 0) k_kacz_levels<<<1, 1024, 0, s>>>(S.nlev, S.lev_ptr.p, S.steps.p, S.pos.p, a);
+    if (S.nsteps > 0) {
+      int nsteps = (int)S.nsteps;
+      unsigned stamp = (unsigned)k;
+      void *args[] = {&nsteps, &S.steps.p, &S.pos.p, &S.pred_ptr.p, &S.preds.p, &stamp,
+                      &done.p, &P.err.p, (void *)&budget, (void *)&stall, &a};
+      AIRT_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *)k_kacz_dag, dim3(dag_grid),
+                                                  dim3(kDagThreads), args, 0, s));
+    }
     AIRT_LAUNCH_CHECK();
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(&herr, P.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (o.relax_table && per_sweep > 0) lam_last = o.relax_table[(k - 1) * per_sweep + per_sweep - 1];
-    const double nrk = resid();
+    const double nrk = resid();  // synchronises the stream (herr is current)
+    if (herr) {
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      set_error("a bounded device wait of the Kaczmarz sweep gave up (sweep %lld)", (long long)k);
+      throw Status{AIRT_ERR_TIMEOUT};
+    }
     resn.push_back(nrk);
     st.judge(k, nrk, ncc);
     if ((l < nK && k == K[l]) || st.stop) {
@@ -385,3 +496,14 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
 }
 
 }  // namespace airt
+
+extern "C" int airt_test_set_wait_budget(long long cycles) {
+  if (cycles <= 0) return AIRT_ERR_ARG;
+  airt::g_kacz_wait_budget = cycles;
+  return AIRT_OK;
+}
+
+extern "C" int airt_test_inject_stall(int on) {
+  airt::g_kacz_inject_stall = on ? 1 : 0;
+  return AIRT_OK;
+}

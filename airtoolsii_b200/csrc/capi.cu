@@ -96,6 +96,10 @@ static void free_problem(Problem *P) {
 
 using namespace airt;
 
+namespace airt {
+int g_alloc_fail_countdown = -1;
+}
+
 #define AIRT_API_BEGIN try {
 #define AIRT_API_END                                   \
   }                                                    \
@@ -665,3 +669,8 @@ int airt_profile_read(airt_problem *h, int which, int64_t *launches, double *tot
 }
 
 }  // extern "C"
+
+extern "C" int airt_test_fail_alloc(int after) {
+  airt::g_alloc_fail_countdown = after < 0 ? -1 : after;
+  return AIRT_OK;
+}

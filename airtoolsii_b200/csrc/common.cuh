@@ -43,6 +43,11 @@ void set_error(const char *fmt, ...);
 #define AIRT_LAUNCH_CHECK() AIRT_CHECK_CUDA(cudaGetLastError())
 
 // ---------------------------------------------------------------- buffers
+// Test hook (airt_test_fail_alloc): < 0 off; otherwise the number of device
+// allocations through DevBuf that still succeed before one fails as if the
+// device were out of memory.
+extern int g_alloc_fail_countdown;
+
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
@@ -75,6 +80,10 @@ struct DevBuf {
     if (count <= n && p) return;
     release();
     size_t bytes = (count ? count : 1) * sizeof(T);
+    if (g_alloc_fail_countdown >= 0 && g_alloc_fail_countdown-- == 0) {
+      set_error("cudaMalloc of %zu bytes failed: injected allocation failure (test hook)", bytes);
+      throw Status{AIRT_ERR_OOM};
+    }
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
       p = nullptr;

@@ -352,6 +352,20 @@ int airt_residual_noalloc(int64_t m, int64_t n, const int64_t *d_rp, const int *
                           const float *d_rv, const double *d_x, const double *d_b, double *d_r,
                           double *d_resnorm, void *cuda_stream);
 
+/* ---- test hooks ----------------------------------------------------------- */
+/* No counterpart in the reference.  For tests of the bounded device waits:
+ * airt_test_set_wait_budget sets the clock64 cycle budget of each wait of the
+ * Kaczmarz sweep kernel (default 4e9, about 2 s); airt_test_inject_stall(1)
+ * makes the first step of every sweep wait for a completion stamp that no
+ * step writes, so the wait runs out, the kernel leaves and airt_art returns
+ * AIRT_ERR_TIMEOUT.  Process-wide; not for production use. */
+int airt_test_set_wait_budget(long long cycles);
+int airt_test_inject_stall(int on);
+/* airt_test_fail_alloc(k), k >= 0: the next k device allocations of the
+ * library succeed and the one after fails as an out-of-memory error
+ * (AIRT_ERR_OOM, message "injected allocation failure"); k < 0 turns it off. */
+int airt_test_fail_alloc(int after);
+
 /* ---- instrumentation ------------------------------------------------------- */
 /* When on, each SIRT kernel launch is bracketed by CUDA events on the problem
  * stream; airt_profile_read returns launches and summed device milliseconds
