@@ -203,6 +203,7 @@ def extra_legs(A_c2, b_c2, wl):
         "gpu_ms": round(info["gpu_ms"], 2), "rays_per_s": round(2 * Af.m * it / (info["gpu_ms"] / 1e3), 0),
         "relerr": round(float(np.linalg.norm(X[:, -1] - xf) / np.linalg.norm(xf)), 5)}
     del Af
+    out["c3_fan_sart_dp"]["cpu_baseline"] = _cpu_fan_sart()
     # C3 ART
     Aa, *_ = airt.paralleltomo(256, np.arange(180.0))
     xa = airt.random_ellipses(256, 10, seed=31)
@@ -214,6 +215,7 @@ def extra_legs(A_c2, b_c2, wl):
         ms = info["gpu_ms"] / 20
         art[meth] = {"sweeps": 20, "ms_per_sweep": round(ms, 4),
                      "GBps_model": round((8 * Aa.nnz + 16 * Aa.m) / (ms / 1e3) / 1e9, 1)}
+    art["cpu_baseline"] = _cpu_kaczmarz(Aa, ba)
     out["c3_art_n256"] = art
     del Aa
     # C4 batch
@@ -251,9 +253,76 @@ def extra_legs(A_c2, b_c2, wl):
                     "GBps_model": round(byts / (info["gpu_ms"] / 1e3) / 1e9, 1)}
     _, ik = B.kaczmarz(np.concatenate(bs), 5)
     c4["kaczmarz_5_sweeps_ms"] = round(ik["gpu_ms"], 2)
+    c4["cpu_baseline"] = _cpu_batch_sample(B, Ns, nAs, bs, tds, B.rho("cimmino"))
     out["c4_batch"] = c4
     out["widened"] = widened_legs(A_c2, b_c2, wl)
     return out
+
+
+def _cpu_kaczmarz(A, b):
+    """One kaczmarz sweep (art.m row order, lbound 0) of the FP64 C oracle on
+    the same matrix and b, one thread (the sweep is sequential)."""
+    from oracle import cbind
+    R = A.to_scipy().tocsr()
+    nrm = np.asarray(R.multiply(R).sum(axis=1)).ravel()
+    order = np.flatnonzero(nrm > 0)
+    cbind.kaczmarz(R, b, nrm, order[:100], 1.0, 0.0, None, 1)
+    t0 = time.perf_counter()
+    cbind.kaczmarz(R, b, nrm, order, 1.0, 0.0, None, 1)
+    dt = time.perf_counter() - t0
+    return {"ms_per_sweep": round(1e3 * dt, 2), "cores": 1, "kind": "port",
+            "sample": "1 kaczmarz sweep of the same problem, FP64 C restatement"}
+
+
+def _cpu_fan_sart():
+    """SART iterations of the FP64 C oracle on the fan geometry restricted to
+    36 of the 720 angles (the full matrix, ~8e8 nonzeros, is not formed on
+    the host): matrix from the C tracer, 3 iterations timed; rays/s counts
+    the 2m rays of an iteration, as the GPU figure does."""
+    from oracle import airt_oracle as O
+    from oracle import cbind
+    theta = (np.arange(720) * 0.5)[::20]
+    th, p, R, _, _, ct, st, cw, sw = O.fan_geometry(1024, theta, 1448, 2.0)
+    rows, cols, vals = cbind.trace_coo(1024, list(O.fan_rays(1024, R, ct, st, cw, sw)), False)
+    Rm = O.coo_to_csc(rows, cols, vals, len(th) * p, 1024 * 1024)
+    del rows, cols, vals
+    x = O.random_ellipses(1024, 10, seed=300)
+    b, _ = O.add_noise(Rm @ x, 0.01, seed=301)
+    M, D, _, _ = O.get_mfun_dfun("sart", Rm)
+    prep = cbind.PreparedSirt(Rm, b, M, D)
+    prep.run(1.9, None, None, 1)
+    t0 = time.perf_counter()
+    prep.run(1.9, None, None, 3)
+    dt = (time.perf_counter() - t0) / 3
+    return {"rays_per_s": round(2 * Rm.shape[0] / dt, 0), "ms_per_iteration": round(1e3 * dt, 2),
+            "cores": cbind.num_threads(), "kind": "port",
+            "sample": "3 SART iterations on 36 of the 720 angles (stored FP64 matrix, C "
+                      "restatement, OpenMP)"}
+
+
+def _cpu_batch_sample(B, Ns, nAs, bs, tds, rho):
+    """cimmino to the DP stop with the FP64 C oracle on the first 8 instances
+    of the batch, one after the other (all host threads each): GB/s by the
+    same CSR+CSC byte model and iteration counts as the GPU figure."""
+    from oracle import airt_oracle as O
+    from oracle import cbind
+    nbytes, dt, its = 0.0, 0.0, []
+    for k in range(8):
+        N = int(Ns[k])
+        th, p, d, ct, st, off = O.parallel_geometry(N, np.arange(nAs[k]) * (180.0 / nAs[k]), None)
+        rows, cols, vals = cbind.trace_coo(N, list(O.parallel_rays(N, ct, st, off)), True)
+        A = O.coo_to_csc(rows, cols, vals, len(th) * p, N * N)
+        M, D, _, _ = O.get_mfun_dfun("cimmino", A)
+        prep = cbind.PreparedSirt(A, bs[k], M, D)
+        t0 = time.perf_counter()
+        _, it, _ = prep.run(1.9 / rho[k], 0.0, None, 2000, taudelta=tds[k])
+        dt += time.perf_counter() - t0
+        its.append(it)
+        nbytes += it * (16 * A.nnz + 16 * A.shape[0] + 16 * A.shape[1])
+    return {"GBps_model": round(nbytes / dt / 1e9, 2), "s_for_8": round(dt, 3),
+            "iters": its, "cores": cbind.num_threads(), "kind": "port",
+            "sample": "cimmino to the DP stop on instances 0-7 of the batch, FP64 C "
+                      "restatement (OpenMP), iterations only"}
 
 
 def widened_legs(A_c2, b_c2, wl):
@@ -529,12 +598,12 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     ach = (fb if dom == 0 else bb) / (avg[dom] / 1e3) / 1e9
-    traffic = None
+    traffic, traffic_src = None, None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
         key = "sirt_fwd" if dom == 0 else "sirt_bwd"
-        if key in prof and not a.small:
-            traffic = prof[key]
+        if key in prof and not (a.small or a.tiny):
+            traffic, traffic_src = prof[key], prof.get("note")
     except Exception:
         pass
     launches_per_step = 3 + 1 + 2 + 3 * it   # weights (3), x copy, initial fwd+ctrl, 3/iteration
@@ -552,6 +621,7 @@ def main():
                                                     "k_sirt_bwd (CSC transpose SpMV + update)"][dom],
                          "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 4), "traffic": traffic,
+                         "traffic_source": traffic_src,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks
                          else "fallback 6650 GB/s (of fallback)",
                          "algorithmic_bytes_per_launch": fb if dom == 0 else bb,
