@@ -38,16 +38,15 @@ __global__ void __launch_bounds__(256) k_ncp_power(int L, int q, const double *_
   pk[(int64_t)j * q + (f - 1)] = re * re + im * im;
 }
 
-// NCP part 2: per column, c = cumsum(pk)/sum(pk) and the distance
-// sqrt(sum((c - (1:q)/q).^2)) to the white-noise line.  256 threads own
-// contiguous chunks of the q values; chunk sums meet in a block scan.
-__global__ void __launch_bounds__(256) k_ncp_col(int q, const double *__restrict__ pk,
-                                                 double *__restrict__ ncc_col, const int *stop_flag) {
-  if (stop_flag && *(volatile const int *)stop_flag) return;
+// NCP part 2 for one column (the calling block): c = cumsum(pk)/sum(pk) of
+// the q periodogram values p[0..q) and the distance
+// sqrt(sum((c - (1:q)/q).^2)) to the white-noise line, returned on thread 0.
+// 256 threads own contiguous chunks of the q values; chunk sums meet in a
+// block scan.
+__device__ __forceinline__ double ncp_distance(int q, const double *__restrict__ p) {
   __shared__ double sh[256];
   __shared__ double tot_sh;
-  const int t = threadIdx.x, j = blockIdx.x;
-  const double *p = pk + (int64_t)j * q;
+  const int t = threadIdx.x;
   const int per = (q + 255) / 256, f0 = min(q, t * per), f1 = min(q, f0 + per);
   double loc = 0.0;
   for (int f = f0; f < f1; ++f) loc += p[f];
@@ -71,7 +70,16 @@ __global__ void __launch_bounds__(256) k_ncp_col(int q, const double *__restrict
     acc += d * d;
   }
   acc = block_sum<256>(acc);
-  if (t == 0) ncc_col[j] = sqrt(acc);
+  return sqrt(acc);
+}
+
+// NCP part 2: the distance of every column (block j = column j).
+__global__ void __launch_bounds__(256) k_ncp_col(int q, const double *__restrict__ pk,
+                                                 double *__restrict__ ncc_col, const int *stop_flag) {
+  if (stop_flag && *(volatile const int *)stop_flag) return;
+  const int j = blockIdx.x;
+  const double d = ncp_distance(q, pk + (int64_t)j * q);
+  if (threadIdx.x == 0) ncc_col[j] = d;
 }
 
 }  // namespace
