@@ -112,6 +112,9 @@ SIGNATURES = {
     "airt_batch_sirt_device": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_void_p, _dp, C.c_int64,
                                          C.c_int, C.c_double, C.c_int, C.c_double, C.c_void_p,
                                          C.c_void_p, _i64p, C.POINTER(C.c_int), _dp]),
+    "airt_batch_sirt_rule": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.c_int, _dp, C.c_int,
+                                       C.c_int64, C.c_int, C.c_double, C.c_int, C.c_double, _dp,
+                                       _dp, _i64p, C.POINTER(C.c_int), _dp]),
     "airt_batch_nnz": (C.c_int, [C.c_void_p, _i64p]),
     "airt_batch_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "airt_batch_backproject": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _dp]),

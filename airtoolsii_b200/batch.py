@@ -36,6 +36,10 @@ def _batch_signatures():
         "airt_batch_sirt_device": (C.c_int, [C.c_void_p, C.c_int, _lib._dp, C.c_void_p, _lib._dp,
                                              C.c_int64, C.c_int, C.c_double, C.c_int, C.c_double,
                                              C.c_void_p, C.c_void_p, i64p, _ip, _lib._dp]),
+        "airt_batch_sirt_rule": (C.c_int, [C.c_void_p, C.c_int, _lib._dp, _lib._dp, C.c_int,
+                                           _lib._dp, C.c_int, C.c_int64, C.c_int, C.c_double,
+                                           C.c_int, C.c_double, _lib._dp, _lib._dp, i64p, _ip,
+                                           _lib._dp]),
         "airt_batch_nnz": (C.c_int, [C.c_void_p, i64p]),
         "airt_batch_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
         "airt_batch_backproject": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, _lib._dp]),
@@ -123,9 +127,12 @@ class ParallelBatch:
         return out
 
     def sirt(self, method, b, kmax, taudelta=None, relaxpar=None, rho=None, lbound=None,
-             ubound=None, x0=None):
+             ubound=None, x0=None, stoprule=None, ncp_smooth=2):
         """SIRT on every instance; b is the concatenation of the instances'
-        right-hand sides (or a list of them).  Returns (x_list, info) with
+        right-hand sides (or a list of them).  stoprule: 'DP' (default when
+        taudelta is given), 'ME', 'NCP' (each instance's residual as its
+        p x nA projections, ncp_smooth values) or 'NONE', applied per
+        instance (check_stoprules.m).  Returns (x_list, info) with
         per-instance finaliter, stoprule, rho and relaxpar."""
         b = np.ascontiguousarray(np.concatenate(b) if isinstance(b, (list, tuple)) else b,
                                  dtype=np.float64)
@@ -150,9 +157,15 @@ class ParallelBatch:
         ms = C.c_double()
         lk, lv = _bounds(lbound)
         uk, uv = _bounds(ubound)
-        check(self._L.airt_batch_sirt(self._h, _lib.METHODS[method], dptr(lam), dptr(b), dptr(td),
-                                      int(kmax), lk, lv, uk, uv, dptr(x0v), dptr(x),
-                                      _lib.i64ptr(fin), rule.ctypes.data_as(_ip), C.byref(ms)))
+        rule_name = (stoprule or ("DP" if td is not None else "NONE")).upper()
+        if rule_name not in _lib.STOP:
+            raise ValueError("The chosen stopping rule is not valid.")
+        if rule_name in ("DP", "ME") and td is None:
+            raise ValueError("For stopping rules DP and ME a scalar taudelta must be given in options.")
+        check(self._L.airt_batch_sirt_rule(self._h, _lib.METHODS[method], dptr(lam), dptr(b),
+                                           _lib.STOP[rule_name], dptr(td), int(ncp_smooth),
+                                           int(kmax), lk, lv, uk, uv, dptr(x0v), dptr(x),
+                                           _lib.i64ptr(fin), rule.ctypes.data_as(_ip), C.byref(ms)))
         info = {"finaliter": fin, "stoprule": rule, "relaxpar": lam,
                 "rho": None if rho is None else np.asarray(rho), "gpu_ms": float(ms.value)}
         return self.split_cols(x), info

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "ncp.cuh"
 #include "spmv.cuh"
 #include "trace.cuh"
 
@@ -79,6 +80,16 @@ struct Batch {
   // row steps of level L at kz_steps[kz_lev_ptr[base_k + L] ..)
   bool kz_ready = false;
   DevBuf<int> kz_lev_ptr, kz_steps, kz_nlev;
+  // ME / NCP stopping rules per instance: the previous residual and the
+  // per-row products of the ME sums; NCP's projection columns (one per angle
+  // of every instance, length p_k), their twiddle tables per distinct p,
+  // periodograms, distances and the ncp_smooth history per instance
+  DevBuf<double> rprev, pp, ppr, p2, pr;
+  bool ncp_ready = false;
+  int ncols = 0;
+  DevBuf<int64_t> ncp_row0, ncp_tw0, ncp_pk0;
+  DevBuf<int> ncp_L, ncp_inst, ncp_col0;
+  DevBuf<double> ncp_tw, ncp_pk, ncp_ccol, ncp_dk;
 };
 
 namespace {
@@ -178,6 +189,9 @@ struct BFwd {
   double *rsq;
   const int *inst_row, *stop;
   int64_t r0;
+  double *rprev;  // ME / NCP: the residual is kept (previous one read first)
+  double *pp;     // ME: rprev.^2 and rprev.*(rprev + r) per row
+  double *ppr;
 };
 
 template <int L>
@@ -194,6 +208,14 @@ __global__ void __launch_bounds__(256, 4)
         const double ri = o.b[r] - s;
         o.mr32[r] = (float)(o.M[r] * ri);
         o.rsq[r] = ri * ri;
+        if (o.rprev) {
+          if (o.pp) {
+            const double pv = o.rprev[r];
+            o.pp[r] = pv * pv;
+            o.ppr[r] = pv * (pv + ri);
+          }
+          o.rprev[r] = ri;
+        }
       });
 }
 
@@ -257,21 +279,102 @@ __global__ void k_active_tiles(int ntiles, int64_t nseg, const int *__restrict__
     }
 }
 
-// ||r_k||^2 per active instance: one block per instance, fixed order.
+// ||r_k||^2 per active instance: one block per instance, fixed order; with
+// pp (ME) also ||r_(k-1)||^2 and r_(k-1)'(r_(k-1) + r_k).
 __global__ void __launch_bounds__(256) k_batch_reduce(const int64_t *__restrict__ roff,
                                                       const double *__restrict__ rsq,
                                                       const int *__restrict__ stop,
-                                                      double *__restrict__ nrm2) {
+                                                      double *__restrict__ nrm2,
+                                                      const double *__restrict__ pp,
+                                                      const double *__restrict__ ppr,
+                                                      double *__restrict__ p2,
+                                                      double *__restrict__ pr) {
   const int k = blockIdx.x;
   if (stop[k]) return;
-  double a = 0;
-  for (int64_t i = roff[k] + threadIdx.x; i < roff[k + 1]; i += blockDim.x) a += rsq[i];
+  double a = 0, c = 0, d = 0;
+  for (int64_t i = roff[k] + threadIdx.x; i < roff[k + 1]; i += blockDim.x) {
+    a += rsq[i];
+    if (pp) {
+      c += pp[i];
+      d += ppr[i];
+    }
+  }
   a = block_sum<256>(a);
-  if (threadIdx.x == 0) nrm2[k] = a;
+  if (pp) {
+    __syncthreads();
+    c = block_sum<256>(c);
+    __syncthreads();
+    d = block_sum<256>(d);
+  }
+  if (threadIdx.x == 0) {
+    nrm2[k] = a;
+    if (pp) {
+      p2[k] = c;
+      pr[k] = d;
+    }
+  }
 }
 
-// Per-instance rule of check_stoprules.m:56-72 (DP) / 153-161 (NONE).
-__global__ void k_batch_ctrl(int ninst, int initial, int64_t kmax, const double *__restrict__ taud,
+// NCP per instance, part 1: the periodogram of every projection column of
+// the active instances (block = column; frequencies 1..floor(L/2) over the
+// threads), by direct summation with the twiddle table of the column's
+// length, as k_ncp_power does for one problem.
+__global__ void __launch_bounds__(128) k_batch_ncp_power(const int64_t *__restrict__ row0,
+                                                         const int *__restrict__ Ls,
+                                                         const int64_t *__restrict__ tw0,
+                                                         const int64_t *__restrict__ pk0,
+                                                         const int *__restrict__ inst,
+                                                         const int *__restrict__ stop,
+                                                         const double *__restrict__ r,
+                                                         const double *__restrict__ tw,
+                                                         double *__restrict__ pk) {
+  const int j = blockIdx.x;
+  if (stop[inst[j]]) return;
+  const int L = Ls[j], q = L / 2;
+  const double *rc = r + row0[j];
+  const double *t = tw + tw0[j];
+  for (int f = threadIdx.x + 1; f <= q; f += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    int idx = 0;
+    for (int n = 0; n < L; ++n) {
+      const double v = __ldg(rc + n);
+      re = fma(v, __ldg(t + 2 * idx), re);
+      im = fma(v, __ldg(t + 2 * idx + 1), im);
+      idx += f;
+      if (idx >= L) idx -= L;
+    }
+    pk[pk0[j] + (f - 1)] = re * re + im * im;
+  }
+}
+
+// NCP per instance, part 2: every active column's distance to the white-
+// noise cumulative line.
+__global__ void __launch_bounds__(256) k_batch_ncp_col(const int *__restrict__ Ls,
+                                                       const int64_t *__restrict__ pk0,
+                                                       const int *__restrict__ inst,
+                                                       const int *__restrict__ stop,
+                                                       const double *__restrict__ pk,
+                                                       double *__restrict__ ccol) {
+  const int j = blockIdx.x;
+  if (stop[inst[j]]) return;
+  const double d = ncp_distance(Ls[j] / 2, pk + pk0[j]);
+  if (threadIdx.x == 0) ccol[j] = d;
+}
+
+// Per-instance rule of check_stoprules.m: DP (56-72), ME (74-94), NCP
+// (96-151, the residual reshaped to the instance's p x nA projections,
+// history of ncp_smooth values per instance) or NONE (153-161).
+struct BCtrl {
+  int rule;  // AIRT_STOP_*
+  const double *taud;
+  const double *p2, *pr;                 // ME
+  const double *ccol;                    // NCP: distances per column
+  const int *col0;                       // NCP: first column of each instance (ninst + 1)
+  double *dk;                            // NCP: ncp_smooth values per instance
+  int ns;
+};
+
+__global__ void k_batch_ctrl(int ninst, int initial, int64_t kmax, BCtrl c,
                              const double *__restrict__ nrm2, int *__restrict__ stop,
                              int *__restrict__ iters, int *__restrict__ rule,
                              double *__restrict__ resn) {
@@ -281,10 +384,49 @@ __global__ void k_batch_ctrl(int ninst, int initial, int64_t kmax, const double 
     iters[k] = it;
     const double nrk = sqrt(nrm2[k]);
     resn[k] = nrk;
-    const bool dp = taud != nullptr;
-    if ((dp && nrk <= taud[k]) || it >= kmax) {
+    bool st = false;
+    int why = 0;
+    switch (c.rule) {
+      case AIRT_STOP_DP:
+        if (nrk <= c.taud[k] || it >= kmax) {
+          st = true;
+          why = it != kmax ? 2 : 0;
+        }
+        break;
+      case AIRT_STOP_ME: {
+        const double dme = c.pr[k] / 2.0;
+        if (it > 0 && dme / sqrt(c.p2[k]) <= c.taud[k]) {
+          st = true;
+          why = 3;
+        } else if (it >= kmax) {
+          st = true;
+        }
+        break;
+      }
+      case AIRT_STOP_NCP: {
+        double sum = 0.0;
+        const int j0 = c.col0[k], j1 = c.col0[k + 1];
+        for (int j = j0; j < j1; ++j) sum += c.ccol[j];
+        const double ncc = sum / (double)(j1 - j0);
+        double *dk = c.dk + (int64_t)k * c.ns;
+        double mx = -INFINITY, mxn = ncc;
+        for (int i = 0; i < c.ns; ++i) mx = fmax(mx, dk[i]);
+        for (int i = 1; i < c.ns; ++i) mxn = fmax(mxn, dk[i]);
+        if (mx < mxn || it >= kmax) {
+          st = true;
+          why = it != kmax ? 1 : 0;
+        } else {
+          for (int i = 0; i + 1 < c.ns; ++i) dk[i] = dk[i + 1];
+          dk[c.ns - 1] = ncc;
+        }
+        break;
+      }
+      default:
+        st = it >= kmax;
+    }
+    if (st) {
       stop[k] = 1;
-      rule[k] = (dp && it != kmax) ? 2 : 0;
+      rule[k] = why;
     }
   }
 }
@@ -671,14 +813,85 @@ void batch_tune(Batch &B) {
   B.tuned = true;
 }
 
-// SIRT over the whole batch with per-instance relaxpar and DP thresholds.
-void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b, const double *taud_host,
-                int64_t kmax, int lbk, double lb, int ubk, double ub, const double *d_x0, double *d_x,
-                int64_t *finaliter, int *stoprule, double *gpu_ms) {
+namespace {
+// NCP column tables of a batch (built once): one column per projection of
+// every instance (instance k: nA_k columns of p_k rows), twiddles per
+// distinct column length.
+void batch_ncp_setup(Batch &B) {
+  if (B.ncp_ready) return;
+  cudaStream_t s = B.P.stream;
+  const int K = B.ninst;
+  std::vector<int64_t> row0, tw0, pk0;
+  std::vector<int> L, inst, col0(K + 1, 0);
+  std::vector<double> tw;
+  std::vector<std::pair<int, int64_t>> tabs;  // (length, offset) of the twiddle tables
+  int64_t pkoff = 0;
+  for (int k = 0; k < K; ++k) {
+    const InstGeom &g = B.hg[k];
+    AIRT_REQUIRE(g.nA == 0 || g.p >= 2, "NCP: instance %d has fewer than 2 rays per projection", k);
+    int64_t toff = -1;
+    for (auto &t : tabs)
+      if (t.first == g.p) toff = t.second;
+    if (toff < 0 && g.nA > 0) {
+      toff = (int64_t)tw.size();
+      const std::vector<double> t = ncp_twiddles(g.p);
+      tw.insert(tw.end(), t.begin(), t.end());
+      tabs.push_back({g.p, toff});
+    }
+    col0[k + 1] = col0[k] + g.nA;
+    for (int c = 0; c < g.nA; ++c) {
+      row0.push_back(B.row_off[k] + (int64_t)c * g.p);
+      L.push_back(g.p);
+      tw0.push_back(toff);
+      pk0.push_back(pkoff);
+      inst.push_back(k);
+      pkoff += g.p / 2;
+    }
+  }
+  B.ncols = (int)row0.size();
+  const size_t nc = std::max<size_t>(row0.size(), 1);
+  B.ncp_row0.ensure(nc);
+  B.ncp_tw0.ensure(nc);
+  B.ncp_pk0.ensure(nc);
+  B.ncp_L.ensure(nc);
+  B.ncp_inst.ensure(nc);
+  if (!row0.empty()) {
+    B.ncp_row0.upload(row0.data(), row0.size(), s);
+    B.ncp_tw0.upload(tw0.data(), tw0.size(), s);
+    B.ncp_pk0.upload(pk0.data(), pk0.size(), s);
+    B.ncp_L.upload(L.data(), L.size(), s);
+    B.ncp_inst.upload(inst.data(), inst.size(), s);
+  }
+  B.ncp_col0.upload(col0.data(), col0.size(), s);
+  if (tw.empty()) B.ncp_tw.ensure(1);
+  else B.ncp_tw.upload(tw.data(), tw.size(), s);
+  B.ncp_pk.ensure(std::max<int64_t>(pkoff, 1));
+  B.ncp_ccol.ensure(nc);
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  B.ncp_ready = true;
+}
+}  // namespace
+
+// SIRT over the whole batch with per-instance relaxpar and a per-instance
+// stopping rule (rule: AIRT_STOP_NONE, DP, ME or NCP; taud_host per
+// instance for DP / ME; ncp_smooth values for NCP).
+void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b, int rule,
+                const double *taud_host, int ncp_smooth, int64_t kmax, int lbk, double lb, int ubk,
+                double ub, const double *d_x0, double *d_x, int64_t *finaliter, int *stoprule,
+                double *gpu_ms) {
   Problem &P = B.P;
   cudaStream_t s = P.stream;
   const int K = B.ninst;
   AIRT_REQUIRE(kmax >= 0 && kmax < INT32_MAX, "kmax out of range");
+  AIRT_REQUIRE(rule == AIRT_STOP_NONE || rule == AIRT_STOP_DP || rule == AIRT_STOP_ME ||
+                   rule == AIRT_STOP_NCP,
+               "The chosen stopping rule is not valid.");
+  AIRT_REQUIRE((rule != AIRT_STOP_DP && rule != AIRT_STOP_ME) || taud_host,
+               "For stopping rules DP and ME a taudelta per instance must be given.");
+  AIRT_REQUIRE(rule != AIRT_STOP_NCP || (ncp_smooth >= 1 && ncp_smooth <= 4096),
+               "NCP: ncp_smooth must be in 1..4096");
+  const bool me = rule == AIRT_STOP_ME, ncp = rule == AIRT_STOP_NCP;
+  if (ncp) batch_ncp_setup(B);
   cudaEvent_t t0, t1;
   AIRT_CHECK_CUDA(cudaEventCreate(&t0));
   AIRT_CHECK_CUDA(cudaEventCreate(&t1));
@@ -695,7 +908,21 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
   B.rule.ensure(K);
   B.resn_last.ensure(K);
   B.lam.upload(lam_host, K, s);
-  if (taud_host) B.taud.upload(taud_host, K, s);
+  if (taud_host && (rule == AIRT_STOP_DP || me)) B.taud.upload(taud_host, K, s);
+  if (me || ncp) {
+    B.rprev.ensure(P.m);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(B.rprev.p, 0, P.m * sizeof(double), s));
+  }
+  if (me) {
+    B.pp.ensure(P.m);
+    B.ppr.ensure(P.m);
+    B.p2.ensure(K);
+    B.pr.ensure(K);
+  }
+  if (ncp) {
+    const std::vector<double> inf((size_t)K * ncp_smooth, INFINITY);
+    B.ncp_dk.upload(inf.data(), inf.size(), s);
+  }
   if (d_x0)
     AIRT_CHECK_CUDA(cudaMemcpyAsync(P.x64.p, d_x0, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   else
@@ -705,23 +932,36 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
   AIRT_CHECK_CUDA(cudaMemsetAsync(B.iters.p, 0, K * sizeof(int), s));
   AIRT_CHECK_CUDA(cudaMemsetAsync(B.rule.p, 0, K * sizeof(int), s));
   build_tiles(B, B.stop.p);
-  BFwd fo{d_b, P.M.p, P.mr32.p, B.rsq.p, B.inst_row.p, B.stop.p, 0};
+  BFwd fo{d_b, P.M.p, P.mr32.p, B.rsq.p, B.inst_row.p, B.stop.p, 0,
+          (me || ncp) ? B.rprev.p : nullptr, me ? B.pp.p : nullptr, me ? B.ppr.p : nullptr};
   BUpd uo{P.D.p, B.lam.p, P.x64.p, P.x32.p, B.inst_col.p, B.stop.p, lbk, ubk, lb, ub, 0};
-  const double *taud = taud_host ? B.taud.p : nullptr;
+  BCtrl co{rule, (rule == AIRT_STOP_DP || me) ? B.taud.p : nullptr, me ? B.p2.p : nullptr,
+           me ? B.pr.p : nullptr, ncp ? B.ncp_ccol.p : nullptr, ncp ? B.ncp_col0.p : nullptr,
+           ncp ? B.ncp_dk.p : nullptr, ncp_smooth};
+  const bool poll = rule != AIRT_STOP_NONE;
   const unsigned gk = (unsigned)((K + 127) / 128);
   auto fwd_reduce = [&]() {
     fwd_classes(B, fo);
-    k_batch_reduce<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, B.stop.p, B.nrm2.p);
+    k_batch_reduce<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, B.stop.p, B.nrm2.p,
+                                     me ? B.pp.p : nullptr, me ? B.ppr.p : nullptr,
+                                     me ? B.p2.p : nullptr, me ? B.pr.p : nullptr);
+    if (ncp && B.ncols > 0) {
+      k_batch_ncp_power<<<B.ncols, 128, 0, s>>>(B.ncp_row0.p, B.ncp_L.p, B.ncp_tw0.p, B.ncp_pk0.p,
+                                                B.ncp_inst.p, B.stop.p, B.rprev.p, B.ncp_tw.p,
+                                                B.ncp_pk.p);
+      k_batch_ncp_col<<<B.ncols, 256, 0, s>>>(B.ncp_L.p, B.ncp_pk0.p, B.ncp_inst.p, B.stop.p,
+                                              B.ncp_pk.p, B.ncp_ccol.p);
+    }
   };
   auto iteration = [&]() {
     bwd_classes(B, uo);
     fwd_reduce();
-    k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
+    k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, co, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
                                     B.resn_last.p);
     build_tiles(B, B.stop.p);
   };
   fwd_reduce();
-  k_batch_ctrl<<<gk, 128, 0, s>>>(K, 1, kmax, taud, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
+  k_batch_ctrl<<<gk, 128, 0, s>>>(K, 1, kmax, co, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
                                   B.resn_last.p);
   AIRT_LAUNCH_CHECK();
   build_tiles(B, B.stop.p);
@@ -751,7 +991,7 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
     }
     AIRT_LAUNCH_CHECK();
     it += cnt;
-    if (!taud) continue;
+    if (!poll) continue;
     AIRT_CHECK_CUDA(cudaMemcpyAsync(hstop.data(), B.stop.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
     AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
     bool all = true;

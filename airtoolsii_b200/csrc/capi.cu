@@ -514,8 +514,9 @@ int airt_batch_sirt_device(airt_batch *h, int method, const double *relaxpar, co
   AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
   AIRT_REQUIRE(lb_kind != AIRT_BOUND_VECTOR && ub_kind != AIRT_BOUND_VECTOR,
                "batched SIRT takes scalar bounds");
-  batch_sirt(*reinterpret_cast<Batch *>(h), method, relaxpar, d_b, taudelta, kmax, lb_kind, lb,
-             ub_kind, ub, d_x0, d_x, finaliter, stoprule, gpu_ms);
+  batch_sirt(*reinterpret_cast<Batch *>(h), method, relaxpar, d_b,
+             taudelta ? AIRT_STOP_DP : AIRT_STOP_NONE, taudelta, 2, kmax, lb_kind, lb, ub_kind, ub,
+             d_x0, d_x, finaliter, stoprule, gpu_ms);
   AIRT_API_END
 }
 
@@ -533,8 +534,30 @@ int airt_batch_sirt(airt_batch *h, int method, const double *relaxpar, const dou
   AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
   AIRT_REQUIRE(lb_kind != AIRT_BOUND_VECTOR && ub_kind != AIRT_BOUND_VECTOR,
                "batched SIRT takes scalar bounds");
-  batch_sirt(B, method, relaxpar, P.b64.p, taudelta, kmax, lb_kind, lb, ub_kind, ub,
-             x0 ? P.vin.p : nullptr, P.Xd.p, finaliter, stoprule, gpu_ms);
+  batch_sirt(B, method, relaxpar, P.b64.p, taudelta ? AIRT_STOP_DP : AIRT_STOP_NONE, taudelta, 2,
+             kmax, lb_kind, lb, ub_kind, ub, x0 ? P.vin.p : nullptr, P.Xd.p, finaliter, stoprule,
+             gpu_ms);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P.Xd.p, P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
+  AIRT_API_END
+}
+
+int airt_batch_sirt_rule(airt_batch *h, int method, const double *relaxpar, const double *b,
+                         int stoprule, const double *taudelta, int ncp_smooth, int64_t kmax,
+                         int lb_kind, double lb, int ub_kind, double ub, const double *x0, double *x,
+                         int64_t *finaliter, int *stoprule_out, double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && relaxpar && b && x, "null pointer argument");
+  Batch &B = *reinterpret_cast<Batch *>(h);
+  Problem &P = batch_problem(B);
+  AIRT_REQUIRE(method >= AIRT_LANDWEBER && method <= AIRT_SART, "SIRT method not defined.");
+  AIRT_REQUIRE(lb_kind != AIRT_BOUND_VECTOR && ub_kind != AIRT_BOUND_VECTOR,
+               "batched SIRT takes scalar bounds");
+  P.b64.upload(b, P.m, P.stream);
+  if (x0) P.vin.upload(x0, P.n, P.stream);
+  P.Xd.ensure(P.n);
+  batch_sirt(B, method, relaxpar, P.b64.p, stoprule, taudelta, ncp_smooth, kmax, lb_kind, lb,
+             ub_kind, ub, x0 ? P.vin.p : nullptr, P.Xd.p, finaliter, stoprule_out, gpu_ms);
   AIRT_CHECK_CUDA(cudaMemcpyAsync(x, P.Xd.p, P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
   AIRT_CHECK_CUDA(cudaStreamSynchronize(P.stream));
   AIRT_API_END

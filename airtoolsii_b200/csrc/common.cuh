@@ -335,9 +335,10 @@ int batch_ninst(const Batch &B);
 const int64_t *batch_row_off(const Batch &B);
 const int64_t *batch_col_off(const Batch &B);
 void batch_rho(Batch &B, int method, double tol, int maxit, double *rho_host);
-void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b, const double *taud_host,
-                int64_t kmax, int lbk, double lb, int ubk, double ub, const double *d_x0, double *d_x,
-                int64_t *finaliter, int *stoprule, double *gpu_ms);
+void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b, int rule,
+                const double *taud_host, int ncp_smooth, int64_t kmax, int lbk, double lb, int ubk,
+                double ub, const double *d_x0, double *d_x, int64_t *finaliter, int *stoprule,
+                double *gpu_ms);
 void batch_kaczmarz(Batch &B, const double *d_b, int64_t sweeps, double lam, int lbk, double lb,
                     int ubk, double ub, double *d_x, double *gpu_ms);
 void batch_backproject(Batch &B, int method, const double *d_b, double *d_x, double *gpu_ms);

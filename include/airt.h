@@ -276,6 +276,14 @@ int airt_batch_sirt_device(airt_batch *h, int method, const double *relaxpar, co
                            const double *taudelta, int64_t kmax, int lb_kind, double lb, int ub_kind,
                            double ub, const double *d_x0, double *d_x, int64_t *finaliter,
                            int *stoprule, double *gpu_ms);
+/* airt_batch_sirt with any stopping rule of auxil/check_stoprules.m applied
+ * per instance: stoprule AIRT_STOP_NONE, DP (54-72), ME (74-94) or NCP
+ * (96-151); taudelta[k] for DP and ME; NCP reshapes instance k's residual to
+ * its p_k x nA_k projections and compares ncp_smooth values. */
+int airt_batch_sirt_rule(airt_batch *h, int method, const double *relaxpar, const double *b,
+                         int stoprule, const double *taudelta, int ncp_smooth, int64_t kmax,
+                         int lb_kind, double lb, int ub_kind, double ub, const double *x0, double *x,
+                         int64_t *finaliter, int *stoprule_out, double *gpu_ms);
 /* Nonzeros of each instance's matrix (ninst entries). */
 int airt_batch_nnz(const airt_batch *h, int64_t *nnz);
 /* The batch's operator (afun of the block-diagonal system, afun_matrix.m:44-53):

@@ -67,6 +67,36 @@ def test_batch_sirt_dp_per_instance(batch, method):
         assert relerr(xs[k], Xo[:, -1]) <= RTOL
 
 
+@pytest.mark.parametrize("method", ["cimmino", "drop"])
+def test_batch_sirt_me_per_instance(batch, method):
+    """The ME rule (check_stoprules.m:74-94) applied per instance."""
+    B, mats, bs, tds, _ = batch
+    rho = B.rho(method)
+    xs, info = B.sirt(method, bs, 400, taudelta=tds, rho=rho, lbound=0.0, stoprule="ME")
+    for k, A in enumerate(mats):
+        Xo, io, _ = O.sirt(method, A, bs[k], [400], options={
+            "stoprule": {"type": "ME", "taudelta": tds[k]}, "rho": float(rho[k]), "lbound": 0.0})
+        assert info["finaliter"][k] == io["finaliter"], (k, info["finaliter"][k], io["finaliter"])
+        assert info["stoprule"][k] == io["stoprule"]
+        assert relerr(xs[k], Xo[:, -1]) <= RTOL
+
+
+@pytest.mark.parametrize("smooth", [1, 2, 4])
+def test_batch_sirt_ncp_per_instance(batch, smooth):
+    """The NCP rule (check_stoprules.m:96-151) per instance, each residual
+    reshaped to its instance's p x nA projections."""
+    B, mats, bs, _, _ = batch
+    rho = B.rho("cimmino")
+    xs, info = B.sirt("cimmino", bs, 300, rho=rho, stoprule="NCP", ncp_smooth=smooth)
+    for k, A in enumerate(mats):
+        Xo, io, _ = O.sirt("cimmino", A, bs[k], [300], options={
+            "stoprule": {"type": "NCP", "res_dims": [B.ps[k], B.nAs[k]], "ncp_smooth": smooth},
+            "rho": float(rho[k])})
+        assert info["finaliter"][k] == io["finaliter"], (k, info["finaliter"][k], io["finaliter"])
+        assert info["stoprule"][k] == io["stoprule"]
+        assert relerr(xs[k], Xo[:, -1]) <= RTOL
+
+
 def test_batch_sirt_fixed_iterations_box(batch):
     B, mats, bs, _, _ = batch
     rho = B.rho("cimmino")
