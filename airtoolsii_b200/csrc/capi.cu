@@ -176,6 +176,7 @@ static int make_geometry(int kind, int N, int nA, const double *cos_t, const dou
     }
     AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
     if (!P->matrix_free) generate_matrix(*P);
+    else mf_prepare(*P);
   } catch (...) {
     free_problem(P);
     throw;
@@ -220,6 +221,7 @@ int airt_problem_seismic(int N, int s, const double *src_x, const double *src_y,
     P->rcv_y.upload(rcv_y, p, P->stream);
     AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
     if (!P->matrix_free) generate_matrix(*P);
+    else mf_prepare(*P);
   } catch (...) {
     free_problem(P);
     throw;
@@ -268,6 +270,7 @@ int airt_problem_spherical(int N, int nA, const double *cos_t, const double *sin
     P->sin_k.upload(sin_k, koff[nc], P->stream);
     AIRT_CHECK_CUDA(cudaStreamSynchronize(P->stream));
     if (!P->matrix_free) generate_matrix(*P);
+    else mf_prepare(*P);
   } catch (...) {
     free_problem(P);
     throw;

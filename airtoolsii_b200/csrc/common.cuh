@@ -184,6 +184,10 @@ struct Problem {
 
   // reusable scratch of the weight and rho computations
   DevBuf<double> w1, w2;
+  // matrix-free back projection in fixed point (trace.cu): bound on
+  // (terms per pixel) x max |entry|, and the per-call max |u| (as bits)
+  double mf_kbound = 0.0;
+  DevBuf<unsigned long long> mf_umax;
 
   cudaStream_t stream = nullptr;
 
@@ -271,6 +275,9 @@ void sphere_stats(Problem &P, double *s2, double *s1, double *colcnt, double *co
 void build_csr_from_host_csc(Problem &P, const uint64_t *jc, const uint64_t *ir, const double *pr);
 void finalize_matrix(Problem &P);
 void generate_matrix(Problem &P);
+// Bounds of the fixed-point back projection of a matrix-free problem (one
+// pass over the rays at creation; trace.cu).
+void mf_prepare(Problem &P);
 void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
 void compute_weights(Problem &P, int method, double *dM, double *dD);
 void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const double *d_x0,

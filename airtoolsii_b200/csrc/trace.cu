@@ -8,11 +8,15 @@
 //    Replaces testprobs/paralleltomo.m:112-301, fanlineartomo.m:141-358 and
 //    seismictomo.m:96-287 (isMatrix = 1).
 //  * apply_matrix_free: forward projection (one thread per ray, FP64 sum in
-//    ray order) and back projection (one thread per ray, FP64 atomic scatter)
-//    that re-trace every ray, as the isMatrix = 0 handles of
+//    ray order) and back projection (one thread per ray, scatter in 64-bit
+//    fixed point, so the result does not depend on the order in which rays
+//    arrive) that re-trace every ray, as the isMatrix = 0 handles of
 //    paralleltomo.m:280-288 do.  Entry values are rounded to FP32 exactly as
 //    the stored matrix holds them, so stored and matrix-free operators agree
 //    up to summation order.
+#include <climits>
+#include <cstring>
+
 #include "common.cuh"
 #include "spmv.cuh"
 #include "stream.cuh"
@@ -68,26 +72,109 @@ __global__ void k_mf_forward(RayGeom g, int64_t nrays, bool excl, const double *
   }
 }
 
-__global__ void k_mf_adjoint(RayGeom g, int64_t nrays, bool excl, const double *__restrict__ u,
-                             double *__restrict__ y) {
+// ---- back projection in fixed point
+// FP64 atomics add the rays' terms in whatever order the rays arrive, so the
+// last bits of a back projection would change from run to run.  Instead
+// every term (float)v * u is rounded once to an integer multiple of 2^-s and
+// added as a 64-bit integer, which is associative.  s is chosen per call so
+// that no sum can leave +-2^62: with kbound = T * max|v| (T the power of two
+// at or above the most terms any pixel receives, max|v| a bound on the
+// entries) and 2^e > kbound * max|u|, each term is below 2^62 / T in
+// magnitude when scaled by 2^(62-e).  The quantum is then 2^-52 of the
+// largest possible term for T = 2^10 -- FP64 accuracy -- and the result is
+// bitwise the same on every run.
+// 2^e > kbound * umax; INT_MIN when the product is 0 (the sums are 0),
+// INT_MAX when it is not finite (the sums are NaN).
+__device__ __forceinline__ int fx_exponent(double kbound, double umax) {
+  const double prod = kbound * umax;
+  if (!(prod < INFINITY)) return INT_MAX;
+  return prod > 0.0 ? ilogb(prod) + 1 : INT_MIN;
+}
+
+__global__ void k_absmax(int64_t n, const double *__restrict__ u, const float *__restrict__ u32,
+                         unsigned long long *__restrict__ bits, const int *stop_flag) {
+  if (stop_flag && *(volatile const int *)stop_flag) return;
+  double m = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(u ? u[i] : (double)u32[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0)  // nonnegative doubles order as their bits
+    atomicMax(bits, (unsigned long long)__double_as_longlong(m));
+}
+
+template <typename TU>
+__global__ void k_mf_adjoint_fx(RayGeom g, int64_t nrays, bool excl, const TU *__restrict__ u,
+                                long long *__restrict__ acc, double kbound,
+                                const unsigned long long *__restrict__ umax_bits,
+                                const int *stop_flag) {
+  if (stop_flag && *(volatile const int *)stop_flag) return;
+  const int e = fx_exponent(kbound, __longlong_as_double((long long)*umax_bits));
+  if (e == INT_MIN || e == INT_MAX) return;  // u == 0 (result 0) or not finite (NaN)
+  const double sc = ldexp(1.0, 62 - e);
   const int64_t nn = (int64_t)g.N * g.N;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
        r += (int64_t)gridDim.x * blockDim.x) {
-    const double ur = u[r];
+    const double ur = (double)u[r];
     if (ur == 0.0) continue;
     row_entries(g, r, excl, [&](int col, double v) {
-      if (col >= 0 && col < nn) atomicAdd(y + col, (double)(float)v * ur);
+      if (col >= 0 && col < nn) {
+        const long long t = __double2ll_rn(__dmul_rn((double)(float)v, ur) * sc);
+        atomicAdd(reinterpret_cast<unsigned long long *>(acc + col), (unsigned long long)t);
+      }
     });
   }
 }
 
+// Fixed-point sums back to FP64, in place (acc and out are the same array).
+__global__ void k_fx_to_f64(int64_t n, double *__restrict__ out, double kbound,
+                            const unsigned long long *__restrict__ umax_bits, const int *stop_flag) {
+  if (stop_flag && *(volatile const int *)stop_flag) return;
+  const int e = fx_exponent(kbound, umax_bits ? __longlong_as_double((long long)*umax_bits) : 1.0);
+  const double inv = e == INT_MIN ? 0.0 : e == INT_MAX ? __longlong_as_double(0x7ff8000000000000LL)
+                                                       : ldexp(1.0, e - 62);
+  long long *acc = reinterpret_cast<long long *>(out);
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    out[j] = (double)acc[j] * inv;
+}
+
+// Terms each pixel receives and the largest entry, over every ray (the
+// bounds of the fixed-point scale).
+__global__ void k_mf_emit_stats(RayGeom g, int64_t nrays, bool excl, int *__restrict__ cnt,
+                                unsigned long long *__restrict__ vmax_bits) {
+  const int64_t nn = (int64_t)g.N * g.N;
+  double vm = 0.0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
+       r += (int64_t)gridDim.x * blockDim.x)
+    row_entries(g, r, excl, [&](int col, double v) {
+      if (col >= 0 && col < nn) {
+        atomicAdd(cnt + col, 1);
+        vm = fmax(vm, fabs((double)(float)v));
+      }
+    });
+  if (vm > 0.0) atomicMax(vmax_bits, (unsigned long long)__double_as_longlong(vm));
+}
+
+__global__ void k_max_int(int64_t n, const int *__restrict__ a, int *__restrict__ out) {
+  int m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, a[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 // Per-ray sums (squares, absolute values, squares weighted by colw) and
 // per-pixel counts and absolute sums, in one pass over the rays.
+// cs1 (column sums of |v|) is accumulated in fixed point (see above) with
+// max|u| = 1 and converted by k_fx_to_f64.
 __global__ void k_mf_stats(RayGeom g, int64_t nrays, bool excl, double *__restrict__ s2,
                            double *__restrict__ s1, double *__restrict__ ccnt,
                            double *__restrict__ cs1, const double *__restrict__ colw,
-                           double *__restrict__ s2w) {
+                           double *__restrict__ s2w, double kbound) {
   const int64_t nn = (int64_t)g.N * g.N;
+  const double sc = ldexp(1.0, 62 - fx_exponent(kbound, 1.0));
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
        r += (int64_t)gridDim.x * blockDim.x) {
     const Ray q = ray_of(g, r);
@@ -99,7 +186,9 @@ __global__ void k_mf_stats(RayGeom g, int64_t nrays, bool excl, double *__restri
       a1 += fabs(v);
       if (colw) aw += v * v * colw[col];
       if (ccnt) atomicAdd(ccnt + col, 1.0);
-      if (cs1) atomicAdd(cs1 + col, fabs(v));
+      if (cs1)
+        atomicAdd(reinterpret_cast<unsigned long long *>(cs1) + col,
+                  (unsigned long long)__double2ll_rn(fabs(v) * sc));
     });
     if (s2) s2[r] = a2;
     if (s1) s1[r] = a1;
@@ -146,6 +235,34 @@ void generate_matrix(Problem &P) {
   AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
 }
 
+void mf_prepare(Problem &P) {
+  cudaStream_t s = P.stream;
+  DevBuf<int> cnt, cmax;
+  DevBuf<unsigned long long> vbits;
+  cnt.ensure(P.n > 0 ? P.n : 1);
+  cmax.ensure(1);
+  vbits.ensure(1);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(cnt.p, 0, (P.n > 0 ? P.n : 1) * sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(cmax.p, 0, sizeof(int), s));
+  AIRT_CHECK_CUDA(cudaMemsetAsync(vbits.p, 0, sizeof(unsigned long long), s));
+  if (P.m > 0)
+    k_mf_emit_stats<<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m, excl_of(P), cnt.p,
+                                                            vbits.p);
+  if (P.n > 0) k_max_int<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, cnt.p, cmax.p);
+  AIRT_LAUNCH_CHECK();
+  int hmax = 0;
+  unsigned long long hv = 0;
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(&hmax, cmax.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(&hv, vbits.p, sizeof(hv), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  double T = 1.0;
+  while (T < (double)hmax) T *= 2.0;
+  double vmax = 0.0;
+  std::memcpy(&vmax, &hv, sizeof(vmax));
+  P.mf_kbound = T * (vmax > 0.0 ? vmax : 1.0);
+  P.mf_umax.ensure(1);
+}
+
 void apply_matrix_free(Problem &P, const double *d_in, double *d_out, int transp) {
   cudaStream_t s = P.stream;
   const RayGeom g = P.geom();
@@ -154,7 +271,12 @@ void apply_matrix_free(Problem &P, const double *d_in, double *d_out, int transp
     k_mf_forward<<<grid, 128, 0, s>>>(g, P.m, excl_of(P), d_in, d_out);
   } else {
     AIRT_CHECK_CUDA(cudaMemsetAsync(d_out, 0, P.n * sizeof(double), s));
-    k_mf_adjoint<<<grid, 128, 0, s>>>(g, P.m, excl_of(P), d_in, d_out);
+    AIRT_CHECK_CUDA(cudaMemsetAsync(P.mf_umax.p, 0, sizeof(unsigned long long), s));
+    k_absmax<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, d_in, nullptr, P.mf_umax.p, nullptr);
+    k_mf_adjoint_fx<double><<<grid, 128, 0, s>>>(g, P.m, excl_of(P), d_in,
+                                                 reinterpret_cast<long long *>(d_out),
+                                                 P.mf_kbound, P.mf_umax.p, nullptr);
+    k_fx_to_f64<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, d_out, P.mf_kbound, P.mf_umax.p, nullptr);
   }
   AIRT_LAUNCH_CHECK();
 }
@@ -169,32 +291,22 @@ void row_col_stats_mf(Problem &P, double *s2, double *s1, double *colcnt, double
   if (colcnt) AIRT_CHECK_CUDA(cudaMemsetAsync(colcnt, 0, P.n * sizeof(double), s));
   if (cols1) AIRT_CHECK_CUDA(cudaMemsetAsync(cols1, 0, P.n * sizeof(double), s));
   k_mf_stats<<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m, excl_of(P), s2, s1, colcnt,
-                                                      cols1, colw, s2w);
+                                                      cols1, colw, s2w, P.mf_kbound);
+  if (cols1)
+    k_fx_to_f64<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, cols1, P.mf_kbound, nullptr, nullptr);
   AIRT_LAUNCH_CHECK();
 }
 
 // Matrix-free pieces of the SIRT iteration (used by sirt.cu).
-namespace {
-__global__ void k_mf_adjoint_f32(RayGeom g, int64_t nrays, bool excl, const float *__restrict__ u,
-                                 double *__restrict__ y, const int *stop_flag) {
-  if (stop_flag && *(volatile const int *)stop_flag) return;
-  const int64_t nn = (int64_t)g.N * g.N;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    const double ur = (double)u[r];
-    if (ur == 0.0) continue;
-    row_entries(g, r, excl, [&](int col, double v) {
-      if (col >= 0 && col < nn) atomicAdd(y + col, (double)(float)v * ur);
-    });
-  }
-}
-}  // namespace
-
 void mf_backproject_f32(Problem &P, const float *u, double *g64, const int *stop_flag) {
   cudaStream_t s = P.stream;
   AIRT_CHECK_CUDA(cudaMemsetAsync(g64, 0, P.n * sizeof(double), s));
-  k_mf_adjoint_f32<<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m, excl_of(P), u, g64,
-                                                          stop_flag);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(P.mf_umax.p, 0, sizeof(unsigned long long), s));
+  k_absmax<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, nullptr, u, P.mf_umax.p, stop_flag);
+  k_mf_adjoint_fx<float><<<grid_for(P.m, 128, 16), 128, 0, s>>>(
+      P.geom(), P.m, excl_of(P), u, reinterpret_cast<long long *>(g64), P.mf_kbound, P.mf_umax.p,
+      stop_flag);
+  k_fx_to_f64<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, g64, P.mf_kbound, P.mf_umax.p, stop_flag);
   AIRT_LAUNCH_CHECK();
 }
 

@@ -56,6 +56,39 @@ __device__ __forceinline__ Ray ray_of(const RayGeom &g, int64_t r) {
   return q;
 }
 
+// Index range [lo, hi] (within 0..N) of the grid lines u = i - h whose
+// crossing with the ray can lie inside the square.  The crossing of line i
+// has the other coordinate v(i) = v0 + (dv/du)(i - h - u0) (u0, v0: the ray
+// origin; du, dv: its direction); lines whose exact v(i) is outside
+// [-h - kBoxSlack, h + kBoxSlack] are left out.  Their computed points differ
+// from the exact ones by far less than kBoxSlack (a few ulps of values of
+// order N), so the box test below would reject every one of them: leaving
+// them out changes no output, it only saves their divisions.  One index of
+// margin on each side absorbs the rounding of the bounds themselves.
+constexpr double kBoxSlack = 1e-6;
+
+__device__ __forceinline__ void crossing_range(int N, double h, double u0, double v0, double du,
+                                               double dv, int &lo, int &hi) {
+  lo = 0;
+  hi = N;
+  if (dv == 0.0) {  // v(i) = v0 for every line
+    if (fabs(v0) > h + kBoxSlack) hi = -1;
+    return;
+  }
+  const double r = du / dv;
+  const double i1 = h + u0 + r * (-h - kBoxSlack - v0);
+  const double i2 = h + u0 + r * (h + kBoxSlack - v0);
+  if (!(isfinite(i1) && isfinite(i2))) return;
+  const double l = fmax(0.0, floor(fmin(i1, i2)) - 1.0);
+  const double u = fmin((double)N, ceil(fmax(i1, i2)) + 1.0);
+  if (l > u) {
+    hi = -1;
+    return;
+  }
+  lo = (int)l;
+  hi = (int)u;
+}
+
 // Traces one ray and calls seg(col, len) for each segment in ray order
 // (before duplicate merging).  col is the 0-based column-major pixel index.
 template <class Seg>
@@ -65,13 +98,24 @@ __device__ __forceinline__ void trace_segments(int N, const Ray &q, bool exclude
   if (exclude_top_right && ((q.b == 0.0 && fabs(__dsub_rn(q.y0t, h)) < 1e-15) ||
                             (q.a == 0.0 && fabs(__dsub_rn(q.x0t, h)) < 1e-15)))
     return;
-  // x-crossing sequence in ascending t
+  // x-crossing sequence in ascending t, restricted to lines whose crossing
+  // can be inside the square
   int nx = 0, ix = 0, sx = 1;
-  if (q.a > 0.0) { nx = N + 1; ix = 0; sx = 1; }
-  else if (q.a < 0.0) { nx = N + 1; ix = N; sx = -1; }
+  if (q.a != 0.0) {
+    int lo, hi;
+    crossing_range(N, h, q.x0t, q.y0t, q.a, q.b, lo, hi);
+    nx = hi >= lo ? hi - lo + 1 : 0;
+    if (q.a > 0.0) { ix = lo; sx = 1; }
+    else { ix = hi; sx = -1; }
+  }
   int ny = 0, iy = 0, sy = 1;
-  if (q.b > 0.0) { ny = N + 1; iy = 0; sy = 1; }
-  else if (q.b < 0.0) { ny = N + 1; iy = N; sy = -1; }
+  if (q.b != 0.0) {
+    int lo, hi;
+    crossing_range(N, h, q.y0t, q.x0t, q.b, q.a, lo, hi);
+    ny = hi >= lo ? hi - lo + 1 : 0;
+    if (q.b > 0.0) { iy = lo; sy = 1; }
+    else { iy = hi; sy = -1; }
+  }
   int cx = 0, cy = 0;
   double tx = 0.0, ty = 0.0;
   if (nx) tx = __ddiv_rn(__dsub_rn((double)ix - h, q.x0t), q.a);
