@@ -242,3 +242,44 @@ class ParallelBatch:
         check(self._L.airt_batch_kaczmarz(self._h, dptr(b), int(sweeps), float(relaxpar), lk, lv,
                                           uk, uv, dptr(x), C.byref(ms)))
         return self.split_cols(x), {"gpu_ms": float(ms.value)}
+
+
+def sirt_multi_device(op, method, d_B, d_X, K, kmax, taudelta=None, relaxpar=None, rho=None,
+                      d_X0=None, lbound=None, ubound=None):
+    """SIRT on K right-hand sides of one stored matrix at once
+    (airt_sirt_multi_device): d_B (K x m), d_X (K x n) and optional d_X0
+    (K x n) are device addresses of instance-major FP64 arrays.  Every
+    instance stops on its own by the DP rule when taudelta (K values) is
+    given, else runs kmax iterations.  relaxpar defaults to 1.9/rho (rho of
+    the method, estimated on the device if not given; 1 for sart).  Returns
+    per-instance finaliter and stoprule and the device time."""
+    from .afun import as_operator
+    op = as_operator(op)
+    L = lib()
+    code = _lib.METHODS[method]
+    if relaxpar is None:
+        if method == "sart":
+            rho = 1.0
+        elif rho is None:
+            r = C.c_double()
+            check(L.airt_rho(op.handle, code, None, None, 1e-7, 200, C.byref(r)))
+            rho = float(r.value)
+        relaxpar = 1.9 / rho
+    o = _lib.SirtOpts()
+    o.method = code
+    o.relax_kind = _lib.RELAX_CONST
+    o.relaxpar = float(relaxpar)
+    o.stoprule = _lib.STOP["DP" if taudelta is not None else "NONE"]
+    o.lb_kind, o.lb = _bounds(lbound)
+    o.ub_kind, o.ub = _bounds(ubound)
+    o.kmax = int(kmax)
+    td = None if taudelta is None else np.ascontiguousarray(
+        np.broadcast_to(np.asarray(taudelta, dtype=np.float64), (K,)))
+    fin = np.zeros(K, np.int64)
+    rule = np.zeros(K, np.int32)
+    ms = C.c_double()
+    check(L.airt_sirt_multi_device(op.handle, C.byref(o), int(K), C.c_void_p(d_B),
+                                   C.c_void_p(d_X0 or None), dptr(td), C.c_void_p(d_X),
+                                   _lib.i64ptr(fin), rule.ctypes.data_as(_ip), C.byref(ms)))
+    return {"finaliter": fin, "stoprule": rule, "relaxpar": float(relaxpar),
+            "gpu_ms": float(ms.value)}

@@ -376,6 +376,16 @@ int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *D
   AIRT_API_END
 }
 
+int airt_sirt_multi_device(airt_problem *h, const airt_sirt_opts *opts, int K, const double *d_B,
+                           const double *d_X0, const double *taudelta, double *d_X,
+                           int64_t *finaliter, int *stoprule, double *gpu_ms) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && opts && d_B && d_X, "null pointer argument");
+  run_sirt_multi(*reinterpret_cast<Problem *>(h), *opts, K, d_B, d_X0, taudelta, d_X, finaliter,
+                 stoprule, gpu_ms);
+  AIRT_API_END
+}
+
 int airt_rho_custom(airt_problem *h, const double *M, int M_full, const double *D, int D_full,
                     double tol, int maxit, double *rho) {
   AIRT_API_BEGIN

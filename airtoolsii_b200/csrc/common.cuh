@@ -138,6 +138,13 @@ struct SirtState {
   double rmr_prev;  // r'*M*r of the previous residual (line search numerator)
 };
 
+// State of the multi-right-hand-side SIRT (multirhs.cu).
+struct MultiState {
+  int iter;    // global iteration whose residuals the control step judges next
+  int active;  // instances not stopped
+  double lam;  // relaxpar of the iteration being computed
+};
+
 struct SirtParams {
   int64_t kmax;
   int stoprule;
@@ -196,6 +203,11 @@ struct Problem {
   // custom SIRT weights given as full matrices (get_mfun_dfun.m:252-307, flag 2):
   // column-major m x m / n x n, and the column sums of D (line search)
   DevBuf<double> Mfull, Dfull, Dcol, dscratch;
+  // multi-right-hand-side SIRT (multirhs.cu): interleaved [row or pixel][instance]
+  DevBuf<double> mr_b, mr_x64, mr_part, mr_resn, mr_taud;
+  DevBuf<float> mr_x32, mr_r32;
+  DevBuf<int> mr_stop, mr_iters, mr_rule;
+  DevBuf<MultiState> mr_state;
   // NCP stopping rule: DFT twiddles (cos, sin pairs), power spectra, column distances, history
   DevBuf<double> ncp_tw, ncp_pk, ncp_col, ncp_dk;
   // fbp: filter kernel, per-column scales, filtered sinogram (kept between calls)
@@ -280,6 +292,9 @@ void generate_matrix(Problem &P);
 void mf_prepare(Problem &P);
 void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
 void compute_weights(Problem &P, int method, double *dM, double *dD);
+void run_sirt_multi(Problem &P, const airt_sirt_opts &o, int K, const double *d_B,
+                    const double *d_X0, const double *taud_host, double *d_X, int64_t *finaliter,
+                    int *stoprule, double *gpu_ms);
 void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const double *d_x0,
               const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
 // Stopping-rule state of the sweep loops of ART and CART (DP, NCP and NONE

@@ -232,6 +232,20 @@ int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *
                      const double *d_x0, const int64_t *K, int64_t nK, double *d_X,
                      double *resnorms, airt_info *info);
 
+/* SIRT on K right-hand sides of the same stored matrix at once (no
+ * counterpart in the reference, which takes one b per sirt call): device
+ * arrays d_B (m x K, column-major: right-hand side after right-hand side),
+ * d_X0 (n x K starting vectors, or NULL for zeros), d_X (n x K final
+ * iterates).  opts gives the built-in method, a constant or tabulated
+ * relaxpar, scalar bounds and kmax; opts->stoprule AIRT_STOP_DP stops every
+ * instance on its own at ||b_k - A x_k|| <= taudelta[k] (check_stoprules.m:
+ * 56-72), AIRT_STOP_NONE runs kmax iterations.  The iterates are kept
+ * interleaved by instance so that A is read once per iteration for all K.
+ * finaliter / stoprule: K entries. */
+int airt_sirt_multi_device(airt_problem *h, const airt_sirt_opts *opts, int K, const double *d_B,
+                           const double *d_X0, const double *taudelta, double *d_X,
+                           int64_t *finaliter, int *stoprule, double *gpu_ms);
+
 /* ART (Kaczmarz) sweeps, art.m:138-309.  Same K / X / info conventions. */
 int airt_art(airt_problem *h, const airt_art_opts *opts, const double *b, const double *x0,
              const int64_t *K, int64_t nK, double *X, double *resnorms, airt_info *info);

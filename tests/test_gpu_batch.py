@@ -154,3 +154,43 @@ def test_batch_apply_matches_instances(batch):
 
 def rng_vec(n, seed):
     return np.random.default_rng(900 + seed).standard_normal(n)
+
+
+@pytest.mark.parametrize("method,K", [("cimmino", 7), ("sart", 40), ("drop", 300)])
+def test_sirt_multi_rhs_vs_oracle(method, K):
+    """SIRT on K right-hand sides of one matrix (interleaved iterates, A read
+    once per iteration; K = 300 runs as two passes of at most 256) against the
+    oracle run per right-hand side: per-instance DP stop and iterate."""
+    import torch
+    from airtoolsii_b200.batch import sirt_multi_device
+    N, theta = 32, np.arange(0.0, 180.0, 6.0)
+    A = O.paralleltomo_matrix(N, theta)
+    op = airt.afun_matrix(A)
+    xs = [airt.random_ellipses(N, 5, seed=700 + k) for k in range(K)]
+    bs, tds = [], []
+    for k in range(K):
+        b, en = airt.add_noise(A @ xs[k], 0.01 + 0.02 * (k % 3), seed=900 + k)
+        bs.append(b)
+        tds.append(1.02 * en)
+    dB = torch.from_numpy(np.stack(bs)).cuda()
+    dX = torch.empty((K, A.shape[1]), dtype=torch.float64, device="cuda")
+    rho = 1.0 if method == "sart" else O.sirt(method, A, bs[0], [1])[1]["rho"]
+    info = sirt_multi_device(op, method, dB.data_ptr(), dX.data_ptr(), K, 500, taudelta=tds,
+                             rho=rho, lbound=0.0)
+    X = dX.cpu().numpy()
+    for k in range(0, K, max(1, K // 12)):
+        Xo, io, _ = O.sirt(method, A, bs[k], [500], options={
+            "stoprule": {"type": "DP", "taudelta": tds[k]}, "rho": rho, "lbound": 0.0})
+        assert info["finaliter"][k] == io["finaliter"], (k, info["finaliter"][k], io["finaliter"])
+        assert info["stoprule"][k] == io["stoprule"]
+        assert relerr(X[k], Xo[:, -1]) <= RTOL
+    # fixed iteration count from a given x0, box [0, 1]
+    dX0 = torch.from_numpy(np.stack(xs)).cuda() * 0.5
+    info = sirt_multi_device(op, method, dB.data_ptr(), dX.data_ptr(), K, 7, rho=rho,
+                             d_X0=dX0.data_ptr(), lbound=0.0, ubound=1.0)
+    assert np.all(info["finaliter"] == 7)
+    X = dX.cpu().numpy()
+    for k in (0, K - 1):
+        Xo, _, _ = O.sirt(method, A, bs[k], [7], 0.5 * xs[k], {"rho": rho, "lbound": 0.0,
+                                                               "ubound": 1.0})
+        assert relerr(X[k], Xo[:, -1]) <= RTOL
