@@ -215,6 +215,59 @@ class WarmStart:
                     net_wall_s=t_net, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
                     plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0))
 
+    def time_to_dp_shared(self, data, batch, kmax=2000):
+        """time_to_dp with the same-geometry engine: every batch of `batch`
+        sinograms is solved as K right-hand sides of the one stored matrix
+        (airt_sirt_multi_device: the matrix is read once per iteration for
+        the whole batch).  plain: cimmino from zero; warm: u = D.*A'(M.*b)
+        (one SART step from zero, through the same engine), x0 = U-Net(u),
+        cimmino from x0.  Same clocks and outputs as time_to_dp (no fbp arm)."""
+        from .batch import sirt_multi_device
+        torch = self.torch
+        total = data["b"].shape[0]
+        nb = total // batch
+        if nb < 1:
+            raise ValueError("need at least one full batch")
+        sels = [np.arange(i * batch, (i + 1) * batch) for i in range(nb)]
+        d_b = [data["b"].index_select(0, torch.from_numpy(sl).cuda()).contiguous() for sl in sels]
+        xp = [torch.empty((batch, self.n), dtype=torch.float64, device="cuda") for _ in range(nb)]
+        xw = [torch.empty_like(xp[0]) for _ in range(nb)]
+        u = [torch.empty_like(xp[0]) for _ in range(nb)]
+        x0 = [torch.empty_like(xp[0]) for _ in range(nb)]
+        tds = [data["taudelta"][sl] for sl in sels]
+        stream = self.A.stream_ptr()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ip = [sirt_multi_device(self.A, self.method, d_b[i].data_ptr(), xp[i].data_ptr(), batch,
+                                kmax, taudelta=tds[i], rho=self.rho) for i in range(nb)]
+        torch.cuda.synchronize()
+        wall_plain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        iw = []
+        for i in range(nb):
+            sirt_multi_device(self.A, "sart", d_b[i].data_ptr(), u[i].data_ptr(), batch, 1,
+                              relaxpar=1.0)
+            self.predict(u[i].data_ptr(), x0[i].data_ptr(), batch, stream)
+            iw.append(sirt_multi_device(self.A, self.method, d_b[i].data_ptr(), xw[i].data_ptr(),
+                                        batch, kmax, taudelta=tds[i], rho=self.rho,
+                                        d_X0=x0[i].data_ptr()))
+        torch.cuda.synchronize()
+        wall_warm = time.perf_counter() - t0
+        xt = data["x"].double()
+
+        def err(xs):
+            out = []
+            for i, sl in enumerate(sels):
+                ref = xt.index_select(0, torch.from_numpy(sl).cuda())
+                out.append((torch.linalg.norm(xs[i] - ref, dim=1) / torch.linalg.norm(ref, dim=1)).cpu().numpy())
+            return np.concatenate(out)
+        return dict(instances=nb * batch, batch=batch, plain_wall_s=wall_plain, warm_wall_s=wall_warm,
+                    plain_iters=np.concatenate([r["finaliter"] for r in ip]),
+                    warm_iters=np.concatenate([r["finaliter"] for r in iw]),
+                    plain_relerr=err(xp), warm_relerr=err(xw), x0_relerr=err(x0),
+                    plain_solver_gpu_ms=sum(r["gpu_ms"] for r in ip),
+                    warm_solver_gpu_ms=sum(r["gpu_ms"] for r in iw))
+
     def time_to_dp(self, data, batch, kmax=2000, fbp_filter="hamming"):
         """Time to the DP stop for all instances of `data`, `batch` at a time
         (a multiple of batch instances): plain, fbp warm start and learned

@@ -384,21 +384,28 @@ def widened_legs(A_c2, b_c2, wl):
 
 
 def warm_leg(a):
-    """Time to the DP stop, learned warm start vs plain batched GPU SIRT.
+    """Time to the DP stop, learned warm start vs plain GPU SIRT.
 
     Workload: paralleltomo N=256, 60 angles (0:3:177 degrees), 2% noise,
     held-out random-ellipse phantoms (seeds 500000..), solved `warm_batch` at
-    a time as one block-diagonal batch with a per-instance DP stop (tau =
-    1.02).  plain: cimmino from x0 = 0, batch after batch.  warm: u =
-    D.*A'(M.*b) (one SART step) of every batch, x0 = U-Net(u) from the
-    committed checkpoint, cimmino from x0, batch after batch.  Both
-    pipelines start from the sinograms resident on the device and end with
-    the solutions resident on the device; times are host wall clocks around
-    each synchronised pipeline, after one untimed pass.  The network was
-    trained on 20000 other seeds (seeds 1000..20999)
-    by this project's kernels (airtoolsii_b200/warmstart.py, train_c5).
-    fbp_baseline: the same solves started from the filtered back projection
-    (auxil/fbp.m, hamming filter) instead of the network's x0."""
+    a time with a per-instance DP stop (tau = 1.02).  plain: cimmino from
+    x0 = 0, batch after batch.  warm: u = D.*A'(M.*b) (one SART step) of
+    every batch, x0 = U-Net(u) from the committed checkpoint, cimmino from
+    x0, batch after batch.  Both pipelines start from the sinograms resident
+    on the device and end with the solutions resident on the device; times
+    are host wall clocks around each synchronised pipeline; one untimed pass,
+    then three timed passes (median and min reported).  The network was
+    trained on 20000 other seeds (seeds 1000..20999) by this project's
+    kernels (airtoolsii_b200/warmstart.py, train_c5).
+
+    Two solver engines, both measured: "shared" solves each batch as many
+    right-hand sides of the one geometry's matrix (read once per iteration
+    for the whole batch) -- the faster plain baseline and the headline --
+    and "block" stores the batch as a block-diagonal system (the engine for
+    batches of uneven geometry; the matrix is re-read per instance).
+    fbp_baseline (block engine): the same solves started from the filtered
+    back projection (auxil/fbp.m, hamming filter) instead of the network's
+    x0."""
     import torch
     from airtoolsii_b200 import warmstart as W
     ws = W.c5_warmstart()
@@ -406,42 +413,54 @@ def warm_leg(a):
     seeds = list(range(500000, 500000 + a.warm_heldout))
     te = ws.prepare(seeds, eta=W.C5["eta"])
     torch.cuda.synchronize()
-    ws.time_to_dp(te, a.warm_batch)            # untimed pass (tuning, first-touch)
-    r = ws.time_to_dp(te, a.warm_batch)
-    done = r["instances"]
-    cat = {k: np.asarray(r[k], dtype=float) for k in
-           ("plain_iters", "warm_iters", "plain_relerr", "warm_relerr", "x0_relerr",
-            "fbp_iters", "fbp_relerr", "fbp_x0_relerr")}
-    tot = {"plain_wall_s": r["plain_wall_s"], "warm_wall_s": r["warm_wall_s"],
-           "plain_gpu_ms": r["plain_solver_gpu_ms"], "warm_gpu_ms": r["warm_solver_gpu_ms"]}
-    return {
-        "metric": "time to the DP stop, warm start vs plain batched GPU SIRT (cimmino)",
-        "config": {"workload": "paralleltomo N=256, 60 angles, 2% noise, DP tau=1.02",
-                   "held_out": done, "batch": a.warm_batch,
-                   "network": "U-Net 4 levels, base 32, BF16 tcgen05 convolutions",
-                   "checkpoint": W.CHECKPOINT, "trained_on": meta.get("train_seeds"),
-                   "epochs": meta.get("epochs")},
-        "plain_s": round(tot["plain_wall_s"], 4), "warm_s": round(tot["warm_wall_s"], 4),
-        "speedup": round(tot["plain_wall_s"] / tot["warm_wall_s"], 3),
-        "plain_solver_gpu_ms": round(tot["plain_gpu_ms"], 2),
-        "warm_solver_gpu_ms": round(tot["warm_gpu_ms"], 2),
-        "plain_iters_mean": round(float(cat["plain_iters"].mean()), 3),
-        "warm_iters_mean": round(float(cat["warm_iters"].mean()), 3),
-        "plain_relerr_mean": round(float(cat["plain_relerr"].mean()), 5),
-        "warm_relerr_mean": round(float(cat["warm_relerr"].mean()), 5),
-        "x0_relerr_mean": round(float(cat["x0_relerr"].mean()), 5),
-        "warm_not_worse_frac": round(float(np.mean(cat["warm_relerr"] <= cat["plain_relerr"] * 1.0001)), 4),
-        "fbp_baseline": {"filter": r["fbp_filter"], "fbp_s": round(r["fbp_wall_s"], 4),
-                         "speedup": round(tot["plain_wall_s"] / r["fbp_wall_s"], 3),
-                         "solver_gpu_ms": round(r["fbp_solver_gpu_ms"], 2),
-                         "iters_mean": round(float(cat["fbp_iters"].mean()), 3),
-                         "relerr_mean": round(float(cat["fbp_relerr"].mean()), 5),
-                         "x0_relerr_mean": round(float(cat["fbp_x0_relerr"].mean()), 5),
-                         # the metric compares warm starts at equal relative error: fbp
-                         # reaches the DP stop sooner but at a larger error than plain SIRT
-                         "relerr_not_worse_than_plain": bool(cat["fbp_relerr"].mean()
-                                                             <= cat["plain_relerr"].mean())},
-    }
+
+    def runs(fn):
+        fn(te, a.warm_batch)                      # untimed pass (tuning, first-touch)
+        return [fn(te, a.warm_batch) for _ in range(3)]
+
+    def summary(rs):
+        sp = [r["plain_wall_s"] / r["warm_wall_s"] for r in rs]
+        r = rs[int(np.argsort(sp)[1])]            # the median run
+        cat = {k: np.asarray(r[k], dtype=float) for k in
+               ("plain_iters", "warm_iters", "plain_relerr", "warm_relerr", "x0_relerr")}
+        return r, {
+            "plain_s": round(r["plain_wall_s"], 4), "warm_s": round(r["warm_wall_s"], 4),
+            "speedup": round(float(np.median(sp)), 3), "speedup_min": round(float(np.min(sp)), 3),
+            "speedup_runs": [round(x, 3) for x in sp],
+            "plain_solver_gpu_ms": round(r["plain_solver_gpu_ms"], 2),
+            "warm_solver_gpu_ms": round(r["warm_solver_gpu_ms"], 2),
+            "plain_iters_mean": round(float(cat["plain_iters"].mean()), 3),
+            "warm_iters_mean": round(float(cat["warm_iters"].mean()), 3),
+            "plain_relerr_mean": round(float(cat["plain_relerr"].mean()), 5),
+            "warm_relerr_mean": round(float(cat["warm_relerr"].mean()), 5),
+            "x0_relerr_mean": round(float(cat["x0_relerr"].mean()), 5),
+            "warm_not_worse_frac": round(float(np.mean(cat["warm_relerr"]
+                                                       <= cat["plain_relerr"] * 1.0001)), 4)}
+
+    rb, block = summary(runs(ws.time_to_dp))
+    _, shared = summary(runs(ws.time_to_dp_shared))
+    fb = {k: np.asarray(rb[k], dtype=float) for k in ("fbp_iters", "fbp_relerr", "fbp_x0_relerr")}
+    block["fbp_baseline"] = {
+        "filter": rb["fbp_filter"], "fbp_s": round(rb["fbp_wall_s"], 4),
+        "speedup": round(rb["plain_wall_s"] / rb["fbp_wall_s"], 3),
+        "solver_gpu_ms": round(rb["fbp_solver_gpu_ms"], 2),
+        "iters_mean": round(float(fb["fbp_iters"].mean()), 3),
+        "relerr_mean": round(float(fb["fbp_relerr"].mean()), 5),
+        "x0_relerr_mean": round(float(fb["fbp_x0_relerr"].mean()), 5),
+        # the metric compares warm starts at equal relative error: fbp reaches
+        # the DP stop sooner but at a larger error than plain SIRT
+        "relerr_not_worse_than_plain": bool(fb["fbp_relerr"].mean()
+                                            <= np.asarray(rb["plain_relerr"]).mean())}
+    out = {"metric": "time to the DP stop, warm start vs plain GPU SIRT (cimmino)",
+           "config": {"workload": "paralleltomo N=256, 60 angles, 2% noise, DP tau=1.02",
+                      "held_out": rb["instances"], "batch": a.warm_batch,
+                      "network": "U-Net 4 levels, base 32, BF16 tcgen05 convolutions",
+                      "checkpoint": W.CHECKPOINT, "trained_on": meta.get("train_seeds"),
+                      "epochs": meta.get("epochs")},
+           "block_engine": block}
+    out.update({"engine": "shared geometry (many right-hand sides of one matrix)"})
+    out.update(shared)
+    return out
 
 
 def mf_leg(a, wl):
