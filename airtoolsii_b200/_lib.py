@@ -88,8 +88,8 @@ SIGNATURES = {
     "airt_weights": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "airt_rho": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.c_double, C.c_int, _dp]),
     "airt_sirt_multi_device": (C.c_int, [C.c_void_p, C.POINTER(SirtOpts), C.c_int, C.c_void_p,
-                                         C.c_void_p, _dp, C.c_void_p, _i64p, C.POINTER(C.c_int),
-                                         _dp]),
+                                         C.c_void_p, _dp, _dp, _i64p, C.c_int64, C.c_void_p,
+                                         C.c_void_p, _i64p, C.POINTER(C.c_int), _dp]),
     "airt_test_set_wait_budget": (C.c_int, [C.c_longlong]),
     "airt_test_inject_stall": (C.c_int, [C.c_int]),
     "airt_test_fail_alloc": (C.c_int, [C.c_int]),

@@ -245,13 +245,15 @@ class ParallelBatch:
 
 
 def sirt_multi_device(op, method, d_B, d_X, K, kmax, taudelta=None, relaxpar=None, rho=None,
-                      d_X0=None, lbound=None, ubound=None):
+                      d_X0=None, lbound=None, ubound=None, save=None, d_Xsave=None):
     """SIRT on K right-hand sides of one stored matrix at once
     (airt_sirt_multi_device): d_B (K x m), d_X (K x n) and optional d_X0
     (K x n) are device addresses of instance-major FP64 arrays.  Every
     instance stops on its own by the DP rule when taudelta (K values) is
-    given, else runs kmax iterations.  relaxpar defaults to 1.9/rho (rho of
-    the method, estimated on the device if not given; 1 for sart).  Returns
+    given, else runs kmax iterations.  relaxpar: a scalar or K values
+    (default 1.9/rho, rho of the method estimated on the device if not
+    given; 1 for sart).  save (iteration numbers) with d_Xsave (len(save) x
+    K x n) keeps every instance's iterate after those iterations.  Returns
     per-instance finaliter and stoprule and the device time."""
     from .afun import as_operator
     op = as_operator(op)
@@ -265,6 +267,10 @@ def sirt_multi_device(op, method, d_B, d_X, K, kmax, taudelta=None, relaxpar=Non
             check(L.airt_rho(op.handle, code, None, None, 1e-7, 200, C.byref(r)))
             rho = float(r.value)
         relaxpar = 1.9 / rho
+    lamk = None
+    if np.ndim(relaxpar) > 0:
+        lamk = np.ascontiguousarray(np.broadcast_to(np.asarray(relaxpar, np.float64), (K,)))
+        relaxpar = float(lamk[0])
     o = _lib.SirtOpts()
     o.method = code
     o.relax_kind = _lib.RELAX_CONST
@@ -278,8 +284,11 @@ def sirt_multi_device(op, method, d_B, d_X, K, kmax, taudelta=None, relaxpar=Non
     fin = np.zeros(K, np.int64)
     rule = np.zeros(K, np.int32)
     ms = C.c_double()
+    Ks = None if save is None else np.ascontiguousarray(save, np.int64)
     check(L.airt_sirt_multi_device(op.handle, C.byref(o), int(K), C.c_void_p(d_B),
-                                   C.c_void_p(d_X0 or None), dptr(td), C.c_void_p(d_X),
+                                   C.c_void_p(d_X0 or None), dptr(td), dptr(lamk),
+                                   _lib.i64ptr(Ks), 0 if Ks is None else Ks.size,
+                                   C.c_void_p(d_Xsave or None), C.c_void_p(d_X),
                                    _lib.i64ptr(fin), rule.ctypes.data_as(_ip), C.byref(ms)))
-    return {"finaliter": fin, "stoprule": rule, "relaxpar": float(relaxpar),
-            "gpu_ms": float(ms.value)}
+    return {"finaliter": fin, "stoprule": rule,
+            "relaxpar": float(relaxpar) if lamk is None else lamk, "gpu_ms": float(ms.value)}

@@ -377,12 +377,13 @@ int airt_rho(airt_problem *h, int method, const double *Mcustom, const double *D
 }
 
 int airt_sirt_multi_device(airt_problem *h, const airt_sirt_opts *opts, int K, const double *d_B,
-                           const double *d_X0, const double *taudelta, double *d_X,
+                           const double *d_X0, const double *taudelta, const double *relaxpar,
+                           const int64_t *Ksave, int64_t nsave, double *d_Xsave, double *d_X,
                            int64_t *finaliter, int *stoprule, double *gpu_ms) {
   AIRT_API_BEGIN
   AIRT_REQUIRE(h && opts && d_B && d_X, "null pointer argument");
-  run_sirt_multi(*reinterpret_cast<Problem *>(h), *opts, K, d_B, d_X0, taudelta, d_X, finaliter,
-                 stoprule, gpu_ms);
+  run_sirt_multi(*reinterpret_cast<Problem *>(h), *opts, K, d_B, d_X0, taudelta, relaxpar, Ksave,
+                 nsave, d_Xsave, d_X, finaliter, stoprule, gpu_ms);
   AIRT_API_END
 }
 

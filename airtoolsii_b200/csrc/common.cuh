@@ -204,7 +204,7 @@ struct Problem {
   // column-major m x m / n x n, and the column sums of D (line search)
   DevBuf<double> Mfull, Dfull, Dcol, dscratch;
   // multi-right-hand-side SIRT (multirhs.cu): interleaved [row or pixel][instance]
-  DevBuf<double> mr_b, mr_x64, mr_part, mr_resn, mr_taud;
+  DevBuf<double> mr_b, mr_x64, mr_part, mr_resn, mr_taud, mr_lam;
   DevBuf<float> mr_x32, mr_r32;
   DevBuf<int> mr_stop, mr_iters, mr_rule;
   DevBuf<MultiState> mr_state;
@@ -293,8 +293,9 @@ void mf_prepare(Problem &P);
 void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
 void compute_weights(Problem &P, int method, double *dM, double *dD);
 void run_sirt_multi(Problem &P, const airt_sirt_opts &o, int K, const double *d_B,
-                    const double *d_X0, const double *taud_host, double *d_X, int64_t *finaliter,
-                    int *stoprule, double *gpu_ms);
+                    const double *d_X0, const double *taud_host, const double *lam_host,
+                    const int64_t *Ksave, int64_t nsave, double *d_Xs, double *d_X,
+                    int64_t *finaliter, int *stoprule, double *gpu_ms);
 void run_sirt(Problem &P, const airt_sirt_opts &o, const double *d_b, const double *d_x0,
               const int64_t *K, int64_t nK, double *d_X, double *resn_host, airt_info *info);
 // Stopping-rule state of the sweep loops of ART and CART (DP, NCP and NONE

@@ -44,6 +44,7 @@ struct MrArgs {
   int lbk, ubk;
   double lb, ub;
   MultiState *st;
+  const double *lamk;  // per-instance relaxpar [Kp], or null (st->lam for all)
 };
 
 __device__ __forceinline__ void load8(const float *p, float v[8]) {
@@ -135,10 +136,13 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_bwd(int64_t n, const int64_t 
   const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
   const int64_t ng = (int64_t)gridDim.x * blockDim.x / G;
   const int Kp = a.Kp;
-  const double lam = a.st->lam;
+  double lam[8];
   bool live[8];
 #pragma unroll
-  for (int s = 0; s < 8; ++s) live[s] = (8 * lane + s) < a.K && !a.stop[8 * lane + s];
+  for (int s = 0; s < 8; ++s) {
+    live[s] = (8 * lane + s) < a.K && !a.stop[8 * lane + s];
+    lam[s] = a.lamk ? a.lamk[8 * lane + s] : a.st->lam;
+  }
   for (int64_t j = gid; j < n; j += ng) {
     double g[8];
     seg_dot<G>(__ldg(cp + j), __ldg(cp + j + 1), ri, cv, a.mr32, Kp, lane, g);
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_bwd(int64_t n, const int64_t 
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
       if (!live[s]) continue;
-      double x = xj[s] + lam * (Dj * g[s]);
+      double x = xj[s] + lam[s] * (Dj * g[s]);
       if (a.lbk) x = fmax(x, a.lb);
       if (a.ubk) x = fmin(x, a.ub);
       xj[s] = x;
@@ -232,6 +236,23 @@ __global__ void k_from_interleaved(int64_t len, int K, int Kp, const double *__r
   }
 }
 
+// After the control step of iteration st->iter: if that iteration is in the
+// save list, copy every instance's iterate to its slot (instance-major;
+// an instance that has stopped keeps its final iterate).
+__global__ void k_mr_save(int64_t n, int K, int Kp, const MultiState *st,
+                          const int *__restrict__ save_slot, const double *__restrict__ x64,
+                          double *__restrict__ Xs, int64_t slot_stride) {
+  const int slot = save_slot[st->iter];
+  if (slot < 0) return;
+  double *dst = Xs + (int64_t)slot * slot_stride;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)K * n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e / n);
+    const int64_t j = e - (int64_t)k * n;
+    dst[e] = x64[j * Kp + k];
+  }
+}
+
 int group_for(int Kp) {
   int G = 1;
   while (8 * G < Kp) G <<= 1;
@@ -240,7 +261,9 @@ int group_for(int Kp) {
 
 // One pass: K <= kMaxK instances.
 void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, const double *d_X0,
-                const double *taud_host, double *d_X, int64_t *finaliter, int *stoprule) {
+                const double *taud_host, const double *lam_host, const int *save_slot,
+                double *d_Xs, int64_t slot_stride, double *d_X, int64_t *finaliter,
+                int *stoprule) {
   cudaStream_t s = P.stream;
   const int64_t m = P.m, n = P.n, kmax = o.kmax;
   const int Kp = (K + 7) / 8 * 8;
@@ -268,13 +291,19 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
   AIRT_CHECK_CUDA(cudaMemsetAsync(P.mr_rule.p, 0, Kp * sizeof(int), s));
   MultiState st0{0, K, o.relaxpar};
   P.mr_state.upload(&st0, 1, s);
+  if (lam_host) {
+    std::vector<double> lk(Kp, 0.0);
+    std::copy(lam_host, lam_host + K, lk.begin());
+    P.mr_lam.upload(lk.data(), Kp, s);
+  }
   if (taud_host) P.mr_taud.upload(taud_host, K, s);
   const double *taud = taud_host ? P.mr_taud.p : nullptr;
   if (o.relax_kind == AIRT_RELAX_TABLE && kmax > 0) P.table.upload(o.relax_table, kmax, s);
   const double *table = o.relax_kind == AIRT_RELAX_TABLE ? P.table.p : nullptr;
 
   MrArgs a{K, Kp, P.mr_b.p, P.M.p, P.D.p, P.mr_x64.p, P.mr_x32.p, P.mr_r32.p, P.mr_stop.p,
-           P.mr_part.p, o.lb_kind, o.ub_kind, o.lb, o.ub, P.mr_state.p};
+           P.mr_part.p, o.lb_kind, o.ub_kind, o.lb, o.ub, P.mr_state.p,
+           lam_host ? P.mr_lam.p : nullptr};
   auto fwd = [&]() {
     switch (G) {
       case 1: k_mr_fwd<1><<<gf, kMrThreads, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, a); break;
@@ -299,6 +328,9 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
     k_mr_ctrl<<<K, 256, 0, s>>>(K, Kp, (int)gf, initial, kmax, P.mr_part.p, taud, P.mr_stop.p,
                                 P.mr_iters.p, P.mr_rule.p, P.mr_resn.p, P.mr_state.p);
     k_mr_advance<<<1, 32, 0, s>>>(P.mr_state.p, table, o.relaxpar, kmax, initial);
+    if (save_slot && !initial)
+      k_mr_save<<<grid_for((int64_t)K * n, 256), 256, 0, s>>>(n, K, Kp, P.mr_state.p, save_slot,
+                                                              P.mr_x64.p, d_Xs, slot_stride);
   };
   fwd();
   ctrl(1);
@@ -369,8 +401,9 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
 }  // namespace
 
 void run_sirt_multi(Problem &P, const airt_sirt_opts &o, int K, const double *d_B,
-                    const double *d_X0, const double *taud_host, double *d_X, int64_t *finaliter,
-                    int *stoprule, double *gpu_ms) {
+                    const double *d_X0, const double *taud_host, const double *lam_host,
+                    const int64_t *Ksave, int64_t nsave, double *d_Xs, double *d_X,
+                    int64_t *finaliter, int *stoprule, double *gpu_ms) {
   AIRT_REQUIRE(!P.matrix_free, "multi-right-hand-side SIRT needs the stored matrix");
   AIRT_REQUIRE(K >= 1, "K must be positive");
   AIRT_REQUIRE(o.method >= AIRT_LANDWEBER && o.method <= AIRT_SART,
@@ -384,7 +417,17 @@ void run_sirt_multi(Problem &P, const airt_sirt_opts &o, int K, const double *d_
   AIRT_REQUIRE(o.lb_kind != AIRT_BOUND_VECTOR && o.ub_kind != AIRT_BOUND_VECTOR,
                "multi-right-hand-side SIRT takes scalar bounds");
   AIRT_REQUIRE(o.kmax >= 0 && o.kmax < (int64_t)INT32_MAX, "kmax out of range");
+  AIRT_REQUIRE(nsave == 0 || (Ksave && d_Xs), "save list without an output array");
   cudaStream_t s = P.stream;
+  for (int64_t l = 0; l < nsave; ++l) {
+    AIRT_REQUIRE(Ksave[l] >= 1 && Ksave[l] <= o.kmax, "saved iterations must lie in 1..kmax");
+    AIRT_REQUIRE(l == 0 || Ksave[l] > Ksave[l - 1], "Elements of K must be strictly increasing.");
+  }
+  if (nsave > 0) {
+    std::vector<int> slots(o.kmax + 1, -1);
+    for (int64_t l = 0; l < nsave; ++l) slots[Ksave[l]] = (int)l;
+    P.save_slot.upload(slots.data(), slots.size(), s);
+  }
   cudaEvent_t t0, t1;
   AIRT_CHECK_CUDA(cudaEventCreate(&t0));
   AIRT_CHECK_CUDA(cudaEventCreate(&t1));
@@ -396,8 +439,10 @@ void run_sirt_multi(Problem &P, const airt_sirt_opts &o, int K, const double *d_
   for (int k0 = 0; k0 < K; k0 += kMaxK) {
     const int kc = std::min(kMaxK, K - k0);
     multi_pass(P, o, kc, d_B + (int64_t)k0 * P.m, d_X0 ? d_X0 + (int64_t)k0 * P.n : nullptr,
-               taud ? taud + k0 : nullptr, d_X + (int64_t)k0 * P.n,
-               finaliter ? finaliter + k0 : nullptr, stoprule ? stoprule + k0 : nullptr);
+               taud ? taud + k0 : nullptr, lam_host ? lam_host + k0 : nullptr,
+               nsave > 0 ? P.save_slot.p : nullptr, nsave > 0 ? d_Xs + (int64_t)k0 * P.n : nullptr,
+               (int64_t)K * P.n, d_X + (int64_t)k0 * P.n, finaliter ? finaliter + k0 : nullptr,
+               stoprule ? stoprule + k0 : nullptr);
   }
   AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
   AIRT_CHECK_CUDA(cudaEventSynchronize(t1));

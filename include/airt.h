@@ -241,9 +241,14 @@ int airt_sirt_device(airt_problem *h, const airt_sirt_opts *opts, const double *
  * instance on its own at ||b_k - A x_k|| <= taudelta[k] (check_stoprules.m:
  * 56-72), AIRT_STOP_NONE runs kmax iterations.  The iterates are kept
  * interleaved by instance so that A is read once per iteration for all K.
- * finaliter / stoprule: K entries. */
+ * relaxpar (host, K values) gives every instance its own relaxpar, NULL the
+ * one of opts.  Ksave (nsave strictly increasing iteration numbers in
+ * 1..kmax) saves every instance's iterate after those iterations into
+ * d_Xsave (nsave blocks of n x K; an instance that has stopped keeps its
+ * final iterate).  finaliter / stoprule: K entries. */
 int airt_sirt_multi_device(airt_problem *h, const airt_sirt_opts *opts, int K, const double *d_B,
-                           const double *d_X0, const double *taudelta, double *d_X,
+                           const double *d_X0, const double *taudelta, const double *relaxpar,
+                           const int64_t *Ksave, int64_t nsave, double *d_Xsave, double *d_X,
                            int64_t *finaliter, int *stoprule, double *gpu_ms);
 
 /* ART (Kaczmarz) sweeps, art.m:138-309.  Same K / X / info conventions. */

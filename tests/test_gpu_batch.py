@@ -194,3 +194,28 @@ def test_sirt_multi_rhs_vs_oracle(method, K):
         Xo, _, _ = O.sirt(method, A, bs[k], [7], 0.5 * xs[k], {"rho": rho, "lbound": 0.0,
                                                                "ubound": 1.0})
         assert relerr(X[k], Xo[:, -1]) <= RTOL
+
+
+def test_sirt_multi_rhs_per_instance_relaxpar_and_saved_iterates():
+    """Every instance with its own relaxpar, iterates saved after iterations
+    2, 5 and 9, against the oracle per instance."""
+    import torch
+    from airtoolsii_b200.batch import sirt_multi_device
+    N, theta = 24, np.arange(0.0, 180.0, 5.0)
+    A = O.paralleltomo_matrix(N, theta)
+    op = airt.afun_matrix(A)
+    K = 11
+    b = A @ O.shepplogan(N)
+    lams = np.linspace(0.2, 1.8, K)
+    dB = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(b, (K, b.size)))).cuda()
+    dX = torch.empty((K, A.shape[1]), dtype=torch.float64, device="cuda")
+    save = np.array([2, 5, 9])
+    dS = torch.empty((3, K, A.shape[1]), dtype=torch.float64, device="cuda")
+    sirt_multi_device(op, "sart", dB.data_ptr(), dX.data_ptr(), K, 9, relaxpar=lams,
+                      save=save, d_Xsave=dS.data_ptr())
+    S = dS.cpu().numpy()
+    for k in range(K):
+        Xo, _, _ = O.sirt("sart", A, b, list(save), None, {"relaxpar": float(lams[k])})
+        for j in range(3):
+            assert relerr(S[j, k], Xo[:, j]) <= RTOL
+        assert np.array_equal(S[2, k], dX[k].cpu().numpy())

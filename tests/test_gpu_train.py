@@ -22,14 +22,18 @@ def prob():
     return A, A_ref, x, b_ex, b, en
 
 
-@pytest.mark.parametrize("method", ["cimmino", "sart", "kaczmarz"])
-def test_train_relaxpar(prob, method):
+@pytest.mark.parametrize("method,batched", [("cimmino", True), ("cimmino", False),
+                                            ("sart", True), ("drop", True), ("kaczmarz", False)])
+def test_train_relaxpar(prob, method, batched):
+    """batched: the golden-section probes of the next three steps run as one
+    multi-right-hand-side solve; the decisions, and so the result, are those
+    of the sequential search."""
     A, A_ref, x, _, b, _ = prob
     opts = {}
-    if method == "cimmino":
+    if method in ("cimmino", "drop"):
         _, io, _ = O.sirt(method, A_ref, b, [1])
         opts["rho"] = io["rho"]
-    r_gpu = T.train_relaxpar(A, b, x, method, 60, opts)
+    r_gpu = T.train_relaxpar(A, b, x, method, 60, opts, batched=batched)
     r_ref = O.train_relaxpar(A_ref, b, x, method, 60, opts)
     assert 0 < r_ref < 2 / (opts.get("rho", 1.0) if method != "kaczmarz" else 1.0)
     assert abs(r_gpu - r_ref) <= 1e-9 * r_ref
@@ -48,13 +52,15 @@ def test_train_relaxpar_columnaction(prob):
     assert abs(r_gpu - r_ref) <= 1e-9 * r_ref
 
 
-@pytest.mark.parametrize("rule", ["DP", "ME"])
-def test_train_dpme(prob, rule):
+@pytest.mark.parametrize("rule,batched", [("DP", True), ("ME", True), ("DP", False)])
+def test_train_dpme(prob, rule, batched):
+    """batched: the replicas run together on the multi-right-hand-side
+    engine with every iterate saved."""
     A, A_ref, x, b_ex, _, en = prob
     _, io, _ = O.sirt("cimmino", A_ref, b_ex, [1])
     opts = {"rho": io["rho"]}
-    E = np.random.default_rng(7).standard_normal((A_ref.shape[0], 3))
-    t_gpu = T.train_dpme(A, b_ex, x, "cimmino", rule, en, 3, 40, opts, E=E)
+    E = np.random.default_rng(7).standard_normal((A_ref.shape[0], 5))
+    t_gpu = T.train_dpme(A, b_ex, x, "cimmino", rule, en, 5, 40, opts, E=E, batched=batched)
     t_ref = O.train_dpme(A_ref, b_ex, x, "cimmino", rule, en, E, 40, opts)
     assert t_ref > 0.5
     assert abs(t_gpu - t_ref) <= 1e-6 * t_ref
