@@ -38,9 +38,10 @@
  *   bh           = airt_mex('batch', int32(N), int32(nA), int32(p), cos_t, sin_t, offsets)
  *   [ro, co, nz] = airt_mex('batch_layout', bh, ninst)
  *   rho          = airt_mex('batch_rho', bh, ninst, method)
- *   [x, it, sr, ms] = airt_mex('batch_sirt', bh, ninst, opts, b, x0)
+ *   [x, it, sr, ms] = airt_mex('batch_sirt', bh, ninst, opts, b, x0)    per-instance rule
  *   [x, ms]      = airt_mex('batch_kaczmarz', bh, ninst, b, sweeps, relaxpar, lbound, ubound)
  *   x            = airt_mex('batch_backproject', bh, ninst, method, b)   b, x: gpuArray
+ *   [X, it, sr]  = airt_mex('sirt_multi', h, opts, B, X0, taudelta)     B, X0, X: gpuArray
  *                  airt_mex('batch_destroy', bh)
  *   uh           = airt_mex('unet', H, W, base, levels, max_batch, seed)
  *   w            = airt_mex('unet_params', uh)                 single vector
@@ -582,10 +583,13 @@ static void cmd_batch_sirt(int nlhs, mxArray *plhs[], int nrhs, const mxArray *p
     mxArray *it = mxCreateNumericMatrix((mwSize)k, 1, mxINT64_CLASS, mxREAL);
     mxArray *sr = mxCreateNumericMatrix((mwSize)k, 1, mxINT32_CLASS, mxREAL);
     double ms = 0.0;
-    chk(airt_batch_sirt(bh, (int)dfield(o, "method", AIRT_CIMMINO), lam, b, td,
-                        (int64_t)dfield(o, "kmax", 100), lbk, lb, ubk, ub, x0,
-                        mxGetDoubles(plhs[0]), (int64_t *)mxGetInt64s(it), (int *)mxGetInt32s(sr),
-                        &ms));
+    /* opts.stoprule (0 NONE, 1 DP, 2 ME, 3 NCP) applies per instance; without it, DP when
+       taudelta is given */
+    const int rule = (int)dfield(o, "stoprule", td ? AIRT_STOP_DP : AIRT_STOP_NONE);
+    chk(airt_batch_sirt_rule(bh, (int)dfield(o, "method", AIRT_CIMMINO), lam, b, rule, td,
+                             (int)dfield(o, "ncp_smooth", 2), (int64_t)dfield(o, "kmax", 100),
+                             lbk, lb, ubk, ub, x0, mxGetDoubles(plhs[0]),
+                             (int64_t *)mxGetInt64s(it), (int *)mxGetInt32s(sr), &ms));
     if (nlhs > 1) plhs[1] = it;
     else mxDestroyArray(it);
     if (nlhs > 2) plhs[2] = sr;
@@ -687,6 +691,61 @@ static void cmd_batch_backproject(int nlhs, mxArray *plhs[], int nrhs, const mxA
     (void)nlhs;
 }
 
+/* [X, it, sr] = airt_mex('sirt_multi', h, opts, gpuArray B, X0, taudelta): SIRT on the K
+   columns of B (m x K) at once; X0 (n x K gpuArray) or empty; taudelta K values or empty. */
+static void cmd_sirt_multi(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
+    need(nrhs == 6 && mxIsStruct(prhs[2]) && mxIsGPUArray(prhs[3]),
+         "airt_mex('sirt_multi', h, opts, gpuArray B, X0, taudelta)");
+    airt_problem *h = (airt_problem *)handle_in(prhs[1]);
+    const mxArray *o = prhs[2];
+    int64_t m = 0, n = 0, ntd = 0;
+    problem_size(h, &m, &n);
+    const mxGPUArray *B = mxGPUCreateFromMxArray(prhs[3]);
+    need(mxGPUGetClassID(B) == mxDOUBLE_CLASS && mxGPUGetNumberOfElements(B) % (mwSize)m == 0,
+         "B must be a double gpuArray with m rows");
+    const int K = (int)(mxGPUGetNumberOfElements(B) / (mwSize)m);
+    const mxGPUArray *X0 = NULL;
+    if (!mxIsEmpty(prhs[4])) {
+        need(mxIsGPUArray(prhs[4]), "X0 must be a gpuArray or empty");
+        X0 = mxGPUCreateFromMxArray(prhs[4]);
+        need(mxGPUGetNumberOfElements(X0) == (mwSize)(n * K), "X0 must be n x K");
+    }
+    const double *td = mxIsEmpty(prhs[5]) ? NULL : dvec(prhs[5], &ntd);
+    need(!td || ntd == K, "taudelta: one threshold per column of B");
+    airt_sirt_opts so;
+    memset(&so, 0, sizeof so);
+    so.method = (int)dfield(o, "method", AIRT_CIMMINO);
+    so.relax_kind = AIRT_RELAX_CONST;
+    so.relaxpar = dfield(o, "relaxpar", 1.0);
+    so.stoprule = td ? AIRT_STOP_DP : AIRT_STOP_NONE;
+    bound(o, "lbound", 1, &so.lb_kind, &so.lb, &so.lbv);
+    bound(o, "ubound", 1, &so.ub_kind, &so.ub, &so.ubv);
+    so.kmax = (int64_t)dfield(o, "kmax", 100);
+    const mwSize dims[2] = {(mwSize)n, (mwSize)K};
+    mxGPUArray *X = mxGPUCreateGPUArray(2, dims, mxDOUBLE_CLASS, mxREAL, MX_GPU_DO_NOT_INITIALIZE);
+    mxArray *it = mxCreateNumericMatrix((mwSize)K, 1, mxINT64_CLASS, mxREAL);
+    mxArray *sr = mxCreateNumericMatrix((mwSize)K, 1, mxINT32_CLASS, mxREAL);
+    double ms = 0.0;
+    const int st = airt_sirt_multi_device(
+        h, &so, K, (const double *)mxGPUGetDataReadOnly(B),
+        X0 ? (const double *)mxGPUGetDataReadOnly(X0) : NULL, td, NULL, NULL, 0, NULL,
+        (double *)mxGPUGetData(X), (int64_t *)mxGetInt64s(it), (int *)mxGetInt32s(sr), &ms);
+    mxGPUDestroyGPUArray(B);
+    if (X0) mxGPUDestroyGPUArray(X0);
+    if (st != AIRT_OK) {
+        mxGPUDestroyGPUArray(X);
+        mxDestroyArray(it);
+        mxDestroyArray(sr);
+    }
+    chk(st);
+    plhs[0] = mxGPUCreateMxArrayOnGPU(X);
+    mxGPUDestroyGPUArray(X);
+    if (nlhs > 1) plhs[1] = it;
+    else mxDestroyArray(it);
+    if (nlhs > 2) plhs[2] = sr;
+    else mxDestroyArray(sr);
+}
+
 static void cmd_unet_forward(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
     need(nrhs == 4 && mxIsGPUArray(prhs[2]), "airt_mex('unet_forward', uh, gpuArray x, B)");
     airt_unet *uh = (airt_unet *)handle_in(prhs[1]);
@@ -741,6 +800,7 @@ static const struct command commands[] = {
     {"unet_destroy", cmd_unet_destroy},
 #ifdef AIRT_MEX_GPUARRAY
     {"batch_backproject", cmd_batch_backproject},
+    {"sirt_multi", cmd_sirt_multi},
     {"unet_forward", cmd_unet_forward},
 #endif
 };

@@ -43,7 +43,7 @@ def test_gateway_has_a_command_for_every_part_of_the_c_abi():
     src = open(GATEWAY).read()
     for cmd in ("matrix", "parallel", "fan", "seismic", "spherical", "size", "export", "apply",
                 "weights", "rho", "sirt", "art", "cart", "fbp", "destroy", "batch",
-                "batch_layout", "batch_rho", "batch_sirt", "batch_kaczmarz", "batch_backproject",
+                "batch_layout", "batch_rho", "batch_sirt", "batch_kaczmarz", "batch_backproject", "sirt_multi",
                 "batch_destroy", "unet", "unet_params", "unet_set_params", "unet_forward",
                 "unet_destroy"):
         assert '{"%s", cmd_' % cmd in src, cmd
