@@ -68,7 +68,7 @@ struct Batch {
   TileSet rt, ct;  // row (CSR) and column (CSC) tiles
   DevBuf<InstGeom> g;
   DevBuf<int64_t> d_row_off, d_col_off;
-  DevBuf<int> inst_row, inst_col, stop, iters, rule;
+  DevBuf<int> inst_row, inst_col, stop, iters, rule, active;
   DevBuf<double> rsq, nrm2, lam, taud, resn_last;
   bool tuned = false;
   // active tiles per class, rebuilt after every stop-rule update:
@@ -279,42 +279,6 @@ __global__ void k_active_tiles(int ntiles, int64_t nseg, const int *__restrict__
     }
 }
 
-// ||r_k||^2 per active instance: one block per instance, fixed order; with
-// pp (ME) also ||r_(k-1)||^2 and r_(k-1)'(r_(k-1) + r_k).
-__global__ void __launch_bounds__(256) k_batch_reduce(const int64_t *__restrict__ roff,
-                                                      const double *__restrict__ rsq,
-                                                      const int *__restrict__ stop,
-                                                      double *__restrict__ nrm2,
-                                                      const double *__restrict__ pp,
-                                                      const double *__restrict__ ppr,
-                                                      double *__restrict__ p2,
-                                                      double *__restrict__ pr) {
-  const int k = blockIdx.x;
-  if (stop[k]) return;
-  double a = 0, c = 0, d = 0;
-  for (int64_t i = roff[k] + threadIdx.x; i < roff[k + 1]; i += blockDim.x) {
-    a += rsq[i];
-    if (pp) {
-      c += pp[i];
-      d += ppr[i];
-    }
-  }
-  a = block_sum<256>(a);
-  if (pp) {
-    __syncthreads();
-    c = block_sum<256>(c);
-    __syncthreads();
-    d = block_sum<256>(d);
-  }
-  if (threadIdx.x == 0) {
-    nrm2[k] = a;
-    if (pp) {
-      p2[k] = c;
-      pr[k] = d;
-    }
-  }
-}
-
 // NCP per instance, part 1: the periodogram of every projection column of
 // the active instances (block = column; frequencies 1..floor(L/2) over the
 // threads), by direct summation with the twiddle table of the column's
@@ -374,60 +338,93 @@ struct BCtrl {
   int ns;
 };
 
-__global__ void k_batch_ctrl(int ninst, int initial, int64_t kmax, BCtrl c,
-                             const double *__restrict__ nrm2, int *__restrict__ stop,
-                             int *__restrict__ iters, int *__restrict__ rule,
-                             double *__restrict__ resn) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ninst; k += gridDim.x * blockDim.x) {
-    if (stop[k]) continue;
-    const int it = iters[k] + (initial ? 0 : 1);
-    iters[k] = it;
-    const double nrk = sqrt(nrm2[k]);
-    resn[k] = nrk;
-    bool st = false;
-    int why = 0;
-    switch (c.rule) {
-      case AIRT_STOP_DP:
-        if (nrk <= c.taud[k] || it >= kmax) {
-          st = true;
-          why = it != kmax ? 2 : 0;
-        }
-        break;
-      case AIRT_STOP_ME: {
-        const double dme = c.pr[k] / 2.0;
-        if (it > 0 && dme / sqrt(c.p2[k]) <= c.taud[k]) {
-          st = true;
-          why = 3;
-        } else if (it >= kmax) {
-          st = true;
-        }
-        break;
+// The rule for instance k after its ||r_k||^2 is known; returns true when k stops.
+__device__ __forceinline__ bool batch_rule(int k, int initial, int64_t kmax, const BCtrl &c,
+                                           double nrm2, int *__restrict__ iters,
+                                           int *__restrict__ rule, double *__restrict__ resn) {
+  const int it = iters[k] + (initial ? 0 : 1);
+  iters[k] = it;
+  const double nrk = sqrt(nrm2);
+  resn[k] = nrk;
+  bool st = false;
+  int why = 0;
+  switch (c.rule) {
+    case AIRT_STOP_DP:
+      if (nrk <= c.taud[k] || it >= kmax) {
+        st = true;
+        why = it != kmax ? 2 : 0;
       }
-      case AIRT_STOP_NCP: {
-        double sum = 0.0;
-        const int j0 = c.col0[k], j1 = c.col0[k + 1];
-        for (int j = j0; j < j1; ++j) sum += c.ccol[j];
-        const double ncc = sum / (double)(j1 - j0);
-        double *dk = c.dk + (int64_t)k * c.ns;
-        double mx = -INFINITY, mxn = ncc;
-        for (int i = 0; i < c.ns; ++i) mx = fmax(mx, dk[i]);
-        for (int i = 1; i < c.ns; ++i) mxn = fmax(mxn, dk[i]);
-        if (mx < mxn || it >= kmax) {
-          st = true;
-          why = it != kmax ? 1 : 0;
-        } else {
-          for (int i = 0; i + 1 < c.ns; ++i) dk[i] = dk[i + 1];
-          dk[c.ns - 1] = ncc;
-        }
-        break;
+      break;
+    case AIRT_STOP_ME: {
+      const double dme = c.pr[k] / 2.0;
+      if (it > 0 && dme / sqrt(c.p2[k]) <= c.taud[k]) {
+        st = true;
+        why = 3;
+      } else if (it >= kmax) {
+        st = true;
       }
-      default:
-        st = it >= kmax;
+      break;
     }
-    if (st) {
-      stop[k] = 1;
-      rule[k] = why;
+    case AIRT_STOP_NCP: {
+      double sum = 0.0;
+      const int j0 = c.col0[k], j1 = c.col0[k + 1];
+      for (int j = j0; j < j1; ++j) sum += c.ccol[j];
+      const double ncc = sum / (double)(j1 - j0);
+      double *dk = c.dk + (int64_t)k * c.ns;
+      double mx = -INFINITY, mxn = ncc;
+      for (int i = 0; i < c.ns; ++i) mx = fmax(mx, dk[i]);
+      for (int i = 1; i < c.ns; ++i) mxn = fmax(mxn, dk[i]);
+      if (mx < mxn || it >= kmax) {
+        st = true;
+        why = it != kmax ? 1 : 0;
+      } else {
+        for (int i = 0; i + 1 < c.ns; ++i) dk[i] = dk[i + 1];
+        dk[c.ns - 1] = ncc;
+      }
+      break;
     }
+    default:
+      st = it >= kmax;
+  }
+  if (st) rule[k] = why;
+  return st;
+}
+
+// One block per unstopped instance: ||r_k||^2 (and the ME sums) in a fixed
+// order, then the instance's stopping rule; a stopping instance raises its
+// flag and takes itself off the active count the host polls.
+__global__ void __launch_bounds__(256) k_batch_step(const int64_t *__restrict__ roff,
+                                                    const double *__restrict__ rsq,
+                                                    const double *__restrict__ pp,
+                                                    const double *__restrict__ ppr,
+                                                    double *__restrict__ p2,
+                                                    double *__restrict__ pr, int initial,
+                                                    int64_t kmax, BCtrl c, int *__restrict__ stop,
+                                                    int *__restrict__ iters, int *__restrict__ rule,
+                                                    double *__restrict__ resn, int *active) {
+  const int k = blockIdx.x;
+  if (stop[k]) return;
+  double a = 0, e = 0, d = 0;
+  for (int64_t i = roff[k] + threadIdx.x; i < roff[k + 1]; i += blockDim.x) {
+    a += rsq[i];
+    if (pp) {
+      e += pp[i];
+      d += ppr[i];
+    }
+  }
+  a = block_sum<256>(a);
+  if (pp) {
+    e = block_sum<256>(e);
+    d = block_sum<256>(d);
+  }
+  if (threadIdx.x != 0) return;
+  if (pp) {
+    p2[k] = e;
+    pr[k] = d;
+  }
+  if (batch_rule(k, initial, kmax, c, a, iters, rule, resn)) {
+    stop[k] = 1;
+    atomicSub(active, 1);
   }
 }
 
@@ -939,12 +936,11 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
            me ? B.pr.p : nullptr, ncp ? B.ncp_ccol.p : nullptr, ncp ? B.ncp_col0.p : nullptr,
            ncp ? B.ncp_dk.p : nullptr, ncp_smooth};
   const bool poll = rule != AIRT_STOP_NONE;
-  const unsigned gk = (unsigned)((K + 127) / 128);
-  auto fwd_reduce = [&]() {
+  B.active.ensure(1);
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(B.active.p, &K, sizeof(int), cudaMemcpyHostToDevice, s));
+  // forward pass, NCP periodograms, then per instance the norm and the rule
+  auto fwd_step = [&](int initial) {
     fwd_classes(B, fo);
-    k_batch_reduce<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, B.stop.p, B.nrm2.p,
-                                     me ? B.pp.p : nullptr, me ? B.ppr.p : nullptr,
-                                     me ? B.p2.p : nullptr, me ? B.pr.p : nullptr);
     if (ncp && B.ncols > 0) {
       k_batch_ncp_power<<<B.ncols, 128, 0, s>>>(B.ncp_row0.p, B.ncp_L.p, B.ncp_tw0.p, B.ncp_pk0.p,
                                                 B.ncp_inst.p, B.stop.p, B.rprev.p, B.ncp_tw.p,
@@ -952,23 +948,25 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
       k_batch_ncp_col<<<B.ncols, 256, 0, s>>>(B.ncp_L.p, B.ncp_pk0.p, B.ncp_inst.p, B.stop.p,
                                               B.ncp_pk.p, B.ncp_ccol.p);
     }
+    k_batch_step<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, me ? B.pp.p : nullptr,
+                                   me ? B.ppr.p : nullptr, me ? B.p2.p : nullptr,
+                                   me ? B.pr.p : nullptr, initial, kmax, co, B.stop.p, B.iters.p,
+                                   B.rule.p, B.resn_last.p, B.active.p);
   };
   auto iteration = [&]() {
     bwd_classes(B, uo);
-    fwd_reduce();
-    k_batch_ctrl<<<gk, 128, 0, s>>>(K, 0, kmax, co, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
-                                    B.resn_last.p);
+    fwd_step(0);
     build_tiles(B, B.stop.p);
   };
-  fwd_reduce();
-  k_batch_ctrl<<<gk, 128, 0, s>>>(K, 1, kmax, co, B.nrm2.p, B.stop.p, B.iters.p, B.rule.p,
-                                  B.resn_last.p);
+  fwd_step(1);
   AIRT_LAUNCH_CHECK();
   build_tiles(B, B.stop.p);
   // A chunk of iterations is captured once as a CUDA graph and replayed:
   // every argument is fixed for the solve and the loop state lives in device
-  // memory.  The host reads the stop flags after each chunk.
+  // memory.  The host reads the active count of chunk c once chunk c+2 is
+  // queued (lagged poll), so the device never idles on the poll.
   const int64_t chunk = 8;
+  const int lag = 2;
   cudaGraphExec_t gexec = nullptr;
   if (kmax >= chunk) {
     cudaGraph_t g = nullptr;
@@ -981,8 +979,12 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
     }
     cudaGetLastError();
   }
-  std::vector<int> hstop(K);
-  for (int64_t it = 1; it <= kmax;) {
+  if (!P.h_state) AIRT_CHECK_CUDA(cudaMallocHost(&P.h_state, 3 * sizeof(SirtState)));
+  int *hact = reinterpret_cast<int *>(P.h_state);  // 3 poll slots in the pinned mirror
+  cudaEvent_t ev[3];
+  for (int q = 0; q < 3; ++q) AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming));
+  int64_t c = 0;
+  for (int64_t it = 1; it <= kmax; ++c) {
     const int64_t cnt = std::min<int64_t>(chunk, kmax - it + 1);
     if (cnt == chunk && gexec) {
       AIRT_CHECK_CUDA(cudaGraphLaunch(gexec, s));
@@ -992,12 +994,14 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
     AIRT_LAUNCH_CHECK();
     it += cnt;
     if (!poll) continue;
-    AIRT_CHECK_CUDA(cudaMemcpyAsync(hstop.data(), B.stop.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
-    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-    bool all = true;
-    for (int k = 0; k < K && all; ++k) all = hstop[k] != 0;
-    if (all) break;
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hact + (c % 3), B.active.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaEventRecord(ev[c % 3], s));
+    if (c >= lag) {
+      AIRT_CHECK_CUDA(cudaEventSynchronize(ev[(c - lag) % 3]));
+      if (hact[(c - lag) % 3] == 0) break;
+    }
   }
+  for (int q = 0; q < 3; ++q) cudaEventDestroy(ev[q]);
   if (gexec) cudaGraphExecDestroy(gexec);
   AIRT_CHECK_CUDA(cudaEventRecord(t1, s));
   AIRT_CHECK_CUDA(cudaMemcpyAsync(d_x, P.x64.p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));

@@ -219,7 +219,24 @@ __device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__r
       for (int64_t q = qb + lane; q < q1; q += LANES)
         a1 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a1);
       const int64_t ve = qb >> 2;
-      for (int64_t v = (qa >> 2) + lane; v < ve; v += LANES) {
+      int64_t v = (qa >> 2) + lane;
+      // two vectors per lane per round (both loads issued before the
+      // gathers), accumulated in the order of the one-vector loop
+      for (; v + LANES < ve; v += 2 * LANES) {
+        const float4 f = __ldg(V4 + v), h = __ldg(V4 + v + LANES);
+        const int4 c = __ldg(I4 + v), d = __ldg(I4 + v + LANES);
+        const TX g0 = __ldg(x + c.x), g1 = __ldg(x + c.y), g2 = __ldg(x + c.z), g3 = __ldg(x + c.w);
+        const TX k0 = __ldg(x + d.x), k1 = __ldg(x + d.y), k2 = __ldg(x + d.z), k3 = __ldg(x + d.w);
+        a0 = fma((double)f.x, (double)g0, a0);
+        a1 = fma((double)f.y, (double)g1, a1);
+        a2 = fma((double)f.z, (double)g2, a2);
+        a3 = fma((double)f.w, (double)g3, a3);
+        a0 = fma((double)h.x, (double)k0, a0);
+        a1 = fma((double)h.y, (double)k1, a1);
+        a2 = fma((double)h.z, (double)k2, a2);
+        a3 = fma((double)h.w, (double)k3, a3);
+      }
+      if (v < ve) {
         const float4 f = __ldg(V4 + v);
         const int4 c = __ldg(I4 + v);
         const TX g0 = __ldg(x + c.x), g1 = __ldg(x + c.y), g2 = __ldg(x + c.z), g3 = __ldg(x + c.w);
