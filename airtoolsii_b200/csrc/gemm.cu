@@ -358,6 +358,13 @@ extern "C" int airt_test_gemm_path(int path) {
   return AIRT_OK;
 }
 
+// Test hook: operand form of the TMA 3x3 convolution (see g_conv_halo).
+extern "C" int airt_test_conv_halo(int mode) {
+  if (mode < 0 || mode > 2) return AIRT_ERR_ARG;
+  airt::g_conv_halo = mode;
+  return AIRT_OK;
+}
+
 // Test hook: D = A * B^T through the tcgen05 kernel, device pointers.
 extern "C" int airt_test_gemm_bf16(int M, int N, int K, const void *A, int lda, int a_mn, const void *B,
                                    int ldb, int b_mn, float *D, int ldd, int bn, int ksplit,

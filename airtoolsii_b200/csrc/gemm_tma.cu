@@ -10,6 +10,17 @@
 //    as zero, which is the convolution's zero padding.  Stage k is tap
 //    k / (C/KS), channels (k % (C/KS))*KS.. +KS; the weights W[N][ldb] carry
 //    the same K index (tap*C + ci);
+//  * MODE_HALO: the same convolution for images whose rows hold whole
+//    128-pixel tiles (W % 128 == 0): instead of nine tap boxes per tile,
+//    each kernel row dh brings one strip of 130 pixels (the tile and one
+//    pixel either side) of image row h + dh - 1, and the three taps of that
+//    row read it shifted by 0, 1 and 2 pixel rows through the descriptor's
+//    start address (and matrix base offset, the phase of the swizzle
+//    pattern).  With 64-byte rows (32 channels) a one-row shift is not a
+//    whole 128-byte swizzle phase, so a second strip starting one pixel
+//    later serves the middle tap.  Per tile 3 (or 6) strips replace 9 boxes;
+//    a stage carries one kernel row (its strips and the three taps'
+//    weight slices);
 //  * MODE_WGRAD: the weight gradient of that convolution, both operands
 //    MN-major: A^T[pixel][tap*C + ci] gathered as 64-pixel boxes of X
 //    shifted per tap (one box per 64/32/16 channels of the 128-row M tile),
@@ -43,11 +54,17 @@ namespace {
 
 using namespace umma;
 
-enum { MODE_DENSE = 0, MODE_CONV = 1, MODE_WGRAD = 2 };
+enum { MODE_DENSE = 0, MODE_CONV = 1, MODE_WGRAD = 2, MODE_HALO = 3 };
+
+// Halo strips: rows (pixels) per strip, a multiple of 8 covering the 130
+// pixels a 128-pixel tile's taps read.
+constexpr int kStripRows = 136;
+constexpr int kStripBox = 130;
 
 struct TmaGeo {
   int W, H;                      // image width and height (CONV, WGRAD)
   int C;                         // channels of X (WGRAD)
+  int base_offset;               // HALO: set the descriptor's matrix base offset
   int cchunks;                   // C / KS (CONV)
   int tiles_m, tiles_n, splits;  // tile grid
   int K, ksplit;                 // K extent and K range per split (DENSE, WGRAD)
@@ -66,8 +83,15 @@ constexpr int ring_stages(uint32_t stage, bool two_per_sm) {
 template <int BN, int MODE, int SWA>
 struct TmaCfg {
   static constexpr bool MN = MODE == MODE_WGRAD;
-  static constexpr int KS = MN ? 64 : SWA / 2;  // K elements per stage
-  static constexpr uint32_t A_BYTES = BM * KS * 2, B_BYTES = BN * KS * 2;
+  static constexpr int KS = MN ? 64 : SWA / 2;  // K elements per stage (per tap for MODE_HALO)
+  static constexpr int STRIPS = SWA == 128 ? 1 : 2;
+  static constexpr uint32_t STRIP_BYTES = round1k((uint32_t)kStripRows * SWA);
+  static constexpr uint32_t A_BYTES = MODE == MODE_HALO ? STRIPS * STRIP_BYTES : BM * KS * 2;
+  static constexpr uint32_t B_BYTES = (MODE == MODE_HALO ? 3 : 1) * BN * KS * 2;
+  // bytes the TMA copies of one stage deliver (a halo strip is kStripBox
+  // rows of its kStripRows-row slot)
+  static constexpr uint32_t TX_BYTES =
+      MODE == MODE_HALO ? STRIPS * (uint32_t)kStripBox * SWA + B_BYTES : A_BYTES + B_BYTES;
   static constexpr uint32_t ST = round1k(A_BYTES + B_BYTES);
   static constexpr bool TWO = BN <= 128;  // TMEM: two CTAs x two accumulators x BN columns
   static constexpr int S = ring_stages(ST, TWO);
@@ -131,6 +155,9 @@ __device__ __forceinline__ TileCoord tile_coord(const TmaGeo &geo, int t) {
   if (MODE == MODE_CONV) {
     c.kb = 0;
     c.nk = 9 * geo.cchunks;
+  } else if (MODE == MODE_HALO) {
+    c.kb = 0;
+    c.nk = 3 * geo.cchunks;  // one stage per kernel row and channel chunk
   } else {
     c.kb = z * geo.ksplit;
     const int ke = min(geo.K, c.kb + geo.ksplit);
@@ -153,7 +180,7 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
                                                      TmaGeo geo) {
   using Cfg = TmaCfg<BN, MODE, SWA>;
   constexpr int S = Cfg::S, KS = Cfg::KS;
-  constexpr uint32_t A_BYTES = Cfg::A_BYTES, B_BYTES = Cfg::B_BYTES, ST = Cfg::ST;
+  constexpr uint32_t A_BYTES = Cfg::A_BYTES, ST = Cfg::ST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_addr(base);
@@ -197,7 +224,7 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
       for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
         const TileCoord tc = tile_coord<BN, MODE, SWA>(geo, t);
         int w0 = 0, h0 = 0, b0 = 0;
-        if (MODE == MODE_CONV) pixel_whb(tc.m0, geo.W, geo.H, w0, h0, b0);
+        if (MODE == MODE_CONV || MODE == MODE_HALO) pixel_whb(tc.m0, geo.W, geo.H, w0, h0, b0);
         for (int k = 0; k < tc.nk; ++k, ++it) {
           const uint32_t st = it % S;
           if (it >= (uint32_t)S && !mbar_wait(smem_addr(&empty[st]), ((it / S) - 1) & 1u)) {
@@ -206,7 +233,7 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
           }
           const uint32_t sa = sbase + st * ST, sb = sa + A_BYTES;
           const uint32_t bar = smem_addr(&full[st]);
-          expect_tx(bar, A_BYTES + B_BYTES);
+          expect_tx(bar, Cfg::TX_BYTES);
           if (MODE == MODE_DENSE) {
             const int kx = tc.kb + k * KS;
             tma2d(sa, &mapA, kx, tc.m0, bar);
@@ -215,6 +242,17 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
             const int tap = k / geo.cchunks, cc = k - tap * geo.cchunks;
             tma4d(sa, &mapA, cc * KS, w0 + tap % 3 - 1, h0 + tap / 3 - 1, b0, bar);
             tma2d(sb, &mapB, k * KS, tc.n0, bar);
+          } else if (MODE == MODE_HALO) {
+            // kernel row dh, channel chunk cc: strip(s) of image row h0 + dh - 1
+            // from pixel w0 - 1 (and w0), then the weights of taps 3dh .. 3dh+2
+            const int dh = k / geo.cchunks, cc = k - dh * geo.cchunks;
+#pragma unroll
+            for (int q = 0; q < Cfg::STRIPS; ++q)
+              tma4d(sa + q * Cfg::STRIP_BYTES, &mapA, cc * KS, w0 - 1 + q, h0 + dh - 1, b0, bar);
+#pragma unroll
+            for (int dw = 0; dw < 3; ++dw)
+              tma2d(sb + dw * (BN * KS * 2), &mapB, ((3 * dh + dw) * geo.cchunks + cc) * KS, tc.n0,
+                    bar);
           } else {
             constexpr int GA = SWA / 2, GB = SWB / 2;  // M / N elements per box
             const int p0 = tc.kb + k * KS;
@@ -258,19 +296,38 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t sa = sbase + st * ST, sb = sa + A_BYTES;
+          if constexpr (MODE == MODE_HALO) {
+            // tap dw reads the strip shifted by dw pixel rows: strip 0 at rows
+            // 0 and 2 (2-row shifts keep 64-byte rows on a swizzle phase), or,
+            // with 128-byte rows, at any row; strip 1 (64-byte rows) at row 0
 #pragma unroll
-          for (int kk = 0; kk < KS / 16; ++kk) {
-            uint64_t da, db;
-            if (MN) {
-              da = make_desc_sw<SWA>(sa + kk * 16 * SWA, 64 * SWA, 8 * SWA);
-              db = make_desc_sw<SWB>(sb + kk * 16 * SWB, 64 * SWB, 8 * SWB);
-            } else {
-              da = make_desc_sw<SWA>(sa + kk * 32, 16, 8 * SWA);
-              db = make_desc_sw<SWA>(sb + kk * 32, 16, 8 * SWA);
+            for (int dw = 0; dw < 3; ++dw) {
+              const uint32_t a0 = Cfg::STRIPS == 2 && dw == 1 ? sa + Cfg::STRIP_BYTES
+                                                              : sa + (uint32_t)dw * SWA;
+#pragma unroll
+              for (int kk = 0; kk < KS / 16; ++kk) {
+                uint64_t da = make_desc_sw<SWA>(a0 + kk * 32, 16, 8 * SWA);
+                if (geo.base_offset) da |= (uint64_t)(((a0 + kk * 32) >> 7) & 7u) << 49;
+                const uint64_t db = make_desc_sw<SWA>(sb + dw * (BN * KS * 2) + kk * 32, 16, 8 * SWA);
+                mma_bf16(dtm, da, db, idesc, (k > 0 || dw > 0 || kk > 0) ? 1u : 0u);
+              }
             }
-            mma_bf16(dtm, da, db, idesc, (k > 0 || kk > 0) ? 1u : 0u);
+            commit(smem_addr(&empty[st]));
+          } else {
+#pragma unroll
+            for (int kk = 0; kk < KS / 16; ++kk) {
+              uint64_t da, db;
+              if (MN) {
+                da = make_desc_sw<SWA>(sa + kk * 16 * SWA, 64 * SWA, 8 * SWA);
+                db = make_desc_sw<SWB>(sb + kk * 16 * SWB, 64 * SWB, 8 * SWB);
+              } else {
+                da = make_desc_sw<SWA>(sa + kk * 32, 16, 8 * SWA);
+                db = make_desc_sw<SWA>(sb + kk * 32, 16, 8 * SWA);
+              }
+              mma_bf16(dtm, da, db, idesc, (k > 0 || kk > 0) ? 1u : 0u);
+            }
+            commit(smem_addr(&empty[st]));
           }
-          commit(smem_addr(&empty[st]));
         }
         if (!ok) {
           *abort_flag = 1;
@@ -437,8 +494,38 @@ bool conv3x3_tma_ok(const GemmArgs &g) {
          g.ldb % 8 == 0 && g.M % (g.conv_H * g.conv_W) == 0 && pixel_box(128, g.conv_H, g.conv_W, bw, bh, bb);
 }
 
+int g_conv_halo = 0;
+
+// MODE_HALO launch: tiles lie within one image row (W % 128 == 0) and the
+// channels fill whole 64- or 128-byte rows.
+static bool conv3x3_halo(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
+  const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
+  const int sw = swizzle_for(C), ks = sw / 2;
+  if (!g_conv_halo || W % 128 != 0 || sw < 64 || W > 4096) return false;
+  const cuuint64_t dx[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
+  const cuuint64_t sx[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t bx[4] = {(cuuint32_t)ks, (cuuint32_t)kStripBox, 1, 1};
+  const CUtensorMap ma = make_map(g.convX, 4, dx, sx, bx, sw);
+  const cuuint64_t dw[2] = {(cuuint64_t)9 * C, (cuuint64_t)g.N}, swt[1] = {(cuuint64_t)g.ldb * 2};
+  const cuuint32_t bwt[2] = {(cuuint32_t)ks, (cuuint32_t)bn};
+  const CUtensorMap mb = make_map(g.B, 2, dw, swt, bwt, sw);
+  TmaGeo geo{};
+  geo.W = W;
+  geo.H = H;
+  geo.C = C;
+  geo.base_offset = g_conv_halo == 1;
+  geo.cchunks = C / ks;
+  geo.tiles_m = (g.M + BM - 1) / BM;
+  geo.tiles_n = (g.N + bn - 1) / bn;
+  geo.splits = 1;
+  if (sw == 128) dispatch_tma<MODE_HALO, 128, 128>(ma, mb, g, geo, bn, epi, s);
+  else dispatch_tma<MODE_HALO, 64, 64>(ma, mb, g, geo, bn, epi, s);
+  return true;
+}
+
 void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   AIRT_REQUIRE(conv3x3_tma_ok(g), "conv3x3: shape unsuitable for TMA");
+  if (conv3x3_halo(g, bn, epi, s)) return;
   const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
   const int sw = swizzle_for(C), ks = sw / 2;
   int bw, bh, bb;

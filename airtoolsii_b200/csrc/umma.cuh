@@ -282,5 +282,9 @@ bool conv3x3_wgrad_tma_ok(const GemmArgs &g);
 void conv3x3_wgrad_bf16_tma(const GemmArgs &g, int bn, cudaStream_t s);
 // Operand path: 0 = TMA where possible, 1 = always cp.async (a test switch).
 extern int g_gemm_path;
+// 3x3 convolution operand form on the TMA path: 0 = nine tap boxes per
+// tile, 1 = halo strips (W % 128 == 0) with the descriptor base offset,
+// 2 = halo strips without it (a layout check).
+extern int g_conv_halo;
 
 }  // namespace airt

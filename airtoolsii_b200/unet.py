@@ -130,15 +130,21 @@ class UNet:
 
 
 def _timing_main():
-    """python -m airtoolsii_b200.unet [--batch B] [--reps R]: device time per
-    image of the forward pass and of one Adam training step of the N=256,
-    4-level, base-32 network (random inputs), CUDA events on its stream."""
+    """python -m airtoolsii_b200.unet [--batch B] [--reps R] [--conv tap|halo]:
+    device time per image of the forward pass and of one Adam training step
+    of the N=256, 4-level, base-32 network (random inputs), CUDA events on
+    its stream; --conv picks the operand form of the TMA 3x3 convolutions."""
     import argparse
     import torch
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--conv", choices=["default", "tap", "halo"], default="default")
     a = ap.parse_args()
+    if a.conv != "default":
+        f = lib().airt_test_conv_halo
+        f.restype, f.argtypes = C.c_int, [C.c_int]
+        check(f(1 if a.conv == "halo" else 0))
     B = a.batch
     net = UNet(256, 256, 32, 4, B, 0)
     u = torch.rand(B, 65536, device="cuda")
@@ -162,7 +168,7 @@ def _timing_main():
         net.train_step(u.data_ptr(), t.data_ptr(), B, 1e-4)
     e1.record(s)
     torch.cuda.synchronize()
-    print({"forward_ms_per_image": round(fwd, 5),
+    print({"conv": a.conv, "forward_ms_per_image": round(fwd, 5),
            "train_ms_per_image": round(e0.elapsed_time(e1) / a.reps / B, 5)})
 
 
