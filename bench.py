@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-extra", action="store_true", help="skip the C2-methods / C3 / C4 legs")
     ap.add_argument("--warm-heldout", type=int, default=1000, help="held-out seeds of the time-to-DP leg")
     ap.add_argument("--warm-batch", type=int, default=250, help="instances per batched solve")
+    ap.add_argument("--leg", choices=["kaczmarz", "multi"], default=None,
+                    help="only one small leg, for profiling captures: 'kaczmarz' = 3 kaczmarz "
+                         "sweeps on paralleltomo N=256, 180 angles; 'multi' = cimmino to the DP "
+                         "stop on 250 right-hand sides of paralleltomo N=256, 60 angles")
     ap.add_argument("--mf-only", action="store_true",
                     help="only the matrix-free projector leg: --iters iterations of --method on the "
                          "matrix-free operator of the (--small) paralleltomo workload (profiling)")
@@ -463,6 +467,43 @@ def warm_leg(a):
     return out
 
 
+def small_leg(which):
+    """One small workload for profiling captures; prints one JSON line with
+    its device time.  kaczmarz: paralleltomo N=256, 180 angles, 10-ellipse
+    phantom, 1% noise, 3 sweeps after a 1-sweep untimed pass.  multi: the
+    warm-start geometry (N=256, 60 angles) with 250 seeded sinograms at 2%
+    noise, cimmino to the per-instance DP stop (tau 1.02) on the
+    multi-right-hand-side engine, after an untimed pass."""
+    import torch
+    import airtoolsii_b200 as airt
+    from airtoolsii_b200.batch import sirt_multi_device
+    if which == "kaczmarz":
+        A, *_ = airt.paralleltomo(256, np.arange(180.0))
+        x = airt.random_ellipses(256, 10, seed=31)
+        b, _ = airt.add_noise(A(x, "notransp"), 0.01, seed=32)
+        airt.kaczmarz(A, b, [1])
+        X, info = airt.kaczmarz(A, b, [3])
+        print(json.dumps({"leg": which, "ms_per_sweep": round(info["gpu_ms"] / 3, 4)}), flush=True)
+        return
+    A, *_ = airt.paralleltomo(256, np.arange(60) * 3.0)
+    K = 250
+    xs = np.stack([airt.random_ellipses(256, 10, seed=600 + k) for k in range(K)])
+    bs, tds = [], []
+    for k in range(K):
+        bk, ek = airt.add_noise(A(xs[k], "notransp"), 0.02, seed=900 + k)
+        bs.append(bk)
+        tds.append(1.02 * ek)
+    dB = torch.from_numpy(np.stack(bs)).cuda()
+    dX = torch.empty((K, A.n), dtype=torch.float64, device="cuda")
+    sirt_multi_device(A, "cimmino", dB.data_ptr(), dX.data_ptr(), K, 2000, taudelta=tds)
+    info = sirt_multi_device(A, "cimmino", dB.data_ptr(), dX.data_ptr(), K, 2000, taudelta=tds)
+    its = info["finaliter"]
+    print(json.dumps({"leg": which, "instances": K, "gpu_ms": round(info["gpu_ms"], 3),
+                      "iters_mean": round(float(its.mean()), 2), "iters_max": int(its.max()),
+                      "ms_per_iteration": round(info["gpu_ms"] / max(int(its.max()), 1), 4)}),
+          flush=True)
+
+
 def mf_leg(a, wl):
     """The matrix-free projector alone: `iters` iterations of `method` (box
     [0,1]) on the matrix-free paralleltomo operator of the workload, after a
@@ -518,6 +559,9 @@ def main():
     from airtoolsii_b200 import dist as D
     from airtoolsii_b200.testprobs import parallel_operator, parallel_tables
 
+    if a.leg:
+        small_leg(a.leg)
+        return
     if a.mf_only:
         mf_leg(a, wl)
         return
