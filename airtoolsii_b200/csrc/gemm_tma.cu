@@ -501,7 +501,9 @@ int g_conv_halo = 0;
 static bool conv3x3_halo(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
   const int sw = swizzle_for(C), ks = sw / 2;
-  if (!g_conv_halo || W % 128 != 0 || sw < 64 || W > 4096) return false;
+  // the three taps' weight slices of a stage stay within 24 KB, so that two
+  // CTAs per SM keep at least two stages each
+  if (!g_conv_halo || W % 128 != 0 || sw < 64 || W > 4096 || 3 * bn * sw > 24576) return false;
   const cuuint64_t dx[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
   const cuuint64_t sx[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
   const cuuint32_t bx[4] = {(cuuint32_t)ks, (cuuint32_t)kStripBox, 1, 1};
