@@ -16,8 +16,9 @@
 //         gather (0 for stopped instances), per-block partial ||r_k||^2;
 //   ctrl: one block per instance sums the partials in a fixed order and
 //         applies check_stoprules.m's DP rule (or kmax) to that instance.
-// A lane owns 8 consecutive instances; a group of G = Kp/8 lanes (Kp = K
-// rounded up to 8, at most 256 per pass) walks one row or column.  All sums
+// A lane owns 8 consecutive instances; a group of G lanes (G the smallest
+// power of two with 8G >= K, Kp = 8G slots, at most 256 per pass) walks one
+// row or column.  All sums
 // run in a fixed order, so results repeat bit for bit.  Matrix values and
 // the gathered vectors are FP32, accumulation and the iterates FP64, as in
 // the single-problem loop.
@@ -266,8 +267,10 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
                 int *stoprule) {
   cudaStream_t s = P.stream;
   const int64_t m = P.m, n = P.n, kmax = o.kmax;
-  const int Kp = (K + 7) / 8 * 8;
-  const int G = group_for(Kp);
+  // every lane of a group owns 8 slots, so the slot count is 8G (G a power
+  // of two): no lane reads or writes past its row
+  const int G = group_for((K + 7) / 8 * 8);
+  const int Kp = 8 * G;
   P.mr_b.ensure((size_t)m * Kp);
   P.mr_x64.ensure((size_t)n * Kp);
   P.mr_x32.ensure((size_t)n * Kp);
