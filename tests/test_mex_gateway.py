@@ -115,6 +115,8 @@ class Mex:
         if cls is None:
             a = a.astype(np.float64)
             cls = DOUBLE
+        if a.size == 0:
+            return L.fm_numeric(cls, 0, 0, None)
         a2 = a.reshape(a.shape[0], -1) if a.ndim >= 1 else a.reshape(1, 1)
         if a.ndim == 1:
             a2 = a.reshape(-1, 1)
