@@ -65,7 +65,15 @@ long long g_kacz_wait_budget = 4000000000ll;
 int g_kacz_inject_stall = 0;
 
 constexpr int kDagCache = 16;  // entries per lane kept in registers (rows <= 512)
-constexpr int kDagThreads = 256;
+// Warps per CTA of the sweep kernel (one CTA per SM) and the pause between
+// two polls of an unfinished predecessor (0: none).
+#ifndef AIRT_KACZ_WARPS
+#define AIRT_KACZ_WARPS 8
+#endif
+#ifndef AIRT_KACZ_BACKOFF_NS
+#define AIRT_KACZ_BACKOFF_NS 0
+#endif
+constexpr int kDagThreads = 32 * AIRT_KACZ_WARPS;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   unsigned v;
@@ -114,6 +122,7 @@ __global__ void __launch_bounds__(kDagThreads, 1)
       const unsigned *f = pi < p1 ? done + __ldg(preds + pi) : done + q;  // stall: own stamp
       const unsigned want = pi < p1 ? stamp : stamp + 1u;
       while (ld_acquire_u32(f) < want) {
+        if (AIRT_KACZ_BACKOFF_NS > 0) __nanosleep(AIRT_KACZ_BACKOFF_NS);
         if (*(volatile int *)err) {
           ok = false;
           break;
