@@ -219,11 +219,17 @@ __global__ void k_copy_d(int64_t n, const double *__restrict__ a, double *__rest
     b[i] = a[i];
 }
 
-struct Schedule {
-  int nlev = 0;
-  int64_t nsteps = 0;
-  DevBuf<int> steps, pos, pred_ptr, preds;
-};
+using Schedule = ArtSchedule;
+
+// FNV-1a hash of a row order (the key of the cached schedule; never 0).
+uint64_t order_key(const int64_t *order, int64_t nsteps) {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)nsteps;
+  for (int64_t t = 0; t < nsteps; ++t) {
+    h ^= (uint64_t)order[t];
+    h *= 1099511628211ull;
+  }
+  return h ? h : 1;
+}
 
 // Level schedule of a row order (see the file comment): steps sorted by
 // level (stable), each with the distinct last earlier writers of its pixels
@@ -351,17 +357,30 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
   AIRT_REQUIRE(o.order_kind != 2 || stride == 0 || (int64_t)order.size() == per_sweep * kmax,
                "each sweep of the row stream must keep the same number of nonzero rows");
 
-  // host copy of the sparsity pattern for the level schedule
-  std::vector<int64_t> hrp(m + 1);
-  std::vector<int> hci(P.nnz);
-  AIRT_CHECK_CUDA(cudaMemcpyAsync(hrp.data(), P.rp.p, (m + 1) * sizeof(int64_t),
-                                  cudaMemcpyDeviceToHost, s));
-  if (P.nnz)
-    AIRT_CHECK_CUDA(cudaMemcpyAsync(hci.data(), P.ci.p, P.nnz * sizeof(int), cudaMemcpyDeviceToHost, s));
-  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-  Schedule S;
+  // the schedule of a fixed order is kept in the problem and rebuilt only for
+  // a new order; per-sweep orders (a row stream) get one per sweep
   const bool per_sweep_sched = (o.order_kind == 2 && stride > 0);
-  if (!per_sweep_sched) build_schedule(hrp, hci, order.data(), per_sweep, n, S, s);
+  Schedule local;
+  Schedule &S = per_sweep_sched ? local : P.art_sched;
+  const uint64_t key = per_sweep_sched ? 0 : order_key(order.data(), per_sweep);
+  const bool need_pattern = per_sweep_sched || S.key != key || S.nsteps != per_sweep;
+  // host copy of the sparsity pattern, only when a schedule is built
+  std::vector<int64_t> hrp;
+  std::vector<int> hci;
+  if (need_pattern) {
+    hrp.resize(m + 1);
+    hci.resize(P.nnz);
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hrp.data(), P.rp.p, (m + 1) * sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, s));
+    if (P.nnz)
+      AIRT_CHECK_CUDA(cudaMemcpyAsync(hci.data(), P.ci.p, P.nnz * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  }
+  if (!per_sweep_sched && need_pattern) {
+    S.key = 0;
+    build_schedule(hrp, hci, order.data(), per_sweep, n, S, s);
+    S.key = key;
+  }
 
   // iterate
   P.x64.ensure(n);
@@ -457,7 +476,10 @@ void run_art(Problem &P, const airt_art_opts &o, const double *d_b, const double
     if (per_sweep_sched) build_schedule(hrp, hci, ord, per_sweep, n, S, s);
     if (k == 1 && bounded && per_sweep > 0) {
       const int64_t r0 = ord[0];
-      const int64_t len = hrp[r0 + 1] - hrp[r0];
+      int64_t rr[2];
+      AIRT_CHECK_CUDA(cudaMemcpyAsync(rr, P.rp.p + r0, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+      const int64_t len = rr[1] - rr[0];
       keep.ensure(std::max<int64_t>(len, 1));
       k_preclamp<<<1, 1024, 0, s>>>(n, (int)r0, keep.p, a);
     }

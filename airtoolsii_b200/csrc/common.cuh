@@ -160,6 +160,15 @@ struct SirtParams {
   int ncp_cols, ncp_smooth;
 };
 
+// Dependency schedule of a Kaczmarz row order (art.cu): the steps sorted by
+// level, their positions in the order, and each step's predecessors.
+struct ArtSchedule {
+  int nlev = 0;
+  int64_t nsteps = 0;
+  uint64_t key = 0;  // hash of the row order it was built for (0: none)
+  DevBuf<int> steps, pos, pred_ptr, preds;
+};
+
 // ---------------------------------------------------------------- problem
 struct Problem {
   int64_t m = 0, n = 0, nnz = 0;
@@ -203,6 +212,9 @@ struct Problem {
   // custom SIRT weights given as full matrices (get_mfun_dfun.m:252-307, flag 2):
   // column-major m x m / n x n, and the column sums of D (line search)
   DevBuf<double> Mfull, Dfull, Dcol, dscratch;
+  // Kaczmarz schedule of the last fixed row order (kept between calls: the
+  // matrix never changes, so the same order gives the same schedule)
+  ArtSchedule art_sched;
   // multi-right-hand-side SIRT (multirhs.cu): interleaved [row or pixel][instance]
   DevBuf<double> mr_b, mr_x64, mr_part, mr_resn, mr_taud, mr_lam;
   DevBuf<float> mr_x32, mr_r32;

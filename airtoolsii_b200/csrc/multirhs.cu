@@ -64,7 +64,26 @@ __device__ __forceinline__ void seg_dot(int64_t q0, int64_t q1, const int *__res
                                         double acc[8]) {
 #pragma unroll
   for (int s = 0; s < 8; ++s) acc[s] = 0.0;
-  for (int64_t q = q0; q < q1; ++q) {
+  int64_t q = q0;
+  // four nonzeros per round: their indices, values and gathers are all in
+  // flight before the first FMA; the FMAs run in nonzero order
+  for (; q + 4 <= q1; q += 4) {
+    int c[4];
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      c[u] = __ldg(idx + q + u);
+      v[u] = __ldg(val + q + u);
+    }
+    float g[4][8];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) load8(vec + (int64_t)c[u] * Kp + 8 * lane, g[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int s = 0; s < 8; ++s) acc[s] = fma((double)v[u], (double)g[u][s], acc[s]);
+  }
+  for (; q < q1; ++q) {
     const int c = __ldg(idx + q);
     const double v = (double)__ldg(val + q);
     float g[8];
@@ -96,7 +115,7 @@ __device__ __forceinline__ void block_partials(double part[8], double *__restric
 
 // R = B - A*X, M.*R (FP32, 0 for stopped instances), per-block ||r_k||^2.
 template <int G>
-__global__ void __launch_bounds__(kMrThreads) k_mr_fwd(int64_t m, const int64_t *__restrict__ rp,
+__global__ void __launch_bounds__(kMrThreads, 2) k_mr_fwd(int64_t m, const int64_t *__restrict__ rp,
                                                        const int *__restrict__ ci,
                                                        const float *__restrict__ rv, MrArgs a) {
   if (a.st->active == 0) return;
@@ -129,7 +148,7 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_fwd(int64_t m, const int64_t 
 
 // g = A'*(M.*R); x += lam*D.*g, box projection, FP32 copy (running instances).
 template <int G>
-__global__ void __launch_bounds__(kMrThreads) k_mr_bwd(int64_t n, const int64_t *__restrict__ cp,
+__global__ void __launch_bounds__(kMrThreads, 2) k_mr_bwd(int64_t n, const int64_t *__restrict__ cp,
                                                        const int *__restrict__ ri,
                                                        const float *__restrict__ cv, MrArgs a) {
   if (a.st->active == 0) return;

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kStreamThreads, kStreamCtasPerSm)
 }
 
 template <bool ME>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(64)
     k_sirt_fwd_mf(RayGeom g, int64_t nrays, bool excl, const float *__restrict__ x32, FwdOut o) {
   if (stopped(o.st)) return;
   Acc4 a;
@@ -143,12 +143,13 @@ __global__ void __launch_bounds__(128)
     });
     resid_row<ME>(r, acc, o, a);
   }
-  double r2 = block_sum<128>(a.r2), rmr = block_sum<128>(a.rmr), p2 = 0, pr = 0;
+  // warp sums (no block barrier: a warp whose rays are short leaves at once)
+  double r2 = warp_sum(a.r2), rmr = warp_sum(a.rmr), p2 = 0, pr = 0;
   if (ME) {
-    p2 = block_sum<128>(a.p2);
-    pr = block_sum<128>(a.pr);
+    p2 = warp_sum(a.p2);
+    pr = warp_sum(a.pr);
   }
-  if (threadIdx.x == 0) {
+  if ((threadIdx.x & 31) == 0) {
     atomicAdd(&o.st->acc[0], r2);
     atomicAdd(&o.st->acc[1], rmr);
     if (ME) {
@@ -488,7 +489,7 @@ void launch_fwd_t(Problem &P, const FwdOut &o) {
     return;
   }
   if (P.matrix_free) {
-    k_sirt_fwd_mf<ME><<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m,
+    k_sirt_fwd_mf<ME><<<grid_for(P.m, 64, 32), 64, 0, s>>>(P.geom(), P.m,
                                                               P.geo_kind == GEO_PARALLEL,
                                                               P.x32.p, o);
     return;

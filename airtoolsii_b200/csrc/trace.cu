@@ -303,7 +303,7 @@ void mf_backproject_f32(Problem &P, const float *u, double *g64, const int *stop
   AIRT_CHECK_CUDA(cudaMemsetAsync(g64, 0, P.n * sizeof(double), s));
   AIRT_CHECK_CUDA(cudaMemsetAsync(P.mf_umax.p, 0, sizeof(unsigned long long), s));
   k_absmax<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, nullptr, u, P.mf_umax.p, stop_flag);
-  k_mf_adjoint_fx<float><<<grid_for(P.m, 128, 16), 128, 0, s>>>(
+  k_mf_adjoint_fx<float><<<grid_for(P.m, 64, 32), 64, 0, s>>>(
       P.geom(), P.m, excl_of(P), u, reinterpret_cast<long long *>(g64), P.mf_kbound, P.mf_umax.p,
       stop_flag);
   k_fx_to_f64<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, g64, P.mf_kbound, P.mf_umax.p, stop_flag);

@@ -125,6 +125,8 @@ class Mex:
 
     # ---- mxArray -> Python
     def val(self, p):
+        if not p:                        # the command set no output
+            return None
         L = self.L
         cls, m, n = L.fm_class(p), L.fm_m(p), L.fm_n(p)
         if L.fm_is_sparse(p):
