@@ -1,6 +1,6 @@
 // tcgen05 GEMM with TMA operand loads, persistent and warp-specialised.
 //
-// Three operand sources share one kernel:
+// Four operand sources (three in k_gemm_tma, one in k_conv_rows):
 //  * MODE_DENSE: A [M][lda] and B [N][ldb] row-major bf16 matrices
 //    (K-major), 2D tensor maps, boxes {64, 128} and {64, BN};
 //  * MODE_CONV: the implicit 3x3 convolution of an NHWC bf16 image X
@@ -15,12 +15,14 @@
 //    each kernel row dh brings one strip of 130 pixels (the tile and one
 //    pixel either side) of image row h + dh - 1, and the three taps of that
 //    row read it shifted by 0, 1 and 2 pixel rows through the descriptor's
-//    start address (and matrix base offset, the phase of the swizzle
-//    pattern).  With 64-byte rows (32 channels) a one-row shift is not a
-//    whole 128-byte swizzle phase, so a second strip starting one pixel
-//    later serves the middle tap.  Per tile 3 (or 6) strips replace 9 boxes;
-//    a stage carries one kernel row (its strips and the three taps'
-//    weight slices);
+//    start address (the swizzle pattern follows the shared-memory address,
+//    so the descriptor's base offset stays 0).  With 64-byte rows (32
+//    channels) a one-row shift is not a whole 128-byte swizzle phase, so a
+//    second strip starting one pixel later serves the middle tap.  Per tile
+//    3 (or 6) strips replace 9 boxes; a stage carries one kernel row (its
+//    strips and the three taps' weight slices);
+//  * row runs (k_conv_rows, below): the halo strips of an input row loaded
+//    once for the three output rows that read it, weights resident;
 //  * MODE_WGRAD: the weight gradient of that convolution, both operands
 //    MN-major: A^T[pixel][tap*C + ci] gathered as 64-pixel boxes of X
 //    shifted per tap (one box per 64/32/16 channels of the 128-row M tile),
@@ -64,7 +66,6 @@ constexpr int kStripBox = 130;
 struct TmaGeo {
   int W, H;                      // image width and height (CONV, WGRAD)
   int C;                         // channels of X (WGRAD)
-  int base_offset;               // HALO: set the descriptor's matrix base offset
   int cchunks;                   // C / KS (CONV)
   int tiles_m, tiles_n, splits;  // tile grid
   int K, ksplit;                 // K extent and K range per split (DENSE, WGRAD)
@@ -306,8 +307,7 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
                                                               : sa + (uint32_t)dw * SWA;
 #pragma unroll
               for (int kk = 0; kk < KS / 16; ++kk) {
-                uint64_t da = make_desc_sw<SWA>(a0 + kk * 32, 16, 8 * SWA);
-                if (geo.base_offset) da |= (uint64_t)(((a0 + kk * 32) >> 7) & 7u) << 49;
+                const uint64_t da = make_desc_sw<SWA>(a0 + kk * 32, 16, 8 * SWA);
                 const uint64_t db = make_desc_sw<SWA>(sb + dw * (BN * KS * 2) + kk * 32, 16, 8 * SWA);
                 mma_bf16(dtm, da, db, idesc, (k > 0 || dw > 0 || kk > 0) ? 1u : 0u);
               }
@@ -353,6 +353,203 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
                              tc.n0, tc.nk > 0);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive_plain(smem_addr(&acc_empty[buf]));
+    }
+  }
+  __syncthreads();
+  if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * BN)));
+}
+
+// ---------------------------------------------------------------- row runs
+// The 3x3 convolution of images whose rows hold whole 128-pixel segments,
+// walked as runs of R consecutive output rows of one segment.  Each input
+// row of a run is loaded once (as the halo strips of MODE_HALO: 130 pixels,
+// one either side; with 64-byte pixel rows a second strip one pixel later),
+// so R + 2 input rows serve R output rows where MODE_HALO loads three per
+// output row, and the nine taps' weight slices are loaded once per CTA and
+// stay resident.  One ring stage holds one input row (all channel chunks);
+// output row i of a run reads the stages of input rows i, i+1 and i+2, and
+// input row i is released once output row i's MMAs complete (it is the last
+// row to read it).  Requires N == BN (one output-channel tile).
+struct RowsGeo {
+  int W, H, R;             // image width, height; output rows per run
+  int segs, hblocks;       // 128-pixel segments per row; runs per column
+  int nunits;              // Bimg * segs * hblocks
+  int cch;                 // channel chunks, C / KS
+  int S;                   // ring stages
+  uint32_t stage_bytes;    // one input row: cch * strips strips
+  uint32_t w_bytes;        // resident weights: 9 * cch slices of BN x KS
+};
+
+constexpr int kRowsMaxStages = 8;
+
+template <int SWA>
+struct RowsCfg {
+  static constexpr int KS = SWA / 2;
+  static constexpr int STRIPS = SWA == 128 ? 1 : 2;
+  static constexpr uint32_t STRIP_BYTES = round1k((uint32_t)kStripRows * SWA);
+};
+
+struct RowsUnit {
+  int w0, h0, b, rows;
+};
+
+__device__ __forceinline__ RowsUnit rows_unit(const RowsGeo &geo, int u) {
+  RowsUnit r;
+  const int hb = u % geo.hblocks, q = u / geo.hblocks;
+  r.w0 = (q % geo.segs) * 128;
+  r.b = q / geo.segs;
+  r.h0 = hb * geo.R;
+  r.rows = min(geo.R, geo.H - r.h0);
+  return r;
+}
+
+template <int BN, int EPI, int SWA>
+__global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CUtensorMap mapA,
+                                                      const __grid_constant__ CUtensorMap mapB, GemmArgs g,
+                                                      RowsGeo geo) {
+  using Cfg = RowsCfg<SWA>;
+  constexpr int KS = Cfg::KS, STRIPS = Cfg::STRIPS;
+  constexpr uint32_t STRIP = Cfg::STRIP_BYTES;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t wbase = smem_addr(base);  // resident weights (w_bytes, a multiple of 1 KB)
+  const uint32_t rbase = wbase + geo.w_bytes;
+  __shared__ __align__(8) uint64_t full[kRowsMaxStages], empty[kRowsMaxStages], acc_full[2], acc_empty[2], wfull;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  volatile int *abort_flag = &s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = geo.S;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&s_tmem)),
+                 "r"((uint32_t)(2 * BN)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int i = 0; i < S; ++i) {
+      mbar_init(smem_addr(&full[i]), 1);
+      mbar_init(smem_addr(&empty[i]), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(smem_addr(&acc_full[i]), 1);
+      mbar_init(smem_addr(&acc_empty[i]), 128);
+    }
+    mbar_init(smem_addr(&wfull), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&mapA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&mapB) : "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer: the weights once, then one stage per input row
+      const uint32_t wb = smem_addr(&wfull);
+      expect_tx(wb, geo.w_bytes);
+      for (int j = 0; j < 9 * geo.cch; ++j) tma2d(wbase + (uint32_t)j * (BN * SWA), &mapB, j * KS, 0, wb);
+      const uint32_t tx = (uint32_t)(geo.cch * STRIPS * kStripBox * SWA);
+      uint32_t it = 0;
+      for (int u = blockIdx.x; u < geo.nunits && !*abort_flag; u += gridDim.x) {
+        const RowsUnit ru = rows_unit(geo, u);
+        bool ok = true;
+        for (int r = 0; r < ru.rows + 2; ++r, ++it) {
+          const uint32_t st = it % S;
+          if (it >= (uint32_t)S && !mbar_wait(smem_addr(&empty[st]), ((it / S) - 1) & 1u)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = rbase + st * geo.stage_bytes, bar = smem_addr(&full[st]);
+          expect_tx(bar, tx);
+          for (int cc = 0; cc < geo.cch; ++cc)
+#pragma unroll
+            for (int q = 0; q < STRIPS; ++q)
+              tma4d(sa + (uint32_t)(cc * STRIPS + q) * STRIP, &mapA, cc * KS, ru.w0 - 1 + q, ru.h0 - 1 + r, ru.b,
+                    bar);
+        }
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      constexpr uint32_t idesc = make_idesc<BN, false, false>();
+      bool ok = mbar_wait(smem_addr(&wfull), 0);
+      uint32_t it = 0, ol = 0;
+      for (int u = blockIdx.x; ok && u < geo.nunits && !*abort_flag; u += gridDim.x) {
+        const RowsUnit ru = rows_unit(geo, u);
+        for (int r = 0; r < 2 && ok; ++r) ok = mbar_wait(smem_addr(&full[(it + r) % S]), ((it + r) / S) & 1u);
+        for (int i = 0; ok && i < ru.rows; ++i, ++ol) {
+          const uint32_t sr = it + i + 2;
+          const uint32_t buf = ol & 1u;
+          if (!mbar_wait(smem_addr(&full[sr % S]), (sr / S) & 1u) ||
+              (ol >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((ol >> 1) - 1) & 1u))) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t dtm = tmem + buf * BN;
+          for (int dh = 0; dh < 3; ++dh) {
+            const uint32_t sa = rbase + ((it + i + dh) % S) * geo.stage_bytes;
+            for (int cc = 0; cc < geo.cch; ++cc) {
+              const uint32_t ca = sa + (uint32_t)(cc * STRIPS) * STRIP;
+              // tap dw reads the strip shifted by dw pixel rows (strip 1 for
+              // the middle tap when pixel rows are 64 bytes: see MODE_HALO)
+#pragma unroll
+              for (int dw = 0; dw < 3; ++dw) {
+                const uint32_t a0 = STRIPS == 2 && dw == 1 ? ca + STRIP : ca + (uint32_t)dw * SWA;
+                const uint32_t b0 = wbase + (uint32_t)((3 * dh + dw) * geo.cch + cc) * (BN * SWA);
+#pragma unroll
+                for (int kk = 0; kk < KS / 16; ++kk) {
+                  const uint64_t da = make_desc_sw<SWA>(a0 + kk * 32, 16, 8 * SWA);
+                  const uint64_t db = make_desc_sw<SWA>(b0 + kk * 32, 16, 8 * SWA);
+                  mma_bf16(dtm, da, db, idesc, (dh > 0 || cc > 0 || dw > 0 || kk > 0) ? 1u : 0u);
+                }
+              }
+            }
+          }
+          commit(smem_addr(&acc_full[buf]));
+          commit(smem_addr(&empty[(it + i) % S]));  // input row i: output row i was its last reader
+        }
+        if (!ok) break;
+        commit(smem_addr(&empty[(it + ru.rows) % S]));
+        commit(smem_addr(&empty[(it + ru.rows + 1) % S]));
+        it += ru.rows + 2;
+      }
+      if (!ok) *abort_flag = 1;
+    }
+  } else {
+    // ---- epilogue warps 2-5: one output row (128 pixels) per accumulator
+    const int quad = warp & 3;
+    uint32_t ol = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; ok && u < geo.nunits; u += gridDim.x) {
+      const RowsUnit ru = rows_unit(geo, u);
+      for (int i = 0; i < ru.rows; ++i, ++ol) {
+        const uint32_t buf = ol & 1u;
+        if (!mbar_wait(smem_addr(&acc_full[buf]), (ol >> 1) & 1u)) {
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int m0 = ((ru.b * geo.H + ru.h0 + i) * geo.W) + ru.w0;
+        gemm_epilogue<BN, EPI>(g, tmem + ((uint32_t)(quad * 32) << 16) + buf * BN, m0 + quad * 32 + lane, 0,
+                               true);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive_plain(smem_addr(&acc_empty[buf]));
+      }
     }
   }
   __syncthreads();
@@ -494,7 +691,7 @@ bool conv3x3_tma_ok(const GemmArgs &g) {
          g.ldb % 8 == 0 && g.M % (g.conv_H * g.conv_W) == 0 && pixel_box(128, g.conv_H, g.conv_W, bw, bh, bb);
 }
 
-int g_conv_halo = 0;
+int g_conv_halo = 2;
 
 // MODE_HALO launch: tiles lie within one image row (W % 128 == 0) and the
 // channels fill whole 64- or 128-byte rows.
@@ -515,7 +712,6 @@ static bool conv3x3_halo(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   geo.W = W;
   geo.H = H;
   geo.C = C;
-  geo.base_offset = g_conv_halo == 1;
   geo.cchunks = C / ks;
   geo.tiles_m = (g.M + BM - 1) / BM;
   geo.tiles_n = (g.N + bn - 1) / bn;
@@ -525,8 +721,89 @@ static bool conv3x3_halo(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   return true;
 }
 
+template <int BN, int EPI, int SWA>
+static void launch_rows(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, const RowsGeo &geo,
+                        size_t smem, int ctas, cudaStream_t s) {
+  auto kern = k_conv_rows<BN, EPI, SWA>;
+  AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ctas, 192, smem, s>>>(ma, mb, g, geo);
+  AIRT_LAUNCH_CHECK();
+}
+
+// Row-run launch (k_conv_rows): W % 128 == 0, 64- or 128-byte pixel rows, one
+// output-channel tile, and the resident weights plus four ring stages within
+// the shared memory of one CTA (two per SM when that fits in half).
+static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
+  const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
+  const int sw = swizzle_for(C), ks = sw / 2;
+  if (g_conv_halo != 2 || W % 128 != 0 || sw < 64 || W > 4096 || g.N != bn || bn > 128) return false;
+  RowsGeo geo{};
+  geo.W = W;
+  geo.H = H;
+  geo.cch = C / ks;
+  const uint32_t strip = round1k((uint32_t)kStripRows * sw);
+  geo.stage_bytes = (uint32_t)geo.cch * (sw == 128 ? 1u : 2u) * strip;
+  geo.w_bytes = (uint32_t)(9 * geo.cch) * (uint32_t)bn * (uint32_t)sw;
+  const uint32_t half = 112640u, whole = 225280u;  // per-CTA budgets: two CTAs or one per SM
+  int per_sm = 2;
+  uint32_t budget = half;
+  if (geo.w_bytes + 4 * geo.stage_bytes + 1024 > half) {
+    per_sm = 1;
+    budget = whole;
+  }
+  if (geo.w_bytes + 4 * geo.stage_bytes + 1024 > budget) return false;
+  geo.S = std::min<int>(kRowsMaxStages, (int)((budget - 1024 - geo.w_bytes) / geo.stage_bytes));
+  const size_t smem = (size_t)geo.w_bytes + (size_t)geo.S * geo.stage_bytes + 1024;
+  geo.segs = W / 128;
+  const int ctas = sm_count() * per_sm;
+  // rows per run: the fewest input rows on the busiest CTA, ceil(units/ctas) * (R + 2)
+  long best = -1;
+  for (int R = 1; R <= H; R *= 2) {
+    const long units = (long)Bimg * geo.segs * ((H + R - 1) / R);
+    const long cost = ((units + ctas - 1) / ctas) * (R + 2);
+    if (best < 0 || cost < best) {
+      best = cost;
+      geo.R = R;
+    }
+  }
+  geo.hblocks = (H + geo.R - 1) / geo.R;
+  geo.nunits = Bimg * geo.segs * geo.hblocks;
+  const cuuint64_t dx[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
+  const cuuint64_t sx[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t bx[4] = {(cuuint32_t)ks, (cuuint32_t)kStripBox, 1, 1};
+  const CUtensorMap ma = make_map(g.convX, 4, dx, sx, bx, sw);
+  const cuuint64_t dw[2] = {(cuuint64_t)9 * C, (cuuint64_t)g.N}, swt[1] = {(cuuint64_t)g.ldb * 2};
+  const cuuint32_t bwt[2] = {(cuuint32_t)ks, (cuuint32_t)bn};
+  const CUtensorMap mb = make_map(g.B, 2, dw, swt, bwt, sw);
+  const int grid = std::max(1, std::min(geo.nunits, ctas));
+#define AIRT_R(BNV, SWV)                                                                                  \
+  switch (epi) {                                                                                          \
+    case EPI_STORE_F32: launch_rows<BNV, EPI_STORE_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;       \
+    case EPI_BIAS_RELU_BF16: launch_rows<BNV, EPI_BIAS_RELU_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break; \
+    case EPI_BIAS_BF16: launch_rows<BNV, EPI_BIAS_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break;       \
+    case EPI_ADD_F32: launch_rows<BNV, EPI_ADD_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;           \
+    default: return false;                                                                                \
+  }
+  if (sw == 128) {
+    switch (bn) {
+      case 32: AIRT_R(32, 128) break;
+      case 64: AIRT_R(64, 128) break;
+      default: AIRT_R(128, 128) break;
+    }
+  } else {
+    switch (bn) {
+      case 32: AIRT_R(32, 64) break;
+      case 64: AIRT_R(64, 64) break;
+      default: AIRT_R(128, 64) break;
+    }
+  }
+#undef AIRT_R
+  return true;
+}
+
 void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   AIRT_REQUIRE(conv3x3_tma_ok(g), "conv3x3: shape unsuitable for TMA");
+  if (conv3x3_rows(g, bn, epi, s)) return;
   if (conv3x3_halo(g, bn, epi, s)) return;
   const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
   const int sw = swizzle_for(C), ks = sw / 2;

@@ -239,7 +239,7 @@ __global__ void k_to_interleaved(int64_t len, int K, int Kp, const double *__res
 }
 
 __global__ void k_from_interleaved(int64_t len, int K, int Kp, const double *__restrict__ src,
-                                   double *__restrict__ dst) {
+                                   double *__restrict__ dst, const int *__restrict__ kmap) {
   __shared__ double t[32][33];
   const int64_t i0 = (int64_t)blockIdx.x * 32;
   const int k0 = blockIdx.y * 32;
@@ -252,7 +252,38 @@ __global__ void k_from_interleaved(int64_t len, int K, int Kp, const double *__r
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int k = k0 + r;
     const int64_t i = i0 + threadIdx.x;
-    if (k < K && i < len) dst[(int64_t)k * len + i] = t[threadIdx.x][r];
+    if (k < K && i < len) dst[(int64_t)(kmap ? kmap[k] : k) * len + i] = t[threadIdx.x][r];
+  }
+}
+
+// Compaction of the interleaved layout to the running instances:
+// dst[i][q] = src[i][map[q]] ([len][Kq] from [len][Kp]; map[q] < 0: 0).
+__global__ void k_mr_compact(int64_t len, int Kp, int Kq, const int *__restrict__ map,
+                             const double *__restrict__ src, double *__restrict__ dst,
+                             float *__restrict__ dst32) {
+  const int64_t total = len * Kq;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e / Kq;
+    const int q = (int)(e - i * Kq);
+    const int k = map[q];
+    const double v = k >= 0 ? src[i * Kp + k] : 0.0;
+    dst[e] = v;
+    if (dst32) dst32[e] = (float)v;
+  }
+}
+
+// Final iterates of the listed slots to their instance-major rows:
+// X[dst_k[c]][j] = x64[j][slot[c]].
+__global__ void k_mr_extract(int64_t n, int Kp, int cnt, const int *__restrict__ slot,
+                             const int *__restrict__ dst_k, const double *__restrict__ x64,
+                             double *__restrict__ X) {
+  const int64_t total = (int64_t)cnt * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n);
+    const int64_t j = e - (int64_t)c * n;
+    X[(int64_t)dst_k[c] * n + j] = x64[j * Kp + slot[c]];
   }
 }
 
@@ -279,8 +310,13 @@ int group_for(int Kp) {
   return G;
 }
 
-// One pass: K <= kMaxK instances.
-void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, const double *d_X0,
+// One pass: K <= kMaxK instances.  Once the running instances fit in half
+// the slots (DP rule, no save list), the pass drains the stream, writes the
+// stopped instances' iterates out and compacts the layout to the running
+// ones, so an iteration's gathers shrink with the instances still running.
+// Every instance's own sums keep their order, so its iterates do not depend
+// on the slot it occupies.
+void multi_pass(Problem &P, const airt_sirt_opts &o, int K0, const double *d_B, const double *d_X0,
                 const double *taud_host, const double *lam_host, const int *save_slot,
                 double *d_Xs, int64_t slot_stride, double *d_X, int64_t *finaliter,
                 int *stoprule) {
@@ -288,8 +324,9 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
   const int64_t m = P.m, n = P.n, kmax = o.kmax;
   // every lane of a group owns 8 slots, so the slot count is 8G (G a power
   // of two): no lane reads or writes past its row
-  const int G = group_for((K + 7) / 8 * 8);
-  const int Kp = 8 * G;
+  int K = K0;
+  int G = group_for((K + 7) / 8 * 8);
+  int Kp = 8 * G;
   P.mr_b.ensure((size_t)m * Kp);
   P.mr_x64.ensure((size_t)n * Kp);
   P.mr_x32.ensure((size_t)n * Kp);
@@ -300,8 +337,12 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
   k_to_interleaved<<<dim3((unsigned)((n + 31) / 32), (unsigned)((Kp + 31) / 32)), tb, 0, s>>>(
       n, K, Kp, d_X0, P.mr_x64.p, P.mr_x32.p);
   AIRT_LAUNCH_CHECK();
-  const unsigned gf = std::min<unsigned>(grid_for(m * G, kMrThreads, 8), (unsigned)num_sms() * 8);
-  const unsigned gb = std::min<unsigned>(grid_for(n * G, kMrThreads, 8), (unsigned)num_sms() * 8);
+  auto grids = [&](unsigned &gf, unsigned &gb) {
+    gf = std::min<unsigned>(grid_for(m * G, kMrThreads, 8), (unsigned)num_sms() * 8);
+    gb = std::min<unsigned>(grid_for(n * G, kMrThreads, 8), (unsigned)num_sms() * 8);
+  };
+  unsigned gf, gb;
+  grids(gf, gb);
   P.mr_part.ensure((size_t)gf * Kp);
   P.mr_stop.ensure(Kp);
   P.mr_iters.ensure(Kp);
@@ -313,19 +354,29 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
   AIRT_CHECK_CUDA(cudaMemsetAsync(P.mr_rule.p, 0, Kp * sizeof(int), s));
   MultiState st0{0, K, o.relaxpar};
   P.mr_state.upload(&st0, 1, s);
+  // per-slot copies of the per-instance inputs (slot q holds instance orig[q])
+  std::vector<int> orig(K);
+  for (int k = 0; k < K; ++k) orig[k] = k;
+  std::vector<double> hlam, htaud;
   if (lam_host) {
-    std::vector<double> lk(Kp, 0.0);
-    std::copy(lam_host, lam_host + K, lk.begin());
-    P.mr_lam.upload(lk.data(), Kp, s);
+    hlam.assign(lam_host, lam_host + K);
+    hlam.resize(Kp, 0.0);
+    P.mr_lam.upload(hlam.data(), Kp, s);
   }
-  if (taud_host) P.mr_taud.upload(taud_host, K, s);
+  if (taud_host) {
+    htaud.assign(taud_host, taud_host + K);
+    P.mr_taud.upload(htaud.data(), K, s);
+  }
   const double *taud = taud_host ? P.mr_taud.p : nullptr;
   if (o.relax_kind == AIRT_RELAX_TABLE && kmax > 0) P.table.upload(o.relax_table, kmax, s);
   const double *table = o.relax_kind == AIRT_RELAX_TABLE ? P.table.p : nullptr;
 
-  MrArgs a{K, Kp, P.mr_b.p, P.M.p, P.D.p, P.mr_x64.p, P.mr_x32.p, P.mr_r32.p, P.mr_stop.p,
-           P.mr_part.p, o.lb_kind, o.ub_kind, o.lb, o.ub, P.mr_state.p,
-           lam_host ? P.mr_lam.p : nullptr};
+  auto args = [&]() {
+    return MrArgs{K, Kp, P.mr_b.p, P.M.p, P.D.p, P.mr_x64.p, P.mr_x32.p, P.mr_r32.p, P.mr_stop.p,
+                  P.mr_part.p, o.lb_kind, o.ub_kind, o.lb, o.ub, P.mr_state.p,
+                  lam_host ? P.mr_lam.p : nullptr};
+  };
+  MrArgs a = args();
   auto fwd = [&]() {
     switch (G) {
       case 1: k_mr_fwd<1><<<gf, kMrThreads, 0, s>>>(m, P.rp.p, P.ci.p, P.rv.p, a); break;
@@ -357,12 +408,16 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
   fwd();
   ctrl(1);
   AIRT_LAUNCH_CHECK();
-  // Chunks of iterations captured once as a CUDA graph; the host reads the
-  // active count of chunk c once chunk c+2 is queued (lagged poll).
+  // Chunks of iterations captured once as a CUDA graph (again after each
+  // compaction); the host reads the active count of chunk c once chunk c+2
+  // is queued (lagged poll).
   const int64_t chunk = 8;
   const int lag = 2;
   cudaGraphExec_t gexec = nullptr;
-  if (kmax >= chunk) {
+  auto capture = [&]() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    if (kmax < chunk) return;
     cudaGraph_t g = nullptr;
     AIRT_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int64_t j = 0; j < chunk; ++j) {
@@ -376,13 +431,99 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
       cudaGraphDestroy(g);
     }
     cudaGetLastError();
-  }
+  };
+  capture();
   if (!P.h_state) AIRT_CHECK_CUDA(cudaMallocHost(&P.h_state, 3 * sizeof(SirtState)));
   static_assert(sizeof(MultiState) <= sizeof(SirtState), "poll slots");
   MultiState *hs = reinterpret_cast<MultiState *>(P.h_state);  // 3 slots in the pinned mirror
   cudaEvent_t ev[3];
   for (int q = 0; q < 3; ++q) AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming));
+  std::vector<int> hstop, hit, hrule;
+  auto record = [&](int q) {  // finaliter / stoprule of slot q's instance
+    if (finaliter) finaliter[orig[q]] = hit[q];
+    if (stoprule) stoprule[orig[q]] = hrule[q];
+  };
+  auto read_slots = [&]() {
+    hstop.resize(K);
+    hit.resize(K);
+    hrule.resize(K);
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hstop.data(), P.mr_stop.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hit.data(), P.mr_iters.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(hrule.data(), P.mr_rule.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  };
+  DevBuf<int> dmap, dslot, ddst;
+  DevBuf<double> tmp64;
+  DevBuf<float> tmp32;
+  // Compacts to the running slots; returns false when none is left.
+  auto compact = [&]() {
+    read_slots();
+    std::vector<int> keep, done_slot, done_k;
+    for (int q = 0; q < K; ++q) {
+      if (hstop[q]) {
+        done_slot.push_back(q);
+        done_k.push_back(orig[q]);
+        record(q);
+      } else {
+        keep.push_back(q);
+      }
+    }
+    if (!done_slot.empty()) {
+      dslot.upload(done_slot.data(), done_slot.size(), s);
+      ddst.upload(done_k.data(), done_k.size(), s);
+      k_mr_extract<<<grid_for((int64_t)done_slot.size() * n, 256), 256, 0, s>>>(
+          n, Kp, (int)done_slot.size(), dslot.p, ddst.p, P.mr_x64.p, d_X);
+    }
+    const int Kn = (int)keep.size();
+    if (Kn == 0) return false;
+    const int Gn = group_for((Kn + 7) / 8 * 8), Kq = 8 * Gn;
+    std::vector<int> map(Kq, -1), norig(Kn);
+    for (int q = 0; q < Kn; ++q) {
+      map[q] = keep[q];
+      norig[q] = orig[keep[q]];
+    }
+    dmap.upload(map.data(), Kq, s);
+    // iterates, FP32 copies and right-hand sides
+    tmp64.ensure((size_t)n * Kq);
+    tmp32.ensure((size_t)n * Kq);
+    k_mr_compact<<<grid_for(n * Kq, 256), 256, 0, s>>>(n, Kp, Kq, dmap.p, P.mr_x64.p, tmp64.p, tmp32.p);
+    std::swap(P.mr_x64, tmp64);
+    std::swap(P.mr_x32, tmp32);
+    tmp64.ensure((size_t)m * Kq);
+    k_mr_compact<<<grid_for(m * Kq, 256), 256, 0, s>>>(m, Kp, Kq, dmap.p, P.mr_b.p, tmp64.p, nullptr);
+    std::swap(P.mr_b, tmp64);
+    AIRT_LAUNCH_CHECK();
+    // per-slot state: every running instance has the same iteration count
+    std::vector<int> zero(Kq, 0), its(Kq, 0);
+    for (int q = 0; q < Kn; ++q) its[q] = hit[keep[q]];
+    P.mr_stop.upload(zero.data(), Kq, s);
+    P.mr_rule.upload(zero.data(), Kq, s);
+    P.mr_iters.upload(its.data(), Kq, s);
+    if (lam_host) {
+      std::vector<double> l(Kq, 0.0);
+      for (int q = 0; q < Kn; ++q) l[q] = hlam[keep[q]];
+      hlam = l;
+      P.mr_lam.upload(hlam.data(), Kq, s);
+    }
+    if (taud_host) {
+      std::vector<double> t(Kn);
+      for (int q = 0; q < Kn; ++q) t[q] = htaud[keep[q]];
+      htaud = t;
+      P.mr_taud.upload(htaud.data(), Kn, s);
+    }
+    orig = norig;
+    K = Kn;
+    G = Gn;
+    Kp = Kq;
+    grids(gf, gb);
+    P.mr_part.ensure((size_t)gf * Kp);
+    P.mr_r32.ensure((size_t)m * Kp);
+    a = args();
+    capture();
+    return true;
+  };
   int64_t c = 0;
+  bool live = true;
   for (int64_t it = 1; it <= kmax; ++c) {
     const int64_t cnt = std::min<int64_t>(chunk, kmax - it + 1);
     if (cnt == chunk && gexec) {
@@ -402,21 +543,29 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K, const double *d_B, c
     AIRT_CHECK_CUDA(cudaEventRecord(ev[c % 3], s));
     if (c >= lag) {
       AIRT_CHECK_CUDA(cudaEventSynchronize(ev[(c - lag) % 3]));
-      if (hs[(c - lag) % 3].active == 0) break;
+      const int act = hs[(c - lag) % 3].active;
+      if (act == 0) break;
+      if (!save_slot && it <= kmax && G > 1 && group_for((act + 7) / 8 * 8) < G) {
+        if (!compact()) {
+          live = false;
+          break;
+        }
+        c = -1;  // fresh poll slots after the drain
+      }
     }
   }
   if (gexec) cudaGraphExecDestroy(gexec);
   for (int q = 0; q < 3; ++q) cudaEventDestroy(ev[q]);
-  k_from_interleaved<<<dim3((unsigned)((n + 31) / 32), (unsigned)((Kp + 31) / 32)), tb, 0, s>>>(
-      n, K, Kp, P.mr_x64.p, d_X);
-  AIRT_LAUNCH_CHECK();
-  std::vector<int> hit(K), hrule(K);
-  AIRT_CHECK_CUDA(cudaMemcpyAsync(hit.data(), P.mr_iters.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
-  AIRT_CHECK_CUDA(cudaMemcpyAsync(hrule.data(), P.mr_rule.p, K * sizeof(int), cudaMemcpyDeviceToHost, s));
-  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
-  for (int k = 0; k < K; ++k) {
-    if (finaliter) finaliter[k] = hit[k];
-    if (stoprule) stoprule[k] = hrule[k];
+  if (live) {
+    const bool ident = K == K0;
+    if (!ident) dmap.upload(orig.data(), K, s);
+    k_from_interleaved<<<dim3((unsigned)((n + 31) / 32), (unsigned)((Kp + 31) / 32)), tb, 0, s>>>(
+        n, K, Kp, P.mr_x64.p, d_X, ident ? nullptr : dmap.p);
+    AIRT_LAUNCH_CHECK();
+    read_slots();
+    for (int q = 0; q < K; ++q) record(q);
+  } else {
+    AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
   }
 }
 

@@ -283,8 +283,8 @@ void conv3x3_wgrad_bf16_tma(const GemmArgs &g, int bn, cudaStream_t s);
 // Operand path: 0 = TMA where possible, 1 = always cp.async (a test switch).
 extern int g_gemm_path;
 // 3x3 convolution operand form on the TMA path: 0 = nine tap boxes per
-// tile, 1 = halo strips (W % 128 == 0) with the descriptor base offset,
-// 2 = halo strips without it (a layout check).
+// tile; 1 = halo strips where W % 128 == 0 (else tap boxes); 2 = row runs
+// with resident weights where they fit (else halo strips, else tap boxes).
 extern int g_conv_halo;
 
 }  // namespace airt

@@ -130,21 +130,23 @@ class UNet:
 
 
 def _timing_main():
-    """python -m airtoolsii_b200.unet [--batch B] [--reps R] [--conv tap|halo]:
-    device time per image of the forward pass and of one Adam training step
-    of the N=256, 4-level, base-32 network (random inputs), CUDA events on
-    its stream; --conv picks the operand form of the TMA 3x3 convolutions."""
+    """python -m airtoolsii_b200.unet [--batch B] [--reps R] [--conv tap|halo|rows]
+    [--forward-only]: device time per image of the forward pass and of one
+    Adam training step of the N=256, 4-level, base-32 network (random
+    inputs), CUDA events on its stream; --conv picks the operand form of the
+    TMA 3x3 convolutions (default: row runs where they apply)."""
     import argparse
     import torch
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--conv", choices=["default", "tap", "halo"], default="default")
+    ap.add_argument("--conv", choices=["default", "tap", "halo", "rows"], default="default")
+    ap.add_argument("--forward-only", action="store_true")
     a = ap.parse_args()
     if a.conv != "default":
         f = lib().airt_test_conv_halo
         f.restype, f.argtypes = C.c_int, [C.c_int]
-        check(f(1 if a.conv == "halo" else 0))
+        check(f({"tap": 0, "halo": 1, "rows": 2}[a.conv]))
     B = a.batch
     net = UNet(256, 256, 32, 4, B, 0)
     u = torch.rand(B, 65536, device="cuda")
@@ -153,7 +155,8 @@ def _timing_main():
     torch.cuda.synchronize()
     for _ in range(2):
         net.forward(u.data_ptr(), o.data_ptr(), B)
-        net.train_step(u.data_ptr(), t.data_ptr(), B, 1e-4)
+        if not a.forward_only:
+            net.train_step(u.data_ptr(), t.data_ptr(), B, 1e-4)
     torch.cuda.synchronize()
     s = torch.cuda.ExternalStream(net.stream_ptr())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -163,6 +166,9 @@ def _timing_main():
     e1.record(s)
     torch.cuda.synchronize()
     fwd = e0.elapsed_time(e1) / a.reps / B
+    if a.forward_only:
+        print({"conv": a.conv, "forward_ms_per_image": round(fwd, 5)})
+        return
     e0.record(s)
     for _ in range(a.reps):
         net.train_step(u.data_ptr(), t.data_ptr(), B, 1e-4)
