@@ -236,10 +236,12 @@ def test_gateway_matrix_sirt_art_cart_fbp_vs_oracle(mex):
     X = mex("cart", h, {"order_kind": 0.0, "relaxpar": 0.25}, b, np.zeros((0, 0)), np.array([4.0]))
     Xo, _ = O.cart("columnaction", A, b, [4])
     assert _relerr(X[:, -1], Xo[:, -1]) <= 1e-5
-    # fbp with the hamming kernel
+    # fbp with the hamming kernel (the handle holds the matrix in FP32)
     from airtoolsii_b200.analytic import fbp_kernel
     xf = mex("fbp", h, b, float(theta.size), fbp_kernel(A.shape[0] // theta.size, "hamming"))
-    assert _relerr(xf.ravel(), O.fbp(A, b, theta, "hamming")) <= 1e-10
+    A32 = A.copy()
+    A32.data = A32.data.astype(np.float32).astype(np.float64)
+    assert _relerr(xf.ravel(), O.fbp(A32, b, theta, "hamming")) <= 1e-10
     mex("destroy", h)
 
 
