@@ -90,6 +90,17 @@ struct Batch {
   DevBuf<int64_t> ncp_row0, ncp_tw0, ncp_pk0;
   DevBuf<int> ncp_L, ncp_inst, ncp_col0;
   DevBuf<double> ncp_tw, ncp_pk, ncp_ccol, ncp_dk;
+  // the lane classes of one direction run side by side: two more streams,
+  // forked from and joined to P.stream by events (graph-capturable)
+  cudaStream_t aux[kClasses - 1] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[kClasses - 1] = {nullptr, nullptr};
+  ~Batch() {
+    for (int i = 0; i < kClasses - 1; ++i) {
+      if (aux[i]) cudaStreamDestroy(aux[i]);
+      if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+  }
 };
 
 namespace {
@@ -202,11 +213,12 @@ __global__ void __launch_bounds__(256, 4)
   for_each_segment_vt<L>(
       nseg, tiles, ntiles, kTileShift, rp + o.r0, ci, rv, x32,
       [&](int64_t i) { return o.stop[o.inst_row[o.r0 + i]] == 0; },
-      [&](int64_t i, double s, bool lead) {
+      [&](int64_t i) { return make_double2(o.b[o.r0 + i], o.M[o.r0 + i]); },
+      [&](int64_t i, double s, bool lead, double2 bm) {
         if (!lead) return;
         const int64_t r = o.r0 + i;
-        const double ri = o.b[r] - s;
-        o.mr32[r] = (float)(o.M[r] * ri);
+        const double ri = bm.x - s;
+        o.mr32[r] = (float)(bm.y * ri);
         o.rsq[r] = ri * ri;
         if (o.rprev) {
           if (o.pp) {
@@ -237,10 +249,14 @@ __global__ void __launch_bounds__(256, 4)
   for_each_segment_vt<L>(
       nseg, tiles, ntiles, kTileShift, cp + u.c0, ri, cv, mr32,
       [&](int64_t j) { return u.stop[u.inst_col[u.c0 + j]] == 0; },
-      [&](int64_t j, double g, bool lead) {
+      [&](int64_t j) {
+        const int64_t c = u.c0 + j;
+        return make_double3(u.x64[c], u.lam[u.inst_col[c]], u.D[c]);
+      },
+      [&](int64_t j, double g, bool lead, double3 xld) {
         if (!lead) return;
         const int64_t c = u.c0 + j;
-        double x = u.x64[c] + u.lam[u.inst_col[c]] * (u.D[c] * g);
+        double x = xld.x + xld.y * (xld.z * g);
         if (u.lbk) x = fmax(x, u.lb);
         if (u.ubk) x = fmin(x, u.ub);
         u.x64[c] = x;
@@ -275,6 +291,35 @@ __global__ void k_active_tiles(int ntiles, int64_t nseg, const int *__restrict__
     if (!stop[k]) {
       const int c = cls[t];
       list[co.off[c] + atomicAdd(count + c, 1)] = t;
+      return;
+    }
+}
+
+// Both directions' active-tile lists in one launch (threads [0, nt_r) the
+// row tiles, the rest the column tiles); the counts were zeroed by the step
+// kernel that ran before.
+struct TileArgs {
+  int ntiles;
+  int64_t nseg;
+  const int *inst_of, *cls;
+  ClassOffsets co;
+  int *list, *count;
+};
+
+__global__ void k_active_tiles2(TileArgs r, TileArgs c, const int *__restrict__ stop) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const TileArgs *a = &r;
+  if (t >= r.ntiles) {
+    t -= r.ntiles;
+    a = &c;
+    if (t >= c.ntiles) return;
+  }
+  const int64_t s0 = (int64_t)t << kTileShift;
+  const int64_t s1 = min(a->nseg, s0 + ((int64_t)1 << kTileShift));
+  for (int k = a->inst_of[s0]; k <= a->inst_of[s1 - 1]; ++k)
+    if (!stop[k]) {
+      const int cl = a->cls[t];
+      a->list[a->co.off[cl] + atomicAdd(a->count + cl, 1)] = t;
       return;
     }
 }
@@ -401,8 +446,11 @@ __global__ void __launch_bounds__(256) k_batch_step(const int64_t *__restrict__ 
                                                     double *__restrict__ pr, int initial,
                                                     int64_t kmax, BCtrl c, int *__restrict__ stop,
                                                     int *__restrict__ iters, int *__restrict__ rule,
-                                                    double *__restrict__ resn, int *active) {
+                                                    double *__restrict__ resn, int *active,
+                                                    int *__restrict__ tcount) {
   const int k = blockIdx.x;
+  // the active-tile counts of the rebuild that follows this step
+  if (tcount && k == 0 && threadIdx.x < 2 * kClasses) tcount[threadIdx.x] = 0;
   if (stop[k]) return;
   double a = 0, e = 0, d = 0;
   for (int64_t i = roff[k] + threadIdx.x; i < roff[k + 1]; i += blockDim.x) {
@@ -505,11 +553,12 @@ float time_launch(cudaStream_t s, F &&f, int reps = 3) {
 // Launch class c of the forward / transpose kernel with L lanes per
 // segment; the grid covers every tile of the class (graph-capturable), the
 // kernel walks only the listed ones.
-void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullptr) {
+void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullptr,
+                 cudaStream_t st = nullptr) {
   Problem &P = B.P;
   if (!x32) x32 = P.x32.p;
   if (B.rt.count[c] == 0) return;
-  cudaStream_t s = P.stream;
+  cudaStream_t s = st ? st : P.stream;
   const int64_t ns = P.m;
   const unsigned g = grid_for((int64_t)B.rt.count[c] * (1 << kTileShift) * L, 256, 4);
   const int *tl = B.rt.list.p + B.rt.off[c], *cnt = B.tcount.p + c;
@@ -523,11 +572,12 @@ void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullp
   }
 }
 
-void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = nullptr) {
+void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = nullptr,
+                 cudaStream_t st = nullptr) {
   Problem &P = B.P;
   if (!mr32) mr32 = P.mr32.p;
   if (B.ct.count[c] == 0) return;
-  cudaStream_t s = P.stream;
+  cudaStream_t s = st ? st : P.stream;
   const int64_t ns = P.n;
   const unsigned g = grid_for((int64_t)B.ct.count[c] * (1 << kTileShift) * L, 256, 4);
   const int *tl = B.ct.list.p + B.ct.off[c], *cnt = B.tcount.p + kClasses + c;
@@ -541,12 +591,36 @@ void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = null
   }
 }
 
+// The classes with tiles run concurrently: the largest on P.stream, the
+// others on the auxiliary streams, joined back before the next step.
+template <class F>
+void run_classes(Batch &B, const TileSet &T, F &&launch) {
+  cudaStream_t s = B.P.stream;
+  int big = 0;
+  for (int c = 1; c < kClasses; ++c)
+    if (T.count[c] > T.count[big]) big = c;
+  int na = 0;
+  for (int c = 0; c < kClasses; ++c)
+    if (c != big && T.count[c] > 0) ++na;
+  if (na > 0) AIRT_CHECK_CUDA(cudaEventRecord(B.ev_fork, s));
+  int q = 0;
+  for (int c = 0; c < kClasses; ++c) {
+    if (c == big || T.count[c] == 0) continue;
+    AIRT_CHECK_CUDA(cudaStreamWaitEvent(B.aux[q], B.ev_fork, 0));
+    launch(c, B.aux[q]);
+    AIRT_CHECK_CUDA(cudaEventRecord(B.ev_join[q], B.aux[q]));
+    ++q;
+  }
+  launch(big, s);
+  for (int i = 0; i < q; ++i) AIRT_CHECK_CUDA(cudaStreamWaitEvent(s, B.ev_join[i], 0));
+}
+
 void fwd_classes(Batch &B, const BFwd &o) {
-  for (int c = 0; c < kClasses; ++c) launch_bfwd(B, c, B.rt.lanes[c], o);
+  run_classes(B, B.rt, [&](int c, cudaStream_t st) { launch_bfwd(B, c, B.rt.lanes[c], o, nullptr, st); });
 }
 
 void bwd_classes(Batch &B, const BUpd &u) {
-  for (int c = 0; c < kClasses; ++c) launch_bbwd(B, c, B.ct.lanes[c], u);
+  run_classes(B, B.ct, [&](int c, cudaStream_t st) { launch_bbwd(B, c, B.ct.lanes[c], u, nullptr, st); });
 }
 
 // Rebuild the active row and column tile lists from stop[].
@@ -563,6 +637,20 @@ void build_tiles(Batch &B, const int *stop) {
                                                            B.rt.list.p, B.tcount.p);
   k_active_tiles<<<(B.ct.ntiles + 127) / 128, 128, 0, s>>>(B.ct.ntiles, P.n, B.inst_col.p, stop, B.ct.cls.p, co,
                                                            B.ct.list.p, B.tcount.p + kClasses);
+  AIRT_LAUNCH_CHECK();
+}
+
+// Rebuild after k_batch_step (which zeroed the counts): one launch.
+void build_tiles_after_step(Batch &B, const int *stop) {
+  Problem &P = B.P;
+  TileArgs r{B.rt.ntiles, P.m, B.inst_row.p, B.rt.cls.p, {}, B.rt.list.p, B.tcount.p};
+  TileArgs c{B.ct.ntiles, P.n, B.inst_col.p, B.ct.cls.p, {}, B.ct.list.p, B.tcount.p + kClasses};
+  for (int q = 0; q < kClasses; ++q) {
+    r.co.off[q] = B.rt.off[q];
+    c.co.off[q] = B.ct.off[q];
+  }
+  const int nt = B.rt.ntiles + B.ct.ntiles;
+  k_active_tiles2<<<(nt + 127) / 128, 128, 0, P.stream>>>(r, c, stop);
   AIRT_LAUNCH_CHECK();
 }
 
@@ -595,6 +683,11 @@ Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const d
   Batch *B = new Batch();
   try {
     AIRT_CHECK_CUDA(cudaStreamCreateWithFlags(&B->P.stream, cudaStreamNonBlocking));
+    for (int i = 0; i < kClasses - 1; ++i) {
+      AIRT_CHECK_CUDA(cudaStreamCreateWithFlags(&B->aux[i], cudaStreamNonBlocking));
+      AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&B->ev_join[i], cudaEventDisableTiming));
+    }
+    AIRT_CHECK_CUDA(cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming));
     Problem &P = B->P;
     cudaStream_t s = P.stream;
     B->ninst = ninst;
@@ -951,16 +1044,16 @@ void batch_sirt(Batch &B, int method, const double *lam_host, const double *d_b,
     k_batch_step<<<K, 256, 0, s>>>(B.d_row_off.p, B.rsq.p, me ? B.pp.p : nullptr,
                                    me ? B.ppr.p : nullptr, me ? B.p2.p : nullptr,
                                    me ? B.pr.p : nullptr, initial, kmax, co, B.stop.p, B.iters.p,
-                                   B.rule.p, B.resn_last.p, B.active.p);
+                                   B.rule.p, B.resn_last.p, B.active.p, B.tcount.p);
   };
   auto iteration = [&]() {
     bwd_classes(B, uo);
     fwd_step(0);
-    build_tiles(B, B.stop.p);
+    build_tiles_after_step(B, B.stop.p);
   };
   fwd_step(1);
   AIRT_LAUNCH_CHECK();
-  build_tiles(B, B.stop.p);
+  build_tiles_after_step(B, B.stop.p);
   // A chunk of iterations is captured once as a CUDA graph and replayed:
   // every argument is fixed for the solve and the loop state lives in device
   // memory.  The host reads the active count of chunk c once chunk c+2 is

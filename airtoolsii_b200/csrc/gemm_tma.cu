@@ -314,16 +314,13 @@ __global__ void __launch_bounds__(192, 1) k_gemm_tma(const __grid_constant__ CUt
             }
             commit(smem_addr(&empty[st]));
           } else {
+            // K step kk: the base descriptors plus the step's byte offset / 16
+            const uint64_t da0 = MN ? make_desc_sw<SWA>(sa, 64 * SWA, 8 * SWA) : make_desc_sw<SWA>(sa, 16, 8 * SWA);
+            const uint64_t db0 = MN ? make_desc_sw<SWB>(sb, 64 * SWB, 8 * SWB) : make_desc_sw<SWA>(sb, 16, 8 * SWA);
 #pragma unroll
             for (int kk = 0; kk < KS / 16; ++kk) {
-              uint64_t da, db;
-              if (MN) {
-                da = make_desc_sw<SWA>(sa + kk * 16 * SWA, 64 * SWA, 8 * SWA);
-                db = make_desc_sw<SWB>(sb + kk * 16 * SWB, 64 * SWB, 8 * SWB);
-              } else {
-                da = make_desc_sw<SWA>(sa + kk * 32, 16, 8 * SWA);
-                db = make_desc_sw<SWA>(sb + kk * 32, 16, 8 * SWA);
-              }
+              const uint64_t da = da0 + (MN ? (uint64_t)kk * SWA : (uint64_t)kk * 2);
+              const uint64_t db = db0 + (MN ? (uint64_t)kk * SWB : (uint64_t)kk * 2);
               mma_bf16(dtm, da, db, idesc, (k > 0 || kk > 0) ? 1u : 0u);
             }
             commit(smem_addr(&empty[st]));
@@ -406,18 +403,31 @@ __device__ __forceinline__ RowsUnit rows_unit(const RowsGeo &geo, int u) {
   return r;
 }
 
+// Epilogue groups of four warps: NE groups drain 2*NE TMEM accumulators in
+// turn (output row ol -> accumulator ol % (2 NE), group ol % NE), so two
+// warps per SM sub-partition hide each other's TMEM-load and store latency.
+template <int BN>
+struct RowsRoles {
+  static constexpr int NE = BN <= 64 ? 2 : 1;
+  static constexpr int NACC = 2 * NE;
+  static constexpr int THREADS = 64 + 128 * NE;
+  static constexpr uint32_t TMEM_COLS = (uint32_t)(NACC * BN);
+};
+
 template <int BN, int EPI, int SWA>
-__global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CUtensorMap mapA,
-                                                      const __grid_constant__ CUtensorMap mapB, GemmArgs g,
-                                                      RowsGeo geo) {
+__global__ void __launch_bounds__(RowsRoles<BN>::THREADS, 1)
+    k_conv_rows(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmArgs g,
+                RowsGeo geo) {
   using Cfg = RowsCfg<SWA>;
-  constexpr int KS = Cfg::KS, STRIPS = Cfg::STRIPS;
+  using Ro = RowsRoles<BN>;
+  constexpr int KS = Cfg::KS, STRIPS = Cfg::STRIPS, NACC = Ro::NACC, NE = Ro::NE;
   constexpr uint32_t STRIP = Cfg::STRIP_BYTES;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t wbase = smem_addr(base);  // resident weights (w_bytes, a multiple of 1 KB)
   const uint32_t rbase = wbase + geo.w_bytes;
-  __shared__ __align__(8) uint64_t full[kRowsMaxStages], empty[kRowsMaxStages], acc_full[2], acc_empty[2], wfull;
+  __shared__ __align__(8) uint64_t full[kRowsMaxStages], empty[kRowsMaxStages], acc_full[NACC],
+      acc_empty[NACC], wfull;
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   volatile int *abort_flag = &s_abort;
@@ -427,7 +437,7 @@ __global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CU
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&s_tmem)),
-                 "r"((uint32_t)(2 * BN)));
+                 "r"(Ro::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (threadIdx.x == 0) {
@@ -436,7 +446,7 @@ __global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CU
       mbar_init(smem_addr(&full[i]), 1);
       mbar_init(smem_addr(&empty[i]), 1);
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < NACC; ++i) {
       mbar_init(smem_addr(&acc_full[i]), 1);
       mbar_init(smem_addr(&acc_empty[i]), 128);
     }
@@ -483,8 +493,12 @@ __global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CU
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      // ---- MMA issuer
+      // ---- MMA issuer.  A descriptor's start-address field is the byte
+      // address / 16 in its low bits, so the descriptors of the taps, chunks
+      // and K steps are the stage's (or the weights') base descriptor plus a
+      // constant: one 64-bit add per operand per MMA.
       constexpr uint32_t idesc = make_idesc<BN, false, false>();
+      const uint64_t wdesc = make_desc_sw<SWA>(wbase, 16, 8 * SWA);
       bool ok = mbar_wait(smem_addr(&wfull), 0);
       uint32_t it = 0, ol = 0;
       for (int u = blockIdx.x; ok && u < geo.nunits && !*abort_flag; u += gridDim.x) {
@@ -492,29 +506,29 @@ __global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CU
         for (int r = 0; r < 2 && ok; ++r) ok = mbar_wait(smem_addr(&full[(it + r) % S]), ((it + r) / S) & 1u);
         for (int i = 0; ok && i < ru.rows; ++i, ++ol) {
           const uint32_t sr = it + i + 2;
-          const uint32_t buf = ol & 1u;
+          const uint32_t buf = ol % NACC;
           if (!mbar_wait(smem_addr(&full[sr % S]), (sr / S) & 1u) ||
-              (ol >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((ol >> 1) - 1) & 1u))) {
+              (ol >= (uint32_t)NACC && !mbar_wait(smem_addr(&acc_empty[buf]), ((ol / NACC) - 1) & 1u))) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t dtm = tmem + buf * BN;
+          uint32_t acc = 0;
           for (int dh = 0; dh < 3; ++dh) {
-            const uint32_t sa = rbase + ((it + i + dh) % S) * geo.stage_bytes;
+            const uint64_t sdesc = make_desc_sw<SWA>(rbase + ((it + i + dh) % S) * geo.stage_bytes, 16, 8 * SWA);
             for (int cc = 0; cc < geo.cch; ++cc) {
-              const uint32_t ca = sa + (uint32_t)(cc * STRIPS) * STRIP;
+              const uint64_t cdesc = sdesc + ((uint64_t)(cc * STRIPS) * STRIP >> 4);
               // tap dw reads the strip shifted by dw pixel rows (strip 1 for
               // the middle tap when pixel rows are 64 bytes: see MODE_HALO)
 #pragma unroll
               for (int dw = 0; dw < 3; ++dw) {
-                const uint32_t a0 = STRIPS == 2 && dw == 1 ? ca + STRIP : ca + (uint32_t)dw * SWA;
-                const uint32_t b0 = wbase + (uint32_t)((3 * dh + dw) * geo.cch + cc) * (BN * SWA);
+                const uint64_t da = cdesc + ((STRIPS == 2 && dw == 1 ? STRIP : (uint32_t)dw * SWA) >> 4);
+                const uint64_t db = wdesc + ((uint64_t)((3 * dh + dw) * geo.cch + cc) * (BN * SWA) >> 4);
 #pragma unroll
                 for (int kk = 0; kk < KS / 16; ++kk) {
-                  const uint64_t da = make_desc_sw<SWA>(a0 + kk * 32, 16, 8 * SWA);
-                  const uint64_t db = make_desc_sw<SWA>(b0 + kk * 32, 16, 8 * SWA);
-                  mma_bf16(dtm, da, db, idesc, (dh > 0 || cc > 0 || dw > 0 || kk > 0) ? 1u : 0u);
+                  mma_bf16(dtm, da + 2 * kk, db + 2 * kk, idesc, acc);
+                  acc = 1;
                 }
               }
             }
@@ -530,15 +544,17 @@ __global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CU
       if (!ok) *abort_flag = 1;
     }
   } else {
-    // ---- epilogue warps 2-5: one output row (128 pixels) per accumulator
-    const int quad = warp & 3;
+    // ---- epilogue groups: warps 2 + 4e .. 5 + 4e; warp w reads TMEM lanes
+    // 32 * (w % 4) ..; group e takes the output rows ol with ol % NE == e
+    const int quad = warp & 3, grp = (warp - 2) >> 2;
     uint32_t ol = 0;
     bool ok = true;
     for (int u = blockIdx.x; ok && u < geo.nunits; u += gridDim.x) {
       const RowsUnit ru = rows_unit(geo, u);
       for (int i = 0; i < ru.rows; ++i, ++ol) {
-        const uint32_t buf = ol & 1u;
-        if (!mbar_wait(smem_addr(&acc_full[buf]), (ol >> 1) & 1u)) {
+        if ((int)(ol % NE) != grp) continue;
+        const uint32_t buf = ol % NACC;
+        if (!mbar_wait(smem_addr(&acc_full[buf]), (ol / NACC) & 1u)) {
           *abort_flag = 1;
           ok = false;
           break;
@@ -556,7 +572,7 @@ __global__ void __launch_bounds__(192, 1) k_conv_rows(const __grid_constant__ CU
   if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * BN)));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Ro::TMEM_COLS));
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -726,7 +742,7 @@ static void launch_rows(const CUtensorMap &ma, const CUtensorMap &mb, const Gemm
                         size_t smem, int ctas, cudaStream_t s) {
   auto kern = k_conv_rows<BN, EPI, SWA>;
   AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ctas, 192, smem, s>>>(ma, mb, g, geo);
+  kern<<<ctas, RowsRoles<BN>::THREADS, smem, s>>>(ma, mb, g, geo);
   AIRT_LAUNCH_CHECK();
 }
 

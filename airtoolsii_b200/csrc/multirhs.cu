@@ -257,9 +257,11 @@ __global__ void k_from_interleaved(int64_t len, int K, int Kp, const double *__r
 }
 
 // Compaction of the interleaved layout to the running instances:
-// dst[i][q] = src[i][map[q]] ([len][Kq] from [len][Kp]; map[q] < 0: 0).
+// dst[i][q] = src[i][map[q]] ([len][Kq] from [len][Kp]; map[q] < 0: 0),
+// and, for FP64 sources, the FP32 copy.
+template <typename T>
 __global__ void k_mr_compact(int64_t len, int Kp, int Kq, const int *__restrict__ map,
-                             const double *__restrict__ src, double *__restrict__ dst,
+                             const T *__restrict__ src, T *__restrict__ dst,
                              float *__restrict__ dst32) {
   const int64_t total = len * Kq;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
@@ -267,7 +269,7 @@ __global__ void k_mr_compact(int64_t len, int Kp, int Kq, const int *__restrict_
     const int64_t i = e / Kq;
     const int q = (int)(e - i * Kq);
     const int k = map[q];
-    const double v = k >= 0 ? src[i * Kp + k] : 0.0;
+    const T v = k >= 0 ? src[i * Kp + k] : (T)0;
     dst[e] = v;
     if (dst32) dst32[e] = (float)v;
   }
@@ -486,12 +488,19 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K0, const double *d_B, 
     // iterates, FP32 copies and right-hand sides
     tmp64.ensure((size_t)n * Kq);
     tmp32.ensure((size_t)n * Kq);
-    k_mr_compact<<<grid_for(n * Kq, 256), 256, 0, s>>>(n, Kp, Kq, dmap.p, P.mr_x64.p, tmp64.p, tmp32.p);
+    k_mr_compact<double><<<grid_for(n * Kq, 256), 256, 0, s>>>(n, Kp, Kq, dmap.p, P.mr_x64.p, tmp64.p,
+                                                             tmp32.p);
     std::swap(P.mr_x64, tmp64);
     std::swap(P.mr_x32, tmp32);
     tmp64.ensure((size_t)m * Kq);
-    k_mr_compact<<<grid_for(m * Kq, 256), 256, 0, s>>>(m, Kp, Kq, dmap.p, P.mr_b.p, tmp64.p, nullptr);
+    k_mr_compact<double><<<grid_for(m * Kq, 256), 256, 0, s>>>(m, Kp, Kq, dmap.p, P.mr_b.p, tmp64.p,
+                                                             nullptr);
     std::swap(P.mr_b, tmp64);
+    // M.*R of the last forward pass: the next transpose pass reads it
+    tmp32.ensure((size_t)m * Kq);
+    k_mr_compact<float><<<grid_for(m * Kq, 256), 256, 0, s>>>(m, Kp, Kq, dmap.p, P.mr_r32.p, tmp32.p,
+                                                             nullptr);
+    std::swap(P.mr_r32, tmp32);
     AIRT_LAUNCH_CHECK();
     // per-slot state: every running instance has the same iteration count
     std::vector<int> zero(Kq, 0), its(Kq, 0);
@@ -517,7 +526,6 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K0, const double *d_B, 
     Kp = Kq;
     grids(gf, gb);
     P.mr_part.ensure((size_t)gf * Kp);
-    P.mr_r32.ensure((size_t)m * Kp);
     a = args();
     capture();
     return true;

@@ -185,16 +185,19 @@ __device__ __forceinline__ void for_each_segment_vpre(int64_t nseg, const int64_
 // groups walk the *ntiles listed tiles (tiles[0 .. *ntiles)), so ranges left
 // out of the list cost nothing, and segments for which active(i) is false
 // are skipped without touching their nonzeros (all lanes of a group evaluate
-// it, so the group stays converged).  epi(i, sum, lead) sees lead = false
-// for skipped segments.
-template <int LANES, typename TX, class Act, class Epi>
+// it, so the group stays converged).  The segment bounds are loaded
+// together with the predicate's operands, not after them, and the leader's
+// pre(i) (the epilogue's per-segment operands) is issued before the
+// segment's loads; epi(i, sum, lead, pre_value) sees lead = false for
+// skipped segments.
+template <int LANES, typename TX, class Act, class Pre, class Epi>
 __device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__restrict__ tiles,
                                                     const int *__restrict__ ntiles, int tshift,
                                                     const int64_t *__restrict__ ptr,
                                                     const int *__restrict__ idx,
                                                     const float *__restrict__ val,
                                                     const TX *__restrict__ x, Act &&active,
-                                                    Epi &&epi) {
+                                                    Pre &&pre, Epi &&epi) {
   const int lane = threadIdx.x % LANES;
   const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / LANES;
   const int64_t ng = (int64_t)gridDim.x * blockDim.x / LANES;
@@ -206,10 +209,17 @@ __device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__r
   for (int64_t t = 0; t < trips; ++t) {
     const int64_t u = gid + t * ng;
     const int64_t i = u < total ? ((int64_t)__ldg(tiles + (u >> tshift)) << tshift) + (u & tmask) : nseg;
-    const bool on = i < nseg && active(i);
+    bool on = false;
+    int64_t q0 = 0, q1 = 0;
+    decltype(pre(i)) pv{};
+    if (i < nseg) {
+      q0 = __ldg(ptr + i);
+      q1 = __ldg(ptr + i + 1);
+      on = active(i);
+      if (on && lane == 0) pv = pre(i);
+    }
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (on) {
-      const int64_t q0 = __ldg(ptr + i), q1 = __ldg(ptr + i + 1);
       int64_t qa = (q0 + 3) & ~(int64_t)3;
       if (qa > q1) qa = q1;
       int64_t qb = q1 & ~(int64_t)3;
@@ -248,7 +258,7 @@ __device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__r
     }
     double acc = (a0 + a1) + (a2 + a3);
     acc = group_sum<LANES>(acc);
-    epi(i, acc, lane == 0 && on);
+    epi(i, acc, lane == 0 && on, pv);
   }
 }
 

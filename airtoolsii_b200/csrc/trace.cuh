@@ -124,20 +124,28 @@ __device__ __forceinline__ void trace_segments(int N, const Ray &q, bool exclude
   bool have_pend = false, have_last = false;
   double px = 0, py = 0, lx = 0, ly = 0;
   while (cx < nx || cy < ny) {
-    double xx, yy;
-    if (cy >= ny || (cx < nx && tx <= ty)) {
-      xx = (double)ix - h;
-      yy = __dadd_rn(__dmul_rn(q.b, tx), q.y0t);
+    // The next point comes from the x family (x-crossing first on equal t)
+    // or the y family.  The step is written with selected operands, so that
+    // the lanes of a warp, whose rays sit at different crossings, run one
+    // multiply-add and one division per step instead of both branches.
+    const bool takex = cy >= ny || (cx < nx && tx <= ty);
+    const double t = takex ? tx : ty;
+    const double fixed = (double)(takex ? ix : iy) - h;
+    const double other = __dadd_rn(__dmul_rn(takex ? q.b : q.a, t), takex ? q.y0t : q.x0t);
+    const double xx = takex ? fixed : other;
+    const double yy = takex ? other : fixed;
+    if (takex) {
       ++cx;
       ix += sx;
-      if (cx < nx) tx = __ddiv_rn(__dsub_rn((double)ix - h, q.x0t), q.a);
     } else {
-      yy = (double)iy - h;
-      xx = __dadd_rn(__dmul_rn(q.a, ty), q.x0t);
       ++cy;
       iy += sy;
-      if (cy < ny) ty = __ddiv_rn(__dsub_rn((double)iy - h, q.y0t), q.b);
     }
+    // the family's next crossing parameter (unused once the family is spent)
+    const double tn = __ddiv_rn(__dsub_rn((double)(takex ? ix : iy) - h, takex ? q.x0t : q.y0t),
+                                takex ? q.a : q.b);
+    if (takex) tx = tn;
+    else ty = tn;
     if (!(xx >= -h && xx <= h && yy >= -h && yy <= h)) continue;
     if (have_pend) {
       const bool close = fabs(__dsub_rn(xx, px)) <= 1e-10 && fabs(__dsub_rn(yy, py)) <= 1e-10;
