@@ -382,10 +382,12 @@ struct RowsGeo {
 
 constexpr int kRowsMaxStages = 8;
 
-template <int SWA>
+// ONE: a single strip per input row also for 64-byte pixel rows, the middle
+// tap reading it one pixel row (64 bytes) further on.
+template <int SWA, bool ONE>
 struct RowsCfg {
   static constexpr int KS = SWA / 2;
-  static constexpr int STRIPS = SWA == 128 ? 1 : 2;
+  static constexpr int STRIPS = SWA == 128 || ONE ? 1 : 2;
   static constexpr uint32_t STRIP_BYTES = round1k((uint32_t)kStripRows * SWA);
 };
 
@@ -414,11 +416,11 @@ struct RowsRoles {
   static constexpr uint32_t TMEM_COLS = (uint32_t)(NACC * BN);
 };
 
-template <int BN, int EPI, int SWA>
+template <int BN, int EPI, int SWA, bool ONE>
 __global__ void __launch_bounds__(RowsRoles<BN>::THREADS, 1)
     k_conv_rows(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmArgs g,
                 RowsGeo geo) {
-  using Cfg = RowsCfg<SWA>;
+  using Cfg = RowsCfg<SWA, ONE>;
   using Ro = RowsRoles<BN>;
   constexpr int KS = Cfg::KS, STRIPS = Cfg::STRIPS, NACC = Ro::NACC, NE = Ro::NE;
   constexpr uint32_t STRIP = Cfg::STRIP_BYTES;
@@ -708,6 +710,7 @@ bool conv3x3_tma_ok(const GemmArgs &g) {
 }
 
 int g_conv_halo = 2;
+int g_conv_one_strip = 0;
 
 // MODE_HALO launch: tiles lie within one image row (W % 128 == 0) and the
 // channels fill whole 64- or 128-byte rows.
@@ -737,10 +740,10 @@ static bool conv3x3_halo(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   return true;
 }
 
-template <int BN, int EPI, int SWA>
+template <int BN, int EPI, int SWA, bool ONE>
 static void launch_rows(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, const RowsGeo &geo,
                         size_t smem, int ctas, cudaStream_t s) {
-  auto kern = k_conv_rows<BN, EPI, SWA>;
+  auto kern = k_conv_rows<BN, EPI, SWA, ONE>;
   AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<ctas, RowsRoles<BN>::THREADS, smem, s>>>(ma, mb, g, geo);
   AIRT_LAUNCH_CHECK();
@@ -758,7 +761,8 @@ static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   geo.H = H;
   geo.cch = C / ks;
   const uint32_t strip = round1k((uint32_t)kStripRows * sw);
-  geo.stage_bytes = (uint32_t)geo.cch * (sw == 128 ? 1u : 2u) * strip;
+  const bool one = sw == 64 && g_conv_one_strip;
+  geo.stage_bytes = (uint32_t)geo.cch * (sw == 128 || one ? 1u : 2u) * strip;
   geo.w_bytes = (uint32_t)(9 * geo.cch) * (uint32_t)bn * (uint32_t)sw;
   const uint32_t half = 112640u, whole = 225280u;  // per-CTA budgets: two CTAs or one per SM
   int per_sm = 2;
@@ -792,25 +796,33 @@ static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const cuuint32_t bwt[2] = {(cuuint32_t)ks, (cuuint32_t)bn};
   const CUtensorMap mb = make_map(g.B, 2, dw, swt, bwt, sw);
   const int grid = std::max(1, std::min(geo.nunits, ctas));
-#define AIRT_R(BNV, SWV)                                                                                  \
+#define AIRT_R(BNV, SWV, ONEV)                                                                            \
   switch (epi) {                                                                                          \
-    case EPI_STORE_F32: launch_rows<BNV, EPI_STORE_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;       \
-    case EPI_BIAS_RELU_BF16: launch_rows<BNV, EPI_BIAS_RELU_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break; \
-    case EPI_BIAS_BF16: launch_rows<BNV, EPI_BIAS_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break;       \
-    case EPI_ADD_F32: launch_rows<BNV, EPI_ADD_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;           \
+    case EPI_STORE_F32: launch_rows<BNV, EPI_STORE_F32, SWV, ONEV>(ma, mb, g, geo, smem, grid, s); break; \
+    case EPI_BIAS_RELU_BF16:                                                                              \
+      launch_rows<BNV, EPI_BIAS_RELU_BF16, SWV, ONEV>(ma, mb, g, geo, smem, grid, s);                     \
+      break;                                                                                              \
+    case EPI_BIAS_BF16: launch_rows<BNV, EPI_BIAS_BF16, SWV, ONEV>(ma, mb, g, geo, smem, grid, s); break; \
+    case EPI_ADD_F32: launch_rows<BNV, EPI_ADD_F32, SWV, ONEV>(ma, mb, g, geo, smem, grid, s); break;     \
     default: return false;                                                                                \
   }
   if (sw == 128) {
     switch (bn) {
-      case 32: AIRT_R(32, 128) break;
-      case 64: AIRT_R(64, 128) break;
-      default: AIRT_R(128, 128) break;
+      case 32: AIRT_R(32, 128, false) break;
+      case 64: AIRT_R(64, 128, false) break;
+      default: AIRT_R(128, 128, false) break;
+    }
+  } else if (one) {
+    switch (bn) {
+      case 32: AIRT_R(32, 64, true) break;
+      case 64: AIRT_R(64, 64, true) break;
+      default: AIRT_R(128, 64, true) break;
     }
   } else {
     switch (bn) {
-      case 32: AIRT_R(32, 64) break;
-      case 64: AIRT_R(64, 64) break;
-      default: AIRT_R(128, 64) break;
+      case 32: AIRT_R(32, 64, false) break;
+      case 64: AIRT_R(64, 64, false) break;
+      default: AIRT_R(128, 64, false) break;
     }
   }
 #undef AIRT_R

@@ -286,5 +286,8 @@ extern int g_gemm_path;
 // tile; 1 = halo strips where W % 128 == 0 (else tap boxes); 2 = row runs
 // with resident weights where they fit (else halo strips, else tap boxes).
 extern int g_conv_halo;
+// Row runs with 64-byte pixel rows: 1 = one strip per input row (the middle
+// tap one pixel row into it), 0 = a second strip one pixel later.
+extern int g_conv_one_strip;
 
 }  // namespace airt

@@ -287,7 +287,9 @@ __global__ void k_up_concat_back(int B, int H, int W, int C1, int C2, const floa
 }
 
 // head: out[p] = b + sum_c w[c]*Y[p][c] (channels in order), one pixel per
-// thread, 8 channels per 16-byte load.
+// thread, 8 channels per 16-byte load.  With the channel count a template
+// constant every 16-byte load of a pixel is issued before the first FMA and
+// the weights sit in registers.
 __global__ void k_head(int64_t P, int C, const __nv_bfloat16 *__restrict__ Y, const float *__restrict__ w,
                        const float *__restrict__ b, float *__restrict__ out) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
@@ -298,6 +300,31 @@ __global__ void k_head(int64_t P, int C, const __nv_bfloat16 *__restrict__ Y, co
       bf8_to_f(*reinterpret_cast<const uint4 *>(Y + p * C + cg * 8), y);
 #pragma unroll
       for (int j = 0; j < 8; ++j) a += w[cg * 8 + j] * y[j];
+    }
+    out[p] = a;
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(256) k_head_c(int64_t P, const __nv_bfloat16 *__restrict__ Y,
+                                                const float *__restrict__ w, const float *__restrict__ b,
+                                                float *__restrict__ out) {
+  float wr[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) wr[c] = __ldg(w + c);
+  const float b0 = __ldg(b);
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    uint4 u[C / 8];
+#pragma unroll
+    for (int cg = 0; cg < C / 8; ++cg) u[cg] = __ldg(reinterpret_cast<const uint4 *>(Y + p * C) + cg);
+    float a = b0;
+#pragma unroll
+    for (int cg = 0; cg < C / 8; ++cg) {
+      float y[8];
+      bf8_to_f(u[cg], y);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) a += wr[cg * 8 + j] * y[j];
     }
     out[p] = a;
   }
@@ -384,6 +411,61 @@ __global__ void k_conv1_fwd(int64_t P, int H, int W, int Co, int Kp, const __nv_
       o[j] = fmaxf(a + sb[co], 0.f);
     }
     reinterpret_cast<uint4 *>(y)[t] = f_to_bf8(o);
+  }
+}
+
+// The same convolution with all Co (a template constant) output channels of
+// one pixel per thread: the nine neighbours are loaded once, the weights are
+// read from shared memory as [tap][co] float4 broadcasts, and the pixel's
+// Co channels leave as 16-byte stores.  Per channel the sum runs over the
+// taps in the same order as k_conv1_fwd.
+template <int CO>
+__global__ void __launch_bounds__(256) k_conv1_fwd_px(int P, int H, int W, int Kp,
+                                                      const __nv_bfloat16 *__restrict__ x,
+                                                      const __nv_bfloat16 *__restrict__ wt,
+                                                      const float *__restrict__ bias,
+                                                      __nv_bfloat16 *__restrict__ y) {
+  __shared__ __align__(16) float sw[9 * CO];
+  __shared__ __align__(16) float sb[CO];
+  for (int i = threadIdx.x; i < CO * 9; i += blockDim.x) {
+    const int tap = i / CO, co = i % CO;
+    sw[i] = __bfloat162float(wt[(int64_t)co * Kp + tap]);
+  }
+  for (int i = threadIdx.x; i < CO; i += blockDim.x) sb[i] = bias[i];
+  __syncthreads();
+  const int HW = H * W;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int q = p % HW, h = q / W, w = q - h * W;
+    float xv[9];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+      const bool in = h + dh >= 0 && h + dh < H && w + dw >= 0 && w + dw < W;
+      xv[tap] = in ? __bfloat162float(x[p + dh * W + dw]) : 0.f;
+    }
+    float a[CO];
+#pragma unroll
+    for (int co = 0; co < CO; ++co) a[co] = 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const float4 *w4 = reinterpret_cast<const float4 *>(sw + tap * CO);
+#pragma unroll
+      for (int c4 = 0; c4 < CO / 4; ++c4) {
+        const float4 wv = w4[c4];
+        a[4 * c4] += wv.x * xv[tap];
+        a[4 * c4 + 1] += wv.y * xv[tap];
+        a[4 * c4 + 2] += wv.z * xv[tap];
+        a[4 * c4 + 3] += wv.w * xv[tap];
+      }
+    }
+    uint4 *yo = reinterpret_cast<uint4 *>(y + (int64_t)p * CO);
+#pragma unroll
+    for (int g8 = 0; g8 < CO / 8; ++g8) {
+      float o[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) o[j] = fmaxf(a[g8 * 8 + j] + sb[g8 * 8 + j], 0.f);
+      yo[g8] = f_to_bf8(o);
+    }
   }
 }
 
@@ -548,8 +630,13 @@ void row_blocks(int64_t P, int64_t &blocks, int64_t &rpb) {
 void conv_forward(UNet &U, Conv &c, int B) {
   const int64_t P = (int64_t)B * c.H * c.W;
   if (c.cin == 1 && c.cout % 8 == 0) {  // first convolution: direct kernel
-    k_conv1_fwd<<<gsz(P * c.cout / 8), kT, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, c.in->y.p, c.w16.p, c.b.p,
-                                                     c.out->y.p);
+    if (c.cout == 32)
+      k_conv1_fwd_px<32><<<gsz(P), kT, 0, U.s>>>((int)P, c.H, c.W, c.kp, c.in->y.p, c.w16.p, c.b.p, c.out->y.p);
+    else if (c.cout == 16)
+      k_conv1_fwd_px<16><<<gsz(P), kT, 0, U.s>>>((int)P, c.H, c.W, c.kp, c.in->y.p, c.w16.p, c.b.p, c.out->y.p);
+    else
+      k_conv1_fwd<<<gsz(P * c.cout / 8), kT, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, c.in->y.p, c.w16.p, c.b.p,
+                                                       c.out->y.p);
     AIRT_LAUNCH_CHECK();
     return;
   }
@@ -858,7 +945,9 @@ void unet_forward_body(UNet &U, int B) {
     conv_forward(U, U.convs[ci++], B);
     conv_forward(U, U.convs[ci++], B);
   }
-  k_head<<<gsz(P0), kT, 0, U.s>>>(P0, U.base, U.db[0]->y.p, U.hw.p, U.hb.p, U.out.p);
+  if (U.base == 32) k_head_c<32><<<gsz(P0), kT, 0, U.s>>>(P0, U.db[0]->y.p, U.hw.p, U.hb.p, U.out.p);
+  else if (U.base == 16) k_head_c<16><<<gsz(P0), kT, 0, U.s>>>(P0, U.db[0]->y.p, U.hw.p, U.hb.p, U.out.p);
+  else k_head<<<gsz(P0), kT, 0, U.s>>>(P0, U.base, U.db[0]->y.p, U.hw.p, U.hb.p, U.out.p);
   AIRT_LAUNCH_CHECK();
 }
 

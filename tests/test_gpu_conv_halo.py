@@ -33,7 +33,7 @@ def _run(net, x, t, B):
     return out.cpu().numpy().astype(np.float64), loss, net.get_grads().astype(np.float64)
 
 
-@pytest.mark.parametrize("mode", [1, 2], ids=["halo", "rows"])
+@pytest.mark.parametrize("mode", [1, 2, 6], ids=["halo", "rows", "rows_one_strip"])
 @pytest.mark.parametrize("H,W,base,levels,B", [(256, 256, 32, 2, 2), (128, 256, 16, 2, 2),
                                                (128, 128, 32, 2, 2), (100, 128, 32, 2, 16)])
 def test_halo_conv_matches_tap_boxes(mode, H, W, base, levels, B):
