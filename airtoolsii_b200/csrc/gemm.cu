@@ -359,9 +359,9 @@ extern "C" int airt_test_gemm_path(int path) {
 }
 
 // Test hook: operand form of the TMA 3x3 convolution (see g_conv_halo).
-// mode 0-2: g_conv_halo; + 4: one strip per input row in the row runs.
+// mode 0-3: g_conv_halo; + 4: one strip per input row in the row runs.
 extern "C" int airt_test_conv_halo(int mode) {
-  if (mode < 0 || (mode & 3) > 2 || mode > 6) return AIRT_ERR_ARG;
+  if (mode < 0 || mode > 7) return AIRT_ERR_ARG;
   airt::g_conv_halo = mode & 3;
   airt::g_conv_one_strip = (mode & 4) ? 1 : 0;
   return AIRT_OK;

@@ -577,6 +577,220 @@ __global__ void __launch_bounds__(RowsRoles<BN>::THREADS, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Ro::TMEM_COLS));
 }
 
+// ---------------------------------------------------------------- stacked rows
+// Row runs with the three kernel rows stacked along N.  An input row r of a
+// run feeds output rows r-2, r-1 and r (kernel rows 2, 1, 0); with the
+// weights of one tap column laid out as [W(dh=2); W(dh=1); W(dh=0)] (3 BN
+// rows) one MMA of N = 3 BN multiplies the input row's strip once into the
+// accumulators of all three output rows, which sit side by side in a ring
+// of RB TMEM blocks (output row ol in block ol % RB).  The A tile (128
+// pixels x 16 channels, 4 KB) is read from shared memory once per three
+// kernel rows instead of once per kernel row, so the MMAs are no longer
+// bound by shared-memory operand bandwidth at small BN.  All MMAs
+// accumulate: the epilogue zeroes a block after draining it (and every block
+// once at the start) before handing it back.  An input row's stage is free
+// as soon as its own MMAs complete; output row i is complete after input row
+// i + 2.  At the run's ends and where the three blocks wrap around the ring
+// the MMA covers fewer rows (N = BN or 2 BN) or splits in two.
+__device__ __forceinline__ uint32_t idesc_n(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+      "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr),
+      "r"(0u)
+      : "memory");
+}
+
+template <int BN>
+struct StackRoles {
+  static constexpr int NE = 2;                   // epilogue groups of four warps
+  static constexpr int RB = 256 / BN;            // TMEM blocks (256 columns: two CTAs per SM)
+  static constexpr int THREADS = 64 + 128 * NE;
+  static constexpr uint32_t TMEM_COLS = 256;
+};
+
+template <int BN, int EPI, int SWA>
+__global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
+    k_conv_stack(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmArgs g,
+                 RowsGeo geo) {
+  using Cfg = RowsCfg<SWA, false>;
+  using Ro = StackRoles<BN>;
+  constexpr int KS = Cfg::KS, STRIPS = Cfg::STRIPS, RB = Ro::RB, NE = Ro::NE;
+  constexpr uint32_t STRIP = Cfg::STRIP_BYTES;
+  static_assert(3 * BN <= 256, "N = 3 BN must fit one MMA");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t wbase = smem_addr(base);
+  const uint32_t rbase = wbase + geo.w_bytes;
+  __shared__ __align__(8) uint64_t full[kRowsMaxStages], empty[kRowsMaxStages], acc_full[RB], acc_empty[RB],
+      wfull;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  volatile int *abort_flag = &s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = geo.S;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&s_tmem)),
+                 "r"(Ro::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int i = 0; i < S; ++i) {
+      mbar_init(smem_addr(&full[i]), 1);
+      mbar_init(smem_addr(&empty[i]), 1);
+    }
+    for (int i = 0; i < RB; ++i) {
+      mbar_init(smem_addr(&acc_full[i]), 1);
+      mbar_init(smem_addr(&acc_empty[i]), 128);
+    }
+    mbar_init(smem_addr(&wfull), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&mapA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&mapB) : "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer: weight slabs [dw][cc][dh = 2, 1, 0], then one
+      // stage per input row
+      const uint32_t wb = smem_addr(&wfull);
+      expect_tx(wb, geo.w_bytes);
+      for (int dw = 0; dw < 3; ++dw)
+        for (int cc = 0; cc < geo.cch; ++cc)
+          for (int dh = 0; dh < 3; ++dh)
+            tma2d(wbase + (uint32_t)((dw * geo.cch + cc) * 3 + (2 - dh)) * (BN * SWA), &mapB,
+                  ((3 * dh + dw) * geo.cch + cc) * KS, 0, wb);
+      const uint32_t tx = (uint32_t)(geo.cch * STRIPS * kStripBox * SWA);
+      uint32_t it = 0;
+      for (int u = blockIdx.x; u < geo.nunits && !*abort_flag; u += gridDim.x) {
+        const RowsUnit ru = rows_unit(geo, u);
+        bool ok = true;
+        for (int r = 0; r < ru.rows + 2; ++r, ++it) {
+          const uint32_t st = it % S;
+          if (it >= (uint32_t)S && !mbar_wait(smem_addr(&empty[st]), ((it / S) - 1) & 1u)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = rbase + st * geo.stage_bytes, bar = smem_addr(&full[st]);
+          expect_tx(bar, tx);
+          for (int cc = 0; cc < geo.cch; ++cc)
+#pragma unroll
+            for (int q = 0; q < STRIPS; ++q)
+              tma4d(sa + (uint32_t)(cc * STRIPS + q) * STRIP, &mapA, cc * KS, ru.w0 - 1 + q, ru.h0 - 1 + r, ru.b,
+                    bar);
+        }
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer: one step per input row r of a run
+      const uint64_t wdesc = make_desc_sw<SWA>(wbase, 16, 8 * SWA);
+      bool ok = mbar_wait(smem_addr(&wfull), 0);
+      uint32_t it = 0, ol0 = 0;  // stage counter; sequence number of the run's first output row
+      for (int u = blockIdx.x; ok && u < geo.nunits && !*abort_flag; u += gridDim.x) {
+        const RowsUnit ru = rows_unit(geo, u);
+        for (int r = 0; ok && r < ru.rows + 2; ++r, ++it) {
+          // a new output row (r) starts here: its block must be drained and zeroed
+          if (r < ru.rows) {
+            const uint32_t ol = ol0 + r;
+            if (!mbar_wait(smem_addr(&acc_empty[ol % RB]), (ol / RB) & 1u)) {
+              ok = false;
+              break;
+            }
+          }
+          if (!mbar_wait(smem_addr(&full[it % S]), (it / S) & 1u)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const int lo = max(0, r - 2), hi = min(ru.rows - 1, r);
+          const uint64_t sdesc = make_desc_sw<SWA>(rbase + (it % S) * geo.stage_bytes, 16, 8 * SWA);
+          // the covered blocks, split where they wrap around the ring
+          const int b_lo = (int)((ol0 + lo) % RB);
+          const int n1 = min(hi - lo + 1, RB - b_lo);  // rows before the wrap
+          for (int part = 0; part < 2; ++part) {
+            const int first = part == 0 ? lo : lo + n1;
+            const int cnt = part == 0 ? n1 : hi - lo + 1 - n1;
+            if (cnt <= 0) continue;
+            const uint32_t dtm = tmem + (uint32_t)((ol0 + first) % RB) * BN;
+            const uint32_t idesc = idesc_n(cnt * BN);
+            const int s0 = first - r + 2;  // slab block of output row `first`
+            for (int cc = 0; cc < geo.cch; ++cc) {
+              const uint64_t cdesc = sdesc + ((uint64_t)(cc * STRIPS) * STRIP >> 4);
+#pragma unroll
+              for (int dw = 0; dw < 3; ++dw) {
+                const uint64_t da = cdesc + ((STRIPS == 2 && dw == 1 ? STRIP : (uint32_t)dw * SWA) >> 4);
+                const uint64_t db =
+                    wdesc + ((uint64_t)((dw * geo.cch + cc) * 3 + s0) * (BN * SWA) >> 4);
+#pragma unroll
+                for (int kk = 0; kk < KS / 16; ++kk) mma_bf16(dtm, da + 2 * kk, db + 2 * kk, idesc, 1u);
+              }
+            }
+          }
+          commit(smem_addr(&empty[it % S]));  // this input row has no other reader
+          if (r >= 2) commit(smem_addr(&acc_full[(ol0 + r - 2) % RB]));  // output row r - 2 is complete
+        }
+        ol0 += ru.rows;
+      }
+      if (!ok) *abort_flag = 1;
+    }
+  } else {
+    // ---- epilogue groups: group e drains the output rows ol with
+    // ol % NE == e, i.e. the blocks b with b % NE == e (RB is a multiple of
+    // NE); warp w reads and zeroes TMEM lanes 32 * (w % 4) ..
+    const int quad = warp & 3, grp = (warp - 2) >> 2;
+    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
+    auto zero_block = [&](int b) {
+#pragma unroll
+      for (int c = 0; c < BN; c += 32) tmem_zero32(lane_base + (uint32_t)(b * BN + c));
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    };
+    for (int b = grp; b < RB; b += NE) {
+      zero_block(b);
+      mbar_arrive_plain(smem_addr(&acc_empty[b]));
+    }
+    uint32_t ol = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; ok && u < geo.nunits; u += gridDim.x) {
+      const RowsUnit ru = rows_unit(geo, u);
+      for (int i = 0; i < ru.rows; ++i, ++ol) {
+        if ((int)(ol % NE) != grp) continue;
+        const int b = (int)(ol % RB);
+        if (!mbar_wait(smem_addr(&acc_full[b]), (ol / RB) & 1u)) {
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int m0 = ((ru.b * geo.H + ru.h0 + i) * geo.W) + ru.w0;
+        gemm_epilogue<BN, EPI>(g, lane_base + (uint32_t)(b * BN), m0 + quad * 32 + lane, 0, true);
+        zero_block(b);
+        mbar_arrive_plain(smem_addr(&acc_empty[b]));
+      }
+    }
+  }
+  __syncthreads();
+  if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Ro::TMEM_COLS));
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -709,7 +923,7 @@ bool conv3x3_tma_ok(const GemmArgs &g) {
          g.ldb % 8 == 0 && g.M % (g.conv_H * g.conv_W) == 0 && pixel_box(128, g.conv_H, g.conv_W, bw, bh, bb);
 }
 
-int g_conv_halo = 2;
+int g_conv_halo = 3;
 int g_conv_one_strip = 0;
 
 // MODE_HALO launch: tiles lie within one image row (W % 128 == 0) and the
@@ -755,7 +969,7 @@ static void launch_rows(const CUtensorMap &ma, const CUtensorMap &mb, const Gemm
 static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
   const int sw = swizzle_for(C), ks = sw / 2;
-  if (g_conv_halo != 2 || W % 128 != 0 || sw < 64 || W > 4096 || g.N != bn || bn > 128) return false;
+  if (g_conv_halo < 2 || W % 128 != 0 || sw < 64 || W > 4096 || g.N != bn || bn > 128) return false;
   RowsGeo geo{};
   geo.W = W;
   geo.H = H;
@@ -829,8 +1043,80 @@ static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   return true;
 }
 
+template <int BN, int EPI, int SWA>
+static void launch_stack(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, const RowsGeo &geo,
+                         size_t smem, int ctas, cudaStream_t s) {
+  auto kern = k_conv_stack<BN, EPI, SWA>;
+  AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ctas, StackRoles<BN>::THREADS, smem, s>>>(ma, mb, g, geo);
+  AIRT_LAUNCH_CHECK();
+}
+
+// Stacked row-run launch (k_conv_stack): as the row runs, with BN = 32 or 64
+// (N = 3 BN <= 256) and 256 TMEM columns per CTA.
+static bool conv3x3_stack(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
+  const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);
+  const int sw = swizzle_for(C), ks = sw / 2;
+  if (g_conv_halo != 3 || W % 128 != 0 || sw < 64 || W > 4096 || g.N != bn || (bn != 32 && bn != 64))
+    return false;
+  RowsGeo geo{};
+  geo.W = W;
+  geo.H = H;
+  geo.cch = C / ks;
+  const uint32_t strip = round1k((uint32_t)kStripRows * sw);
+  geo.stage_bytes = (uint32_t)geo.cch * (sw == 128 ? 1u : 2u) * strip;
+  geo.w_bytes = (uint32_t)(9 * geo.cch) * (uint32_t)bn * (uint32_t)sw;
+  const uint32_t half = 112640u, whole = 225280u;
+  int per_sm = 2;
+  uint32_t budget = half;
+  if (geo.w_bytes + 4 * geo.stage_bytes + 1024 > half) {
+    per_sm = 1;
+    budget = whole;
+  }
+  if (geo.w_bytes + 4 * geo.stage_bytes + 1024 > budget) return false;
+  geo.S = std::min<int>(kRowsMaxStages, (int)((budget - 1024 - geo.w_bytes) / geo.stage_bytes));
+  const size_t smem = (size_t)geo.w_bytes + (size_t)geo.S * geo.stage_bytes + 1024;
+  geo.segs = W / 128;
+  const int ctas = sm_count() * per_sm;
+  long best = -1;
+  for (int R = 1; R <= H; R *= 2) {
+    const long units = (long)Bimg * geo.segs * ((H + R - 1) / R);
+    const long cost = ((units + ctas - 1) / ctas) * (R + 2);
+    if (best < 0 || cost < best) {
+      best = cost;
+      geo.R = R;
+    }
+  }
+  geo.hblocks = (H + geo.R - 1) / geo.R;
+  geo.nunits = Bimg * geo.segs * geo.hblocks;
+  const cuuint64_t dx[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
+  const cuuint64_t sx[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t bx[4] = {(cuuint32_t)ks, (cuuint32_t)kStripBox, 1, 1};
+  const CUtensorMap ma = make_map(g.convX, 4, dx, sx, bx, sw);
+  const cuuint64_t dw[2] = {(cuuint64_t)9 * C, (cuuint64_t)g.N}, swt[1] = {(cuuint64_t)g.ldb * 2};
+  const cuuint32_t bwt[2] = {(cuuint32_t)ks, (cuuint32_t)bn};
+  const CUtensorMap mb = make_map(g.B, 2, dw, swt, bwt, sw);
+  const int grid = std::max(1, std::min(geo.nunits, ctas));
+#define AIRT_S(BNV, SWV)                                                                                  \
+  switch (epi) {                                                                                          \
+    case EPI_STORE_F32: launch_stack<BNV, EPI_STORE_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;      \
+    case EPI_BIAS_RELU_BF16: launch_stack<BNV, EPI_BIAS_RELU_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break; \
+    case EPI_BIAS_BF16: launch_stack<BNV, EPI_BIAS_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break;      \
+    case EPI_ADD_F32: launch_stack<BNV, EPI_ADD_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;          \
+    default: return false;                                                                                \
+  }
+  if (sw == 128) {
+    if (bn == 32) { AIRT_S(32, 128) } else { AIRT_S(64, 128) }
+  } else {
+    if (bn == 32) { AIRT_S(32, 64) } else { AIRT_S(64, 64) }
+  }
+#undef AIRT_S
+  return true;
+}
+
 void conv3x3_bf16_tma(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   AIRT_REQUIRE(conv3x3_tma_ok(g), "conv3x3: shape unsuitable for TMA");
+  if (conv3x3_stack(g, bn, epi, s)) return;
   if (conv3x3_rows(g, bn, epi, s)) return;
   if (conv3x3_halo(g, bn, epi, s)) return;
   const int C = g.conv_C, H = g.conv_H, W = g.conv_W, Bimg = g.M / (H * W);

@@ -284,7 +284,9 @@ void conv3x3_wgrad_bf16_tma(const GemmArgs &g, int bn, cudaStream_t s);
 extern int g_gemm_path;
 // 3x3 convolution operand form on the TMA path: 0 = nine tap boxes per
 // tile; 1 = halo strips where W % 128 == 0 (else tap boxes); 2 = row runs
-// with resident weights where they fit (else halo strips, else tap boxes).
+// with resident weights where they fit (else halo strips, else tap boxes);
+// 3 = row runs with the kernel rows stacked along N where BN is 32 or 64
+// (else as 2).
 extern int g_conv_halo;
 // Row runs with 64-byte pixel rows: 1 = one strip per input row (the middle
 // tap one pixel row into it), 0 = a second strip one pixel later.

@@ -414,17 +414,20 @@ __global__ void k_conv1_fwd(int64_t P, int H, int W, int Co, int Kp, const __nv_
   }
 }
 
-// The same convolution with all Co (a template constant) output channels of
-// one pixel per thread: the nine neighbours are loaded once, the weights are
-// read from shared memory as [tap][co] float4 broadcasts, and the pixel's
-// Co channels leave as 16-byte stores.  Per channel the sum runs over the
-// taps in the same order as k_conv1_fwd.
-template <int CO>
-__global__ void __launch_bounds__(256) k_conv1_fwd_px(int P, int H, int W, int Kp,
-                                                      const __nv_bfloat16 *__restrict__ x,
-                                                      const __nv_bfloat16 *__restrict__ wt,
-                                                      const float *__restrict__ bias,
-                                                      __nv_bfloat16 *__restrict__ y) {
+// The same convolution with CPT (a template constant, 16) output channels of
+// one pixel per thread (CO / CPT threads per pixel, so that three blocks fit
+// per SM): the nine neighbours are loaded once per thread, the weights are
+// read from shared memory as [tap][co] float4 broadcasts, and the channels
+// leave as 16-byte stores.  Per channel the sum runs over the taps in the
+// same order as k_conv1_fwd.
+template <int CO, int CPT>
+__global__ void __launch_bounds__(256, 3) k_conv1_fwd_px(int P, int H, int W, int Kp,
+                                                         const __nv_bfloat16 *__restrict__ x,
+                                                         const __nv_bfloat16 *__restrict__ wt,
+                                                         const float *__restrict__ bias,
+                                                         __nv_bfloat16 *__restrict__ y) {
+  static_assert(CO % CPT == 0 && CPT % 8 == 0, "channel split");
+  constexpr int G = CO / CPT;
   __shared__ __align__(16) float sw[9 * CO];
   __shared__ __align__(16) float sb[CO];
   for (int i = threadIdx.x; i < CO * 9; i += blockDim.x) {
@@ -434,7 +437,8 @@ __global__ void __launch_bounds__(256) k_conv1_fwd_px(int P, int H, int W, int K
   for (int i = threadIdx.x; i < CO; i += blockDim.x) sb[i] = bias[i];
   __syncthreads();
   const int HW = H * W;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P * G; t += gridDim.x * blockDim.x) {
+    const int p = t / G, c0 = (t - p * G) * CPT;
     const int q = p % HW, h = q / W, w = q - h * W;
     float xv[9];
 #pragma unroll
@@ -443,14 +447,14 @@ __global__ void __launch_bounds__(256) k_conv1_fwd_px(int P, int H, int W, int K
       const bool in = h + dh >= 0 && h + dh < H && w + dw >= 0 && w + dw < W;
       xv[tap] = in ? __bfloat162float(x[p + dh * W + dw]) : 0.f;
     }
-    float a[CO];
+    float a[CPT];
 #pragma unroll
-    for (int co = 0; co < CO; ++co) a[co] = 0.f;
+    for (int co = 0; co < CPT; ++co) a[co] = 0.f;
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
-      const float4 *w4 = reinterpret_cast<const float4 *>(sw + tap * CO);
+      const float4 *w4 = reinterpret_cast<const float4 *>(sw + tap * CO + c0);
 #pragma unroll
-      for (int c4 = 0; c4 < CO / 4; ++c4) {
+      for (int c4 = 0; c4 < CPT / 4; ++c4) {
         const float4 wv = w4[c4];
         a[4 * c4] += wv.x * xv[tap];
         a[4 * c4 + 1] += wv.y * xv[tap];
@@ -458,12 +462,12 @@ __global__ void __launch_bounds__(256) k_conv1_fwd_px(int P, int H, int W, int K
         a[4 * c4 + 3] += wv.w * xv[tap];
       }
     }
-    uint4 *yo = reinterpret_cast<uint4 *>(y + (int64_t)p * CO);
+    uint4 *yo = reinterpret_cast<uint4 *>(y + (int64_t)p * CO + c0);
 #pragma unroll
-    for (int g8 = 0; g8 < CO / 8; ++g8) {
+    for (int g8 = 0; g8 < CPT / 8; ++g8) {
       float o[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) o[j] = fmaxf(a[g8 * 8 + j] + sb[g8 * 8 + j], 0.f);
+      for (int j = 0; j < 8; ++j) o[j] = fmaxf(a[g8 * 8 + j] + sb[c0 + g8 * 8 + j], 0.f);
       yo[g8] = f_to_bf8(o);
     }
   }
@@ -631,9 +635,11 @@ void conv_forward(UNet &U, Conv &c, int B) {
   const int64_t P = (int64_t)B * c.H * c.W;
   if (c.cin == 1 && c.cout % 8 == 0) {  // first convolution: direct kernel
     if (c.cout == 32)
-      k_conv1_fwd_px<32><<<gsz(P), kT, 0, U.s>>>((int)P, c.H, c.W, c.kp, c.in->y.p, c.w16.p, c.b.p, c.out->y.p);
+      k_conv1_fwd_px<32, 16><<<gsz(2 * P), kT, 0, U.s>>>((int)P, c.H, c.W, c.kp, c.in->y.p, c.w16.p, c.b.p,
+                                                          c.out->y.p);
     else if (c.cout == 16)
-      k_conv1_fwd_px<16><<<gsz(P), kT, 0, U.s>>>((int)P, c.H, c.W, c.kp, c.in->y.p, c.w16.p, c.b.p, c.out->y.p);
+      k_conv1_fwd_px<16, 16><<<gsz(P), kT, 0, U.s>>>((int)P, c.H, c.W, c.kp, c.in->y.p, c.w16.p, c.b.p,
+                                                      c.out->y.p);
     else
       k_conv1_fwd<<<gsz(P * c.cout / 8), kT, 0, U.s>>>(P, c.H, c.W, c.cout, c.kp, c.in->y.p, c.w16.p, c.b.p,
                                                        c.out->y.p);

@@ -130,24 +130,25 @@ class UNet:
 
 
 def _timing_main():
-    """python -m airtoolsii_b200.unet [--batch B] [--reps R] [--conv tap|halo|rows|rows1]
+    """python -m airtoolsii_b200.unet [--batch B] [--reps R] [--conv tap|halo|rows|rows1|stack]
     [--forward-only]: device time per image of the forward pass and of one
     Adam training step of the N=256, 4-level, base-32 network (random
     inputs), CUDA events on its stream; --conv picks the operand form of the
     TMA 3x3 convolutions (default: row runs where they apply; rows1: row runs
-    with one strip per input row for 64-byte pixel rows)."""
+    with one strip per input row for 64-byte pixel rows; stack: row runs with
+    the kernel rows stacked along N)."""
     import argparse
     import torch
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--conv", choices=["default", "tap", "halo", "rows", "rows1"], default="default")
+    ap.add_argument("--conv", choices=["default", "tap", "halo", "rows", "rows1", "stack"], default="default")
     ap.add_argument("--forward-only", action="store_true")
     a = ap.parse_args()
     if a.conv != "default":
         f = lib().airt_test_conv_halo
         f.restype, f.argtypes = C.c_int, [C.c_int]
-        check(f({"tap": 0, "halo": 1, "rows": 2, "rows1": 6}[a.conv]))
+        check(f({"tap": 0, "halo": 1, "rows": 2, "rows1": 6, "stack": 3}[a.conv]))
     B = a.batch
     net = UNet(256, 256, 32, 4, B, 0)
     u = torch.rand(B, 65536, device="cuda")

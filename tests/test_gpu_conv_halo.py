@@ -1,7 +1,8 @@
 """The halo-strip forms of the TMA 3x3 convolution (images whose rows hold
 whole 128-pixel tiles: one 130-pixel strip per kernel row, the three taps
-read it through shifted descriptors; per output row, or per run of output
-rows with the weights resident) against the nine-tap-box form on the same
+read it through shifted descriptors; per output row, per run of output
+rows with the weights resident, or per run with the three kernel rows
+stacked along N) against the nine-tap-box form on the same
 network, inputs and weights: forward output, loss and every gradient
 tensor.  The two forms add the same products in a different order for
 inputs of more than one channel chunk, so the bar is the BF16-level one of
@@ -33,7 +34,7 @@ def _run(net, x, t, B):
     return out.cpu().numpy().astype(np.float64), loss, net.get_grads().astype(np.float64)
 
 
-@pytest.mark.parametrize("mode", [1, 2, 6], ids=["halo", "rows", "rows_one_strip"])
+@pytest.mark.parametrize("mode", [1, 2, 6, 3], ids=["halo", "rows", "rows_one_strip", "stacked"])
 @pytest.mark.parametrize("H,W,base,levels,B", [(256, 256, 32, 2, 2), (128, 256, 16, 2, 2),
                                                (128, 128, 32, 2, 2), (100, 128, 32, 2, 16)])
 def test_halo_conv_matches_tap_boxes(mode, H, W, base, levels, B):
@@ -48,7 +49,7 @@ def test_halo_conv_matches_tap_boxes(mode, H, W, base, levels, B):
         _hook("airt_test_conv_halo", mode)
         o1, l1, g1 = _run(net, x, t, B)
     finally:
-        _hook("airt_test_conv_halo", 2)      # the library default
+        _hook("airt_test_conv_halo", 3)      # the library default
     assert np.linalg.norm(o1 - o0) <= 1e-2 * np.linalg.norm(o0)
     assert abs(l1 - l0) <= 1e-3 * abs(l0)
     off = 0
