@@ -75,6 +75,12 @@ struct Batch {
   // tcount[c] row tiles, tcount[kClasses + c] column tiles of class c
   DevBuf<int> tcount;
   int wmethod = -1;  // method whose M and D are in P.M / P.D (the matrix never changes)
+  // M and D of methods used earlier on this batch, saved when the batch
+  // switches to another method (the warm start alternates a SART step and
+  // cimmino solves: a copy instead of two passes over the matrix per switch)
+  static constexpr int kWCache = 8;
+  DevBuf<double> wc_M[kWCache], wc_D[kWCache];
+  bool wc_ok[kWCache] = {};
   // Kaczmarz level schedules (built on first use): per instance k, levels
   // kz_lev_ptr[base_k .. base_k + kz_nlev[k]] with base_k = row_off[k] + k,
   // row steps of level L at kz_steps[kz_lev_ptr[base_k + L] ..)
@@ -800,9 +806,23 @@ __global__ void k_fill1(int64_t n, double *__restrict__ a) {
 void batch_weights(Batch &B, int method) {
   Problem &P = B.P;
   if (B.wmethod == method) return;
+  cudaStream_t s = P.stream;
+  const int prev = B.wmethod;
+  if (prev >= 0 && prev < Batch::kWCache && !B.wc_ok[prev]) {
+    B.wc_M[prev].ensure(P.m);
+    B.wc_D[prev].ensure(P.n);
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(B.wc_M[prev].p, P.M.p, P.m * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(B.wc_D[prev].p, P.D.p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    B.wc_ok[prev] = true;
+  }
   P.M.ensure(P.m);
   P.D.ensure(P.n);
   B.wmethod = method;
+  if (method >= 0 && method < Batch::kWCache && B.wc_ok[method]) {
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(P.M.p, B.wc_M[method].p, P.m * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    AIRT_CHECK_CUDA(cudaMemcpyAsync(P.D.p, B.wc_D[method].p, P.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return;
+  }
   if (method != AIRT_CIMMINO) {
     compute_weights(P, method, P.M.p, P.D.p);
     return;

@@ -378,6 +378,7 @@ struct RowsGeo {
   int S;                   // ring stages
   uint32_t stage_bytes;    // one input row: cch * strips strips
   uint32_t w_bytes;        // resident weights: 9 * cch slices of BN x KS
+  int tma_out;             // k_conv_stack: BF16 output rows leave by TMA stores
 };
 
 constexpr int kRowsMaxStages = 8;
@@ -610,13 +611,28 @@ struct StackRoles {
   static constexpr int RB = 256 / BN;            // TMEM blocks (256 columns: two CTAs per SM)
   static constexpr int THREADS = 64 + 128 * NE;
   static constexpr uint32_t TMEM_COLS = 256;
+  // BN = 32: two CTAs per SM (their shared memory fits), so the registers
+  // of two 320-thread CTAs must fit as well
+  static constexpr int MIN_CTAS = BN == 32 ? 2 : 1;
 };
 
-template <int BN, int EPI, int SWA>
-__global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
-    k_conv_stack(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmArgs g,
-                 RowsGeo geo) {
-  using Cfg = RowsCfg<SWA, false>;
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void tma_store4d(const CUtensorMap *map, uint32_t src, int x, int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map), "r"(x),
+      "r"(y), "r"(z), "r"(w), "r"(src)
+      : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+template <int BN, int EPI, int SWA, bool ONE>
+__global__ void __launch_bounds__(StackRoles<BN>::THREADS, StackRoles<BN>::MIN_CTAS)
+    k_conv_stack(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                 const __grid_constant__ CUtensorMap mapD, GemmArgs g, RowsGeo geo) {
+  using Cfg = RowsCfg<SWA, ONE>;
   using Ro = StackRoles<BN>;
   constexpr int KS = Cfg::KS, STRIPS = Cfg::STRIPS, RB = Ro::RB, NE = Ro::NE;
   constexpr uint32_t STRIP = Cfg::STRIP_BYTES;
@@ -626,7 +642,7 @@ __global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
   const uint32_t wbase = smem_addr(base);
   const uint32_t rbase = wbase + geo.w_bytes;
   __shared__ __align__(8) uint64_t full[kRowsMaxStages], empty[kRowsMaxStages], acc_full[RB], acc_empty[RB],
-      wfull;
+      wfull, stg_free[NE], stg_full[NE];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   volatile int *abort_flag = &s_abort;
@@ -650,6 +666,10 @@ __global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
       mbar_init(smem_addr(&acc_empty[i]), 128);
     }
     mbar_init(smem_addr(&wfull), 1);
+    for (int e = 0; e < NE; ++e) {
+      mbar_init(smem_addr(&stg_free[e]), 1);
+      mbar_init(smem_addr(&stg_full[e]), 128);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&mapA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&mapB) : "memory");
@@ -751,9 +771,21 @@ __global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
   } else {
     // ---- epilogue groups: group e drains the output rows ol with
     // ol % NE == e, i.e. the blocks b with b % NE == e (RB is a multiple of
-    // NE); warp w reads and zeroes TMEM lanes 32 * (w % 4) ..
-    const int quad = warp & 3, grp = (warp - 2) >> 2;
+    // NE); warp w reads and zeroes TMEM lanes 32 * (w % 4) ..  With tma_out
+    // a row's BF16 result is written to the group's staging tile in the
+    // output map's swizzled layout and leaves by one TMA store (the bias
+    // comes from shared memory), instead of 16-byte stores per thread.
+    constexpr bool BF = EPI == EPI_BIAS_RELU_BF16 || EPI == EPI_BIAS_BF16;
+    constexpr int ROWB = BN * 2;  // bytes of one output pixel row
+    const int quad = warp & 3, grp = (warp - 2) >> 2, gtid = threadIdx.x - 64 - 128 * grp;
     const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
+    const bool tma_out = BF && geo.tma_out;
+    const uint32_t stg = rbase + (uint32_t)S * geo.stage_bytes + (uint32_t)grp * (128u * ROWB);
+    __shared__ __align__(16) float s_bias[64];
+    if (tma_out) {
+      if (threadIdx.x - 64 < BN) s_bias[threadIdx.x - 64] = g.bias ? g.bias[threadIdx.x - 64] : 0.f;
+      named_sync(3, 128 * NE);
+    }
     auto zero_block = [&](int b) {
 #pragma unroll
       for (int c = 0; c < BN; c += 32) tmem_zero32(lane_base + (uint32_t)(b * BN + c));
@@ -764,7 +796,7 @@ __global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
       zero_block(b);
       mbar_arrive_plain(smem_addr(&acc_empty[b]));
     }
-    uint32_t ol = 0;
+    uint32_t ol = 0, nst = 0;
     bool ok = true;
     for (int u = blockIdx.x; ok && u < geo.nunits; u += gridDim.x) {
       const RowsUnit ru = rows_unit(geo, u);
@@ -777,12 +809,68 @@ __global__ void __launch_bounds__(StackRoles<BN>::THREADS, 1)
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int m0 = ((ru.b * geo.H + ru.h0 + i) * geo.W) + ru.w0;
-        gemm_epilogue<BN, EPI>(g, lane_base + (uint32_t)(b * BN), m0 + quad * 32 + lane, 0, true);
+        if (!tma_out) {
+          const int m0 = ((ru.b * geo.H + ru.h0 + i) * geo.W) + ru.w0;
+          gemm_epilogue<BN, EPI>(g, lane_base + (uint32_t)(b * BN), m0 + quad * 32 + lane, 0, true);
+          zero_block(b);
+          mbar_arrive_plain(smem_addr(&acc_empty[b]));
+          continue;
+        }
+        if constexpr (BF) {
+        // drain and pack: pk[k] holds channels 2k, 2k+1 of this pixel
+        uint32_t pk[BN / 2];
+#pragma unroll
+        for (int c = 0; c < BN; c += 32) {
+          float v[32];
+          tmem_ld32(lane_base + (uint32_t)(b * BN + c), v);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            float lo = v[2 * q] + s_bias[c + 2 * q], hi = v[2 * q + 1] + s_bias[c + 2 * q + 1];
+            if (EPI == EPI_BIAS_RELU_BF16) {
+              lo = fmaxf(lo, 0.f);
+              hi = fmaxf(hi, 0.f);
+            }
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
+            pk[c / 2 + q] = *reinterpret_cast<const uint32_t *>(&h2);
+          }
+        }
         zero_block(b);
         mbar_arrive_plain(smem_addr(&acc_empty[b]));
+        // the staging tile is free once the group's previous store has read
+        // it (the leader waits for that and opens stg_free); bounded waits
+        const uint32_t k = nst++;
+        if (gtid == 0) {
+          asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          mbar_arrive_plain(smem_addr(&stg_free[grp]));
+        }
+        if (!mbar_wait(smem_addr(&stg_free[grp]), k & 1u)) {
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        const int p = quad * 32 + lane;  // pixel row of the tile
+#pragma unroll
+        for (int j = 0; j < ROWB / 16; ++j) {
+          const int sj = ROWB == 128 ? (j ^ (p & 7)) : (j ^ ((p >> 1) & 3));
+          const uint32_t dst = stg + (uint32_t)(p * ROWB + sj * 16);
+          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(pk[4 * j]), "r"(pk[4 * j + 1]),
+                       "r"(pk[4 * j + 2]), "r"(pk[4 * j + 3])
+                       : "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_plain(smem_addr(&stg_full[grp]));
+        if (gtid == 0) {
+          if (!mbar_wait(smem_addr(&stg_full[grp]), k & 1u)) {
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tma_store4d(&mapD, stg, 0, ru.w0, ru.h0 + i, ru.b);
+        }
+        }  // BF
       }
     }
+    if (tma_out && gtid == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   __syncthreads();
   if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
@@ -1043,12 +1131,12 @@ static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   return true;
 }
 
-template <int BN, int EPI, int SWA>
-static void launch_stack(const CUtensorMap &ma, const CUtensorMap &mb, const GemmArgs &g, const RowsGeo &geo,
-                         size_t smem, int ctas, cudaStream_t s) {
-  auto kern = k_conv_stack<BN, EPI, SWA>;
+template <int BN, int EPI, int SWA, bool ONE>
+static void launch_stack(const CUtensorMap &ma, const CUtensorMap &mb, const CUtensorMap &md, const GemmArgs &g,
+                         const RowsGeo &geo, size_t smem, int ctas, cudaStream_t s) {
+  auto kern = k_conv_stack<BN, EPI, SWA, ONE>;
   AIRT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ctas, StackRoles<BN>::THREADS, smem, s>>>(ma, mb, g, geo);
+  kern<<<ctas, StackRoles<BN>::THREADS, smem, s>>>(ma, mb, md, g, geo);
   AIRT_LAUNCH_CHECK();
 }
 
@@ -1066,16 +1154,27 @@ static bool conv3x3_stack(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const uint32_t strip = round1k((uint32_t)kStripRows * sw);
   geo.stage_bytes = (uint32_t)geo.cch * (sw == 128 ? 1u : 2u) * strip;
   geo.w_bytes = (uint32_t)(9 * geo.cch) * (uint32_t)bn * (uint32_t)sw;
+  // with 64-byte pixel rows the middle tap reads a second strip one pixel
+  // later; where four stages of two strips do not fit, one strip serves all
+  // three taps (shifted by 64 bytes)
+  bool one = false;
+  geo.tma_out = (epi == EPI_BIAS_RELU_BF16 || epi == EPI_BIAS_BF16) && g.ldd == g.N &&
+                ((uintptr_t)g.D & 15) == 0;
+  const uint32_t fixed = geo.w_bytes + (geo.tma_out ? 2u * 128u * (uint32_t)bn * 2u : 0u) + 1024u;
   const uint32_t half = 112640u, whole = 225280u;
+  if (sw == 64 && fixed + 4 * geo.stage_bytes > whole) {
+    one = true;
+    geo.stage_bytes /= 2;
+  }
   int per_sm = 2;
   uint32_t budget = half;
-  if (geo.w_bytes + 4 * geo.stage_bytes + 1024 > half) {
+  if (fixed + 4 * geo.stage_bytes > half) {
     per_sm = 1;
     budget = whole;
   }
-  if (geo.w_bytes + 4 * geo.stage_bytes + 1024 > budget) return false;
-  geo.S = std::min<int>(kRowsMaxStages, (int)((budget - 1024 - geo.w_bytes) / geo.stage_bytes));
-  const size_t smem = (size_t)geo.w_bytes + (size_t)geo.S * geo.stage_bytes + 1024;
+  if (fixed + 4 * geo.stage_bytes > budget) return false;
+  geo.S = std::min<int>(kRowsMaxStages, (int)((budget - fixed) / geo.stage_bytes));
+  const size_t smem = (size_t)fixed + (size_t)geo.S * geo.stage_bytes;
   geo.segs = W / 128;
   const int ctas = sm_count() * per_sm;
   long best = -1;
@@ -1096,19 +1195,30 @@ static bool conv3x3_stack(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const cuuint64_t dw[2] = {(cuuint64_t)9 * C, (cuuint64_t)g.N}, swt[1] = {(cuuint64_t)g.ldb * 2};
   const cuuint32_t bwt[2] = {(cuuint32_t)ks, (cuuint32_t)bn};
   const CUtensorMap mb = make_map(g.B, 2, dw, swt, bwt, sw);
+  CUtensorMap md = ma;  // unused without tma_out
+  if (geo.tma_out) {
+    const cuuint64_t dd[4] = {(cuuint64_t)g.N, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Bimg};
+    const cuuint64_t sd[3] = {(cuuint64_t)g.N * 2, (cuuint64_t)W * g.N * 2, (cuuint64_t)H * W * g.N * 2};
+    const cuuint32_t bd[4] = {(cuuint32_t)bn, 128, 1, 1};
+    md = make_map(g.D, 4, dd, sd, bd, bn * 2);
+  }
   const int grid = std::max(1, std::min(geo.nunits, ctas));
-#define AIRT_S(BNV, SWV)                                                                                  \
+#define AIRT_S(BNV, SWV, ONEV)                                                                            \
   switch (epi) {                                                                                          \
-    case EPI_STORE_F32: launch_stack<BNV, EPI_STORE_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;      \
-    case EPI_BIAS_RELU_BF16: launch_stack<BNV, EPI_BIAS_RELU_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break; \
-    case EPI_BIAS_BF16: launch_stack<BNV, EPI_BIAS_BF16, SWV>(ma, mb, g, geo, smem, grid, s); break;      \
-    case EPI_ADD_F32: launch_stack<BNV, EPI_ADD_F32, SWV>(ma, mb, g, geo, smem, grid, s); break;          \
+    case EPI_STORE_F32: launch_stack<BNV, EPI_STORE_F32, SWV, ONEV>(ma, mb, md, g, geo, smem, grid, s); break; \
+    case EPI_BIAS_RELU_BF16:                                                                              \
+      launch_stack<BNV, EPI_BIAS_RELU_BF16, SWV, ONEV>(ma, mb, md, g, geo, smem, grid, s);                \
+      break;                                                                                              \
+    case EPI_BIAS_BF16: launch_stack<BNV, EPI_BIAS_BF16, SWV, ONEV>(ma, mb, md, g, geo, smem, grid, s); break; \
+    case EPI_ADD_F32: launch_stack<BNV, EPI_ADD_F32, SWV, ONEV>(ma, mb, md, g, geo, smem, grid, s); break; \
     default: return false;                                                                                \
   }
   if (sw == 128) {
-    if (bn == 32) { AIRT_S(32, 128) } else { AIRT_S(64, 128) }
+    if (bn == 32) { AIRT_S(32, 128, false) } else { AIRT_S(64, 128, false) }
+  } else if (one) {
+    if (bn == 32) { AIRT_S(32, 64, true) } else { AIRT_S(64, 64, true) }
   } else {
-    if (bn == 32) { AIRT_S(32, 64) } else { AIRT_S(64, 64) }
+    if (bn == 32) { AIRT_S(32, 64, false) } else { AIRT_S(64, 64, false) }
   }
 #undef AIRT_S
   return true;
