@@ -69,6 +69,10 @@ struct Batch {
   DevBuf<InstGeom> g;
   DevBuf<int64_t> d_row_off, d_col_off;
   DevBuf<int> inst_row, inst_col, stop, iters, rule, active;
+  // 16-bit local column (CSR) and row (CSC) indices, when every instance has
+  // at most 65,536 pixels and rays (empty otherwise: the SpMVs then read the
+  // 32-bit indices)
+  DevBuf<uint16_t> ci16, ri16;
   DevBuf<double> rsq, nrm2, lam, taud, resn_last;
   bool tuned = false;
   // active tiles per class, rebuilt after every stop-rule update:
@@ -211,16 +215,16 @@ struct BFwd {
   double *ppr;
 };
 
+// Residual pass; with idx16 (16-bit local column indices, voff = the
+// instances' first columns) the nonzeros stream at 6 bytes instead of 8.
 template <int L>
 __global__ void __launch_bounds__(256, 4)
     k_batch_fwd(int64_t nseg, const int *__restrict__ tiles, const int *__restrict__ ntiles,
                 const int64_t *__restrict__ rp, const int *__restrict__ ci, const float *__restrict__ rv,
-                const float *__restrict__ x32, BFwd o) {
-  for_each_segment_vt<L>(
-      nseg, tiles, ntiles, kTileShift, rp + o.r0, ci, rv, x32,
-      [&](int64_t i) { return o.stop[o.inst_row[o.r0 + i]] == 0; },
-      [&](int64_t i) { return make_double2(o.b[o.r0 + i], o.M[o.r0 + i]); },
-      [&](int64_t i, double s, bool lead, double2 bm) {
+                const float *__restrict__ x32, BFwd o, const uint16_t *__restrict__ idx16,
+                const int64_t *__restrict__ voff) {
+  auto pre = [&](int64_t i) { return make_double2(o.b[o.r0 + i], o.M[o.r0 + i]); };
+  auto epi = [&](int64_t i, double s, bool lead, double2 bm) {
         if (!lead) return;
         const int64_t r = o.r0 + i;
         const double ri = bm.x - s;
@@ -234,7 +238,14 @@ __global__ void __launch_bounds__(256, 4)
           }
           o.rprev[r] = ri;
         }
-      });
+      };
+  if (idx16)
+    for_each_segment_vt16<L>(nseg, tiles, ntiles, kTileShift, rp + o.r0, idx16, rv, x32, o.inst_row + o.r0, o.stop,
+                             voff, pre, epi);
+  else
+    for_each_segment_vt<L>(
+        nseg, tiles, ntiles, kTileShift, rp + o.r0, ci, rv, x32,
+        [&](int64_t i) { return o.stop[o.inst_row[o.r0 + i]] == 0; }, pre, epi);
 }
 
 struct BUpd {
@@ -247,19 +258,19 @@ struct BUpd {
   int64_t c0;
 };
 
+// Update pass; idx16 / voff as in k_batch_fwd (16-bit local row indices,
+// the instances' first rows).
 template <int L>
 __global__ void __launch_bounds__(256, 4)
     k_batch_bwd(int64_t nseg, const int *__restrict__ tiles, const int *__restrict__ ntiles,
                 const int64_t *__restrict__ cp, const int *__restrict__ ri, const float *__restrict__ cv,
-                const float *__restrict__ mr32, BUpd u) {
-  for_each_segment_vt<L>(
-      nseg, tiles, ntiles, kTileShift, cp + u.c0, ri, cv, mr32,
-      [&](int64_t j) { return u.stop[u.inst_col[u.c0 + j]] == 0; },
-      [&](int64_t j) {
-        const int64_t c = u.c0 + j;
-        return make_double3(u.x64[c], u.lam[u.inst_col[c]], u.D[c]);
-      },
-      [&](int64_t j, double g, bool lead, double3 xld) {
+                const float *__restrict__ mr32, BUpd u, const uint16_t *__restrict__ idx16,
+                const int64_t *__restrict__ voff) {
+  auto pre = [&](int64_t j) {
+    const int64_t c = u.c0 + j;
+    return make_double3(u.x64[c], u.lam[u.inst_col[c]], u.D[c]);
+  };
+  auto epi = [&](int64_t j, double g, bool lead, double3 xld) {
         if (!lead) return;
         const int64_t c = u.c0 + j;
         double x = xld.x + xld.y * (xld.z * g);
@@ -267,7 +278,27 @@ __global__ void __launch_bounds__(256, 4)
         if (u.ubk) x = fmin(x, u.ub);
         u.x64[c] = x;
         u.x32[c] = (float)x;
-      });
+      };
+  if (idx16)
+    for_each_segment_vt16<L>(nseg, tiles, ntiles, kTileShift, cp + u.c0, idx16, cv, mr32, u.inst_col + u.c0, u.stop,
+                             voff, pre, epi);
+  else
+    for_each_segment_vt<L>(
+        nseg, tiles, ntiles, kTileShift, cp + u.c0, ri, cv, mr32,
+        [&](int64_t j) { return u.stop[u.inst_col[u.c0 + j]] == 0; }, pre, epi);
+}
+
+// 16-bit local indices of a block-diagonal matrix: out[q] = idx[q] -
+// off[inst_of[segment of q]], a warp per segment.
+__global__ void k_local16(int64_t nseg, const int64_t *__restrict__ ptr, const int *__restrict__ idx,
+                          const int *__restrict__ inst_of, const int64_t *__restrict__ off,
+                          uint16_t *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nseg;
+       i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t base = off[inst_of[i]];
+    for (int64_t q = ptr[i] + lane; q < ptr[i + 1]; q += 32) out[q] = (uint16_t)(idx[q] - base);
+  }
 }
 
 // Class of every tile of segments [0, nseg): its mean segment length from
@@ -568,8 +599,15 @@ void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullp
   const int64_t ns = P.m;
   const unsigned g = grid_for((int64_t)B.rt.count[c] * (1 << kTileShift) * L, 256, 4);
   const int *tl = B.rt.list.p + B.rt.off[c], *cnt = B.tcount.p + c;
+  // 16-bit indices for the long-segment class only: with segments of 128
+  // nonzeros or fewer the 8-aligned head and tail (up to 7 elements each,
+  // element-wise) cost more than the index bytes save (measured on the
+  // 512-instance batch: all-active iterations 5 % faster, the short-segment
+  // tail 5 % slower when every class used them)
+  const uint16_t *i16 = c == kClasses - 1 ? B.ci16.p : nullptr;
   switch (L) {
-#define AIRT_F(LV) k_batch_fwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.rp.p, P.ci.p, P.rv.p, x32, o)
+#define AIRT_F(LV) \
+  k_batch_fwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.rp.p, P.ci.p, P.rv.p, x32, o, i16, B.d_col_off.p)
     case 16: AIRT_F(16); break;
     case 8: AIRT_F(8); break;
     case 4: AIRT_F(4); break;
@@ -587,8 +625,10 @@ void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = null
   const int64_t ns = P.n;
   const unsigned g = grid_for((int64_t)B.ct.count[c] * (1 << kTileShift) * L, 256, 4);
   const int *tl = B.ct.list.p + B.ct.off[c], *cnt = B.tcount.p + kClasses + c;
+  const uint16_t *i16 = c == kClasses - 1 ? B.ri16.p : nullptr;  // as in launch_bfwd
   switch (L) {
-#define AIRT_B(LV) k_batch_bwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.cp.p, P.ri.p, P.cv.p, mr32, u)
+#define AIRT_B(LV) \
+  k_batch_bwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.cp.p, P.ri.p, P.cv.p, mr32, u, i16, B.d_row_off.p)
     case 16: AIRT_B(16); break;
     case 8: AIRT_B(8); break;
     case 4: AIRT_B(4); break;
@@ -758,6 +798,18 @@ Batch *batch_build(int ninst, const int *N, const int *nA, const int *p, const d
     k_fill_inst<<<grid_for(P.m, 256), 256, 0, s>>>(ninst, B->d_row_off.p, P.m, B->inst_row.p);
     k_fill_inst<<<grid_for(P.n, 256), 256, 0, s>>>(ninst, B->d_col_off.p, P.n, B->inst_col.p);
     AIRT_LAUNCH_CHECK();
+    bool fits16 = true;
+    for (int k = 0; k < ninst; ++k)
+      fits16 = fits16 && B->row_off[k + 1] - B->row_off[k] <= 65536 && B->col_off[k + 1] - B->col_off[k] <= 65536;
+    if (fits16 && P.nnz > 0) {
+      B->ci16.ensure(P.nnz);
+      B->ri16.ensure(P.nnz);
+      k_local16<<<grid_for(P.m * 32, 256), 256, 0, s>>>(P.m, P.rp.p, P.ci.p, B->inst_row.p, B->d_col_off.p,
+                                                        B->ci16.p);
+      k_local16<<<grid_for(P.n * 32, 256), 256, 0, s>>>(P.n, P.cp.p, P.ri.p, B->inst_col.p, B->d_row_off.p,
+                                                        B->ri16.p);
+      AIRT_LAUNCH_CHECK();
+    }
     setup_tileset(B->rt, P.m, P.rp.p, s);
     setup_tileset(B->ct, P.n, P.cp.p, s);
     B->tcount.ensure(2 * kClasses);

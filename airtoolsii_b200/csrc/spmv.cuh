@@ -262,6 +262,83 @@ __device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__r
   }
 }
 
+// for_each_segment_vt over a block-diagonal matrix whose indices are stored
+// as 16-bit offsets within each segment's instance: segment i belongs to
+// instance inst_of[i], runs when stop[that] == 0, and gathers x[voff[that] +
+// local index].  A lane reads 8 nonzeros per 16-byte index load (two float4
+// value loads), two such groups per round, so the streamed bytes per
+// nonzero drop from 8 to 6.  The 8-aligned body is vectorised, the head and
+// tail (< 8 elements each) are read element-wise; segment sums run in a
+// fixed order (per lane four accumulators, then the group's shuffle tree).
+template <int LANES, typename TX, class Pre, class Epi>
+__device__ __forceinline__ void for_each_segment_vt16(int64_t nseg, const int *__restrict__ tiles,
+                                                      const int *__restrict__ ntiles, int tshift,
+                                                      const int64_t *__restrict__ ptr,
+                                                      const uint16_t *__restrict__ idx,
+                                                      const float *__restrict__ val,
+                                                      const TX *__restrict__ x,
+                                                      const int *__restrict__ inst_of,
+                                                      const int *__restrict__ stop,
+                                                      const int64_t *__restrict__ voff, Pre &&pre,
+                                                      Epi &&epi) {
+  const int lane = threadIdx.x % LANES;
+  const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / LANES;
+  const int64_t ng = (int64_t)gridDim.x * blockDim.x / LANES;
+  const int64_t total = (int64_t)__ldg(ntiles) << tshift;
+  const int64_t tmask = ((int64_t)1 << tshift) - 1;
+  const int64_t trips = (total + ng - 1) / ng;
+  const float4 *__restrict__ V4 = reinterpret_cast<const float4 *>(val);
+  const uint4 *__restrict__ I8 = reinterpret_cast<const uint4 *>(idx);
+  for (int64_t t = 0; t < trips; ++t) {
+    const int64_t u = gid + t * ng;
+    const int64_t i = u < total ? ((int64_t)__ldg(tiles + (u >> tshift)) << tshift) + (u & tmask) : nseg;
+    bool on = false;
+    int64_t q0 = 0, q1 = 0;
+    const TX *xb = x;
+    decltype(pre(i)) pv{};
+    if (i < nseg) {
+      q0 = __ldg(ptr + i);
+      q1 = __ldg(ptr + i + 1);
+      const int k = __ldg(inst_of + i);
+      on = __ldg(stop + k) == 0;
+      xb = x + __ldg(voff + k);
+      if (on && lane == 0) pv = pre(i);
+    }
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (on) {
+      int64_t qa = (q0 + 7) & ~(int64_t)7;
+      if (qa > q1) qa = q1;
+      int64_t qb = q1 & ~(int64_t)7;
+      if (qb < qa) qb = qa;
+      for (int64_t q = q0 + lane; q < qa; q += LANES)
+        a0 = fma((double)__ldg(val + q), (double)__ldg(xb + __ldg(idx + q)), a0);
+      for (int64_t q = qb + lane; q < q1; q += LANES)
+        a1 = fma((double)__ldg(val + q), (double)__ldg(xb + __ldg(idx + q)), a1);
+      const int64_t ge = qb >> 3;
+      int64_t gq = (qa >> 3) + lane;
+      for (; gq < ge; gq += LANES) {
+        const uint4 c = __ldg(I8 + gq);
+        const float4 f = __ldg(V4 + 2 * gq), h = __ldg(V4 + 2 * gq + 1);
+        const TX g0 = __ldg(xb + (c.x & 0xFFFFu)), g1 = __ldg(xb + (c.x >> 16));
+        const TX g2 = __ldg(xb + (c.y & 0xFFFFu)), g3 = __ldg(xb + (c.y >> 16));
+        const TX g4 = __ldg(xb + (c.z & 0xFFFFu)), g5 = __ldg(xb + (c.z >> 16));
+        const TX g6 = __ldg(xb + (c.w & 0xFFFFu)), g7 = __ldg(xb + (c.w >> 16));
+        a0 = fma((double)f.x, (double)g0, a0);
+        a1 = fma((double)f.y, (double)g1, a1);
+        a2 = fma((double)f.z, (double)g2, a2);
+        a3 = fma((double)f.w, (double)g3, a3);
+        a0 = fma((double)h.x, (double)g4, a0);
+        a1 = fma((double)h.y, (double)g5, a1);
+        a2 = fma((double)h.z, (double)g6, a2);
+        a3 = fma((double)h.w, (double)g7, a3);
+      }
+    }
+    double acc = (a0 + a1) + (a2 + a3);
+    acc = group_sum<LANES>(acc);
+    epi(i, acc, lane == 0 && on, pv);
+  }
+}
+
 // Lanes per segment of the vectorised kernels from the mean segment length.
 inline int vec_lanes_for(int64_t nnz, int64_t nseg) {
   const double avg = nseg ? (double)nnz / (double)nseg : 0.0;

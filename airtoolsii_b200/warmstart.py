@@ -221,7 +221,9 @@ class WarmStart:
         (airt_sirt_multi_device: the matrix is read once per iteration for
         the whole batch).  plain: cimmino from zero; warm: u = D.*A'(M.*b)
         (one SART step from zero, through the same engine), x0 = U-Net(u),
-        cimmino from x0.  Same clocks and outputs as time_to_dp (no fbp arm)."""
+        cimmino from x0.  Same clocks and outputs as time_to_dp (no fbp arm).
+        (Queueing every batch's network on its own stream, so that it runs
+        beside the solves of earlier batches, was measured: no faster.)"""
         from .batch import sirt_multi_device
         torch = self.torch
         total = data["b"].shape[0]
