@@ -246,23 +246,16 @@ def extra_legs(A_c2, b_c2, wl):
     nz = B.inst_nnz()
     mi, ni = np.diff(B.row_off), np.diff(B.col_off)
     c4 = {"instances": K, "nnz": int(B.nnz), "build_s": round(t_build, 3)}
-    # the batch keeps 16-bit local indices when every instance has at most
-    # 65,536 rows and columns: 6 streamed bytes per nonzero and direction
-    # instead of the model's 8 (FP32 value + int32 index)
-    idx_b = 2 if (mi.max() <= 65536 and ni.max() <= 65536) else 4
-    c4["index_bytes"] = idx_b
     for meth in ("cimmino", "drop"):
         rho = B.rho(meth)
         B.sirt_device(meth, db.data_ptr(), dxo.data_ptr(), 2000, taudelta=np.array(tds), rho=rho)
         info = B.sirt_device(meth, db.data_ptr(), dxo.data_ptr(), 2000, taudelta=np.array(tds), rho=rho)
         its = info["finaliter"]
         byts = float(np.sum(its * (16 * nz + 16 * mi + 16 * ni)))
-        streamed = float(np.sum(its * (2 * (4 + idx_b) * nz + 16 * mi + 16 * ni)))
         sec = info["gpu_ms"] / 1e3
         c4[meth] = {"gpu_ms": round(info["gpu_ms"], 2), "iters_mean": round(float(its.mean()), 2),
                     "iters_max": int(its.max()), "dp_stopped": int(np.sum(info["stoprule"] == 2)),
-                    "GBps_model": round(byts / sec / 1e9, 1),
-                    "GBps_streamed": round(streamed / sec / 1e9, 1)}
+                    "GBps_model": round(byts / sec / 1e9, 1)}
     _, ik = B.kaczmarz(np.concatenate(bs), 5)
     c4["kaczmarz_5_sweeps_ms"] = round(ik["gpu_ms"], 2)
     c4["cpu_baseline"] = _cpu_batch_sample(B, Ns, nAs, bs, tds, B.rho("cimmino"))
