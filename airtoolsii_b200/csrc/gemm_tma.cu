@@ -1078,9 +1078,10 @@ static bool conv3x3_rows(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   const size_t smem = (size_t)geo.w_bytes + (size_t)geo.S * geo.stage_bytes + 1024;
   geo.segs = W / 128;
   const int ctas = sm_count() * per_sm;
-  // rows per run: the fewest input rows on the busiest CTA, ceil(units/ctas) * (R + 2)
+  // rows per run (any R up to H; the last run of a column may be shorter):
+  // the fewest input rows on the busiest CTA, ceil(units/ctas) * (R + 2)
   long best = -1;
-  for (int R = 1; R <= H; R *= 2) {
+  for (int R = 1; R <= H; ++R) {
     const long units = (long)Bimg * geo.segs * ((H + R - 1) / R);
     const long cost = ((units + ctas - 1) / ctas) * (R + 2);
     if (best < 0 || cost < best) {
@@ -1178,7 +1179,7 @@ static bool conv3x3_stack(const GemmArgs &g, int bn, int epi, cudaStream_t s) {
   geo.segs = W / 128;
   const int ctas = sm_count() * per_sm;
   long best = -1;
-  for (int R = 1; R <= H; R *= 2) {
+  for (int R = 1; R <= H; ++R) {
     const long units = (long)Bimg * geo.segs * ((H + R - 1) / R);
     const long cost = ((units + ctas - 1) / ctas) * (R + 2);
     if (best < 0 || cost < best) {

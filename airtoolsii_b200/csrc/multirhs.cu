@@ -411,10 +411,13 @@ void multi_pass(Problem &P, const airt_sirt_opts &o, int K0, const double *d_B, 
   ctrl(1);
   AIRT_LAUNCH_CHECK();
   // Chunks of iterations captured once as a CUDA graph (again after each
-  // compaction); the host reads the active count of chunk c once chunk c+2
-  // is queued (lagged poll).
-  const int64_t chunk = 8;
-  const int lag = 2;
+  // compaction).  With the DP rule the host reads the active count after
+  // every chunk of 4 (no lag): a drained stream costs tens of microseconds
+  // against a chunk of several milliseconds, and an exact, current count
+  // lets the layout compact in time for warm-started solves of 10-20
+  // iterations, which a count two chunks late would miss.
+  const int64_t chunk = taud_host ? 4 : 8;
+  const int lag = 0;
   cudaGraphExec_t gexec = nullptr;
   auto capture = [&]() {
     if (gexec) cudaGraphExecDestroy(gexec);
