@@ -220,40 +220,37 @@ __device__ __forceinline__ void for_each_segment_vt(int64_t nseg, const int *__r
     }
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (on) {
-      int64_t qa = (q0 + 3) & ~(int64_t)3;
-      if (qa > q1) qa = q1;
-      int64_t qb = q1 & ~(int64_t)3;
-      if (qb < qa) qb = qa;
-      for (int64_t q = q0 + lane; q < qa; q += LANES)
-        a0 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a0);
-      for (int64_t q = qb + lane; q < q1; q += LANES)
-        a1 = fma((double)__ldg(val + q), (double)__ldg(x + __ldg(idx + q)), a1);
-      const int64_t ve = qb >> 2;
-      int64_t v = (qa >> 2) + lane;
-      // two vectors per lane per round (both loads issued before the
-      // gathers), accumulated in the order of the one-vector loop
+      // every aligned 16-byte group that overlaps [q0, q1), its elements
+      // outside the segment masked out (they belong to the neighbouring
+      // segments or the zero padding, so the loads stay inside the arrays):
+      // no element-wise head or tail loop, which on short segments (tens of
+      // nonzeros) would hold a large share of the loads in serial chains
+      const int64_t ve = (q1 + 3) >> 2;
+      int64_t v = (q0 >> 2) + lane;
       for (; v + LANES < ve; v += 2 * LANES) {
         const float4 f = __ldg(V4 + v), h = __ldg(V4 + v + LANES);
         const int4 c = __ldg(I4 + v), d = __ldg(I4 + v + LANES);
         const TX g0 = __ldg(x + c.x), g1 = __ldg(x + c.y), g2 = __ldg(x + c.z), g3 = __ldg(x + c.w);
         const TX k0 = __ldg(x + d.x), k1 = __ldg(x + d.y), k2 = __ldg(x + d.z), k3 = __ldg(x + d.w);
-        a0 = fma((double)f.x, (double)g0, a0);
-        a1 = fma((double)f.y, (double)g1, a1);
-        a2 = fma((double)f.z, (double)g2, a2);
-        a3 = fma((double)f.w, (double)g3, a3);
-        a0 = fma((double)h.x, (double)k0, a0);
-        a1 = fma((double)h.y, (double)k1, a1);
-        a2 = fma((double)h.z, (double)k2, a2);
-        a3 = fma((double)h.w, (double)k3, a3);
+        const int64_t e = v << 2, e2 = (v + LANES) << 2;
+        if (e >= q0 && e < q1) a0 = fma((double)f.x, (double)g0, a0);
+        if (e + 1 >= q0 && e + 1 < q1) a1 = fma((double)f.y, (double)g1, a1);
+        if (e + 2 >= q0 && e + 2 < q1) a2 = fma((double)f.z, (double)g2, a2);
+        if (e + 3 >= q0 && e + 3 < q1) a3 = fma((double)f.w, (double)g3, a3);
+        if (e2 < q1) a0 = fma((double)h.x, (double)k0, a0);
+        if (e2 + 1 < q1) a1 = fma((double)h.y, (double)k1, a1);
+        if (e2 + 2 < q1) a2 = fma((double)h.z, (double)k2, a2);
+        if (e2 + 3 < q1) a3 = fma((double)h.w, (double)k3, a3);
       }
       if (v < ve) {
         const float4 f = __ldg(V4 + v);
         const int4 c = __ldg(I4 + v);
         const TX g0 = __ldg(x + c.x), g1 = __ldg(x + c.y), g2 = __ldg(x + c.z), g3 = __ldg(x + c.w);
-        a0 = fma((double)f.x, (double)g0, a0);
-        a1 = fma((double)f.y, (double)g1, a1);
-        a2 = fma((double)f.z, (double)g2, a2);
-        a3 = fma((double)f.w, (double)g3, a3);
+        const int64_t e = v << 2;
+        if (e >= q0 && e < q1) a0 = fma((double)f.x, (double)g0, a0);
+        if (e + 1 >= q0 && e + 1 < q1) a1 = fma((double)f.y, (double)g1, a1);
+        if (e + 2 >= q0 && e + 2 < q1) a2 = fma((double)f.z, (double)g2, a2);
+        if (e + 3 >= q0 && e + 3 < q1) a3 = fma((double)f.w, (double)g3, a3);
       }
     }
     double acc = (a0 + a1) + (a2 + a3);
