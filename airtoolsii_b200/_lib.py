@@ -93,6 +93,7 @@ SIGNATURES = {
     "airt_test_set_wait_budget": (C.c_int, [C.c_longlong]),
     "airt_test_inject_stall": (C.c_int, [C.c_int]),
     "airt_test_fail_alloc": (C.c_int, [C.c_int]),
+    "airt_test_split_trace": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "airt_rho_custom": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, C.c_int, C.c_double, C.c_int,
                                   _dp]),
     "airt_sirt": (C.c_int, [C.c_void_p, C.POINTER(SirtOpts), _dp, _dp, _i64p, C.c_int64, _dp,

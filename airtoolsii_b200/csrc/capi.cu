@@ -707,6 +707,14 @@ int airt_profile_read(airt_problem *h, int which, int64_t *launches, double *tot
 
 }  // extern "C"
 
+extern "C" int airt_test_split_trace(airt_problem *h, int64_t *mismatched, int64_t *split) {
+  AIRT_API_BEGIN
+  AIRT_REQUIRE(h && mismatched, "null pointer argument");
+  Problem *P = reinterpret_cast<Problem *>(h);
+  *mismatched = test_split_trace(*P, split);
+  AIRT_API_END
+}
+
 extern "C" int airt_test_fail_alloc(int after) {
   airt::g_alloc_fail_countdown = after < 0 ? -1 : after;
   return AIRT_OK;

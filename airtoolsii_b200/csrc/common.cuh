@@ -302,6 +302,8 @@ void generate_matrix(Problem &P);
 // Bounds of the fixed-point back projection of a matrix-free problem (one
 // pass over the rays at creation; trace.cu).
 void mf_prepare(Problem &P);
+// Rays whose two-part trace differs from the whole trace (test hook); *nsplit: rays split.
+int64_t test_split_trace(Problem &P, int64_t *nsplit);
 void apply_operator(Problem &P, const double *d_in, double *d_out, int transp);
 void compute_weights(Problem &P, int method, double *dM, double *dD);
 void run_sirt_multi(Problem &P, const airt_sirt_opts &o, int K, const double *d_B,

@@ -135,13 +135,19 @@ __global__ void __launch_bounds__(64)
   if (stopped(o.st)) return;
   Acc4 a;
   const int64_t nn = (int64_t)g.N * g.N;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
-       r += (int64_t)gridDim.x * blockDim.x) {
+  // two adjacent threads per ray, each tracing one half (row_entries_part);
+  // the pair adds its halves by a shuffle, every lane runs every trip
+  const int part = threadIdx.x & 1;
+  const int64_t np = ((int64_t)gridDim.x * blockDim.x) >> 1;
+  const int64_t trips = (nrays + np - 1) / np;
+  for (int64_t t = 0, r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 1; t < trips; ++t, r += np) {
     double acc = 0.0;
-    row_entries(g, r, excl, [&](int col, double v) {
-      if (col >= 0 && col < nn) acc = fma((double)(float)v, (double)x32[col], acc);
-    });
-    resid_row<ME>(r, acc, o, a);
+    if (r < nrays)
+      row_entries_part(g, r, excl, part, [&](int col, double v) {
+        if (col >= 0 && col < nn) acc = fma((double)(float)v, (double)x32[col], acc);
+      });
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    if (r < nrays && part == 0) resid_row<ME>(r, acc, o, a);
   }
   // warp sums (no block barrier: a warp whose rays are short leaves at once)
   double r2 = warp_sum(a.r2), rmr = warp_sum(a.rmr), p2 = 0, pr = 0;
@@ -489,7 +495,7 @@ void launch_fwd_t(Problem &P, const FwdOut &o) {
     return;
   }
   if (P.matrix_free) {
-    k_sirt_fwd_mf<ME><<<grid_for(P.m, 64, 32), 64, 0, s>>>(P.geom(), P.m,
+    k_sirt_fwd_mf<ME><<<grid_for(2 * P.m, 64, 32), 64, 0, s>>>(P.geom(), P.m,
                                                               P.geo_kind == GEO_PARALLEL,
                                                               P.x32.p, o);
     return;

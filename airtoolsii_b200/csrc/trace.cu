@@ -113,11 +113,15 @@ __global__ void k_mf_adjoint_fx(RayGeom g, int64_t nrays, bool excl, const TU *_
   if (e == INT_MIN || e == INT_MAX) return;  // u == 0 (result 0) or not finite (NaN)
   const double sc = ldexp(1.0, 62 - e);
   const int64_t nn = (int64_t)g.N * g.N;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
-       r += (int64_t)gridDim.x * blockDim.x) {
+  // two adjacent threads per ray, each scattering one half of its entries
+  // (row_entries_part): the entries are the same, and integer sums do not
+  // depend on their order
+  const int part = threadIdx.x & 1;
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 1; r < nrays;
+       r += ((int64_t)gridDim.x * blockDim.x) >> 1) {
     const double ur = (double)u[r];
     if (ur == 0.0) continue;
-    row_entries(g, r, excl, [&](int col, double v) {
+    row_entries_part(g, r, excl, part, [&](int col, double v) {
       if (col >= 0 && col < nn) {
         const long long t = __double2ll_rn(__dmul_rn((double)(float)v, ur) * sc);
         atomicAdd(reinterpret_cast<unsigned long long *>(acc + col), (unsigned long long)t);
@@ -273,7 +277,7 @@ void apply_matrix_free(Problem &P, const double *d_in, double *d_out, int transp
     AIRT_CHECK_CUDA(cudaMemsetAsync(d_out, 0, P.n * sizeof(double), s));
     AIRT_CHECK_CUDA(cudaMemsetAsync(P.mf_umax.p, 0, sizeof(unsigned long long), s));
     k_absmax<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, d_in, nullptr, P.mf_umax.p, nullptr);
-    k_mf_adjoint_fx<double><<<grid, 128, 0, s>>>(g, P.m, excl_of(P), d_in,
+    k_mf_adjoint_fx<double><<<grid_for(2 * P.m, 128, 16), 128, 0, s>>>(g, P.m, excl_of(P), d_in,
                                                  reinterpret_cast<long long *>(d_out),
                                                  P.mf_kbound, P.mf_umax.p, nullptr);
     k_fx_to_f64<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, d_out, P.mf_kbound, P.mf_umax.p, nullptr);
@@ -297,13 +301,58 @@ void row_col_stats_mf(Problem &P, double *s2, double *s1, double *colcnt, double
   AIRT_LAUNCH_CHECK();
 }
 
+// ---- check of the split trace: per ray, the entries of trace_entries and
+// the union of trace_entries_part(0) and (1) compared by count and an
+// order-independent hash of (pixel, FP64 value bits).
+namespace {
+__device__ __forceinline__ unsigned long long entry_hash(int col, double v) {
+  unsigned long long z = (unsigned long long)__double_as_longlong(v) ^ ((unsigned long long)(unsigned)col << 1);
+  z ^= z >> 33;
+  z *= 0xff51afd7ed558ccdull;
+  z ^= z >> 33;
+  z *= 0xc4ceb9fe1a85ec53ull;
+  z ^= z >> 33;
+  return z;
+}
+
+__global__ void k_test_split(RayGeom g, int64_t nrays, bool excl, unsigned long long *__restrict__ bad,
+                             unsigned long long *__restrict__ nsplit) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrays;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const Ray q = ray_of(g, r);
+    unsigned long long h0 = 0, h1 = 0;
+    long long c0 = 0, c1 = 0, c2 = 0;
+    trace_entries(g.N, q, excl, [&](int col, double v) { h0 += entry_hash(col, v); ++c0; });
+    trace_entries_part(g.N, q, excl, 0, [&](int col, double v) { h1 += entry_hash(col, v); ++c1; });
+    trace_entries_part(g.N, q, excl, 1, [&](int col, double v) { h1 += entry_hash(col, v); ++c2; });
+    if (h0 != h1 || c0 != c1 + c2) atomicAdd(bad, 1ull);
+    if (c2 > 0) atomicAdd(nsplit, 1ull);
+  }
+}
+}  // namespace
+
+int64_t test_split_trace(Problem &P, int64_t *nsplit) {
+  AIRT_REQUIRE(P.geo_kind != GEO_NONE && P.geo_kind != GEO_SPHERE, "the problem has no straight-ray geometry");
+  cudaStream_t s = P.stream;
+  DevBuf<unsigned long long> c;
+  c.ensure(2);
+  AIRT_CHECK_CUDA(cudaMemsetAsync(c.p, 0, 2 * sizeof(unsigned long long), s));
+  k_test_split<<<grid_for(P.m, 128, 16), 128, 0, s>>>(P.geom(), P.m, excl_of(P), c.p, c.p + 1);
+  AIRT_LAUNCH_CHECK();
+  unsigned long long hc[2] = {0, 0};
+  AIRT_CHECK_CUDA(cudaMemcpyAsync(hc, c.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+  AIRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (nsplit) *nsplit = (int64_t)hc[1];
+  return (int64_t)hc[0];
+}
+
 // Matrix-free pieces of the SIRT iteration (used by sirt.cu).
 void mf_backproject_f32(Problem &P, const float *u, double *g64, const int *stop_flag) {
   cudaStream_t s = P.stream;
   AIRT_CHECK_CUDA(cudaMemsetAsync(g64, 0, P.n * sizeof(double), s));
   AIRT_CHECK_CUDA(cudaMemsetAsync(P.mf_umax.p, 0, sizeof(unsigned long long), s));
   k_absmax<<<grid_for(P.m, 256), 256, 0, s>>>(P.m, nullptr, u, P.mf_umax.p, stop_flag);
-  k_mf_adjoint_fx<float><<<grid_for(P.m, 64, 32), 64, 0, s>>>(
+  k_mf_adjoint_fx<float><<<grid_for(2 * P.m, 64, 32), 64, 0, s>>>(
       P.geom(), P.m, excl_of(P), u, reinterpret_cast<long long *>(g64), P.mf_kbound, P.mf_umax.p,
       stop_flag);
   k_fx_to_f64<<<grid_for(P.n, 256), 256, 0, s>>>(P.n, g64, P.mf_kbound, P.mf_umax.p, stop_flag);

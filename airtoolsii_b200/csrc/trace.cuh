@@ -185,13 +185,13 @@ __device__ __forceinline__ void trace_segments(int N, const Ray &q, bool exclude
 // appearance, with the FP64 sum.
 constexpr int kMergeWindow = 4;
 
-template <class Emit>
-__device__ __forceinline__ void trace_entries(int N, const Ray &q, bool exclude_top_right,
-                                              Emit &&emit) {
+// The window of the last kMergeWindow distinct pixels (oldest at index 0).
+struct MergeWindow {
   int wc[kMergeWindow];
   double wv[kMergeWindow];
-  int cnt = 0;  // entries held in the window (oldest at index 0)
-  trace_segments(N, q, exclude_top_right, [&](int col, double len) {
+  int cnt = 0;
+  template <class Emit>
+  __device__ __forceinline__ void add(int col, double len, Emit &&emit) {
 #pragma unroll
     for (int k = 0; k < kMergeWindow; ++k)
       if (k < cnt && wc[k] == col) {
@@ -214,10 +214,206 @@ __device__ __forceinline__ void trace_entries(int N, const Ray &q, bool exclude_
         wv[k] = len;
       }
     ++cnt;
-  });
+  }
+  template <class Emit>
+  __device__ __forceinline__ void flush(Emit &&emit) {
 #pragma unroll
-  for (int k = 0; k < kMergeWindow; ++k)
-    if (k < cnt) emit(wc[k], wv[k]);
+    for (int k = 0; k < kMergeWindow; ++k)
+      if (k < cnt) emit(wc[k], wv[k]);
+  }
+};
+
+template <class Emit>
+__device__ __forceinline__ void trace_entries(int N, const Ray &q, bool exclude_top_right,
+                                              Emit &&emit) {
+  MergeWindow w;
+  trace_segments(N, q, exclude_top_right, [&](int col, double len) { w.add(col, len, emit); });
+  w.flush(emit);
+}
+
+// ---- one ray traced by two threads
+// trace_segments_part(part = 0 or 1) emits the first or the second half of
+// the segments trace_segments emits, so that two threads can share a long
+// ray.  The split is at the middle crossing S of the family with more
+// crossings (the primary family), provided S is clean: no crossing of the
+// other family lies within kSplitGap of it in t.  Then S is a kept point
+// (its successor is not within 1e-10), the segment ending at S is emitted by
+// part 0 as its last one and the segment starting at S by part 1 as its
+// first, every other point has the same neighbours as in the whole trace,
+// and the two halves lie on either side of one grid line, so no pixel
+// appears in both (the duplicate merge of trace_entries stays within a
+// half).  Part 0 runs the merge from the ray's start and stops after S; part
+// 1 starts from S as the pending point with the other family's position
+// found from t(S) (an estimate, then exact comparisons of crossing
+// parameters).  Rays too short to be worth splitting, or without a clean
+// crossing near the middle, go to part 0 whole (part 1 emits nothing).
+constexpr int kSplitMin = 48;        // crossings (both families) of a ray worth splitting
+constexpr double kSplitGap = 1e-7;   // minimum |t| distance of S to the other family
+
+__device__ __forceinline__ double cross_t(int i, double h, double o, double d) {
+  return __ddiv_rn(__dsub_rn((double)i - h, o), d);
+}
+
+template <class Seg>
+__device__ __forceinline__ void trace_segments_part(int N, const Ray &q, bool exclude_top_right, int part,
+                                                    Seg &&seg) {
+  const double h = 0.5 * (double)N;
+  if (exclude_top_right && ((q.b == 0.0 && fabs(__dsub_rn(q.y0t, h)) < 1e-15) ||
+                            (q.a == 0.0 && fabs(__dsub_rn(q.x0t, h)) < 1e-15)))
+    return;
+  int nx = 0, ix0 = 0, sx = 1;
+  if (q.a != 0.0) {
+    int lo, hi;
+    crossing_range(N, h, q.x0t, q.y0t, q.a, q.b, lo, hi);
+    nx = hi >= lo ? hi - lo + 1 : 0;
+    if (q.a > 0.0) { ix0 = lo; sx = 1; }
+    else { ix0 = hi; sx = -1; }
+  }
+  int ny = 0, iy0 = 0, sy = 1;
+  if (q.b != 0.0) {
+    int lo, hi;
+    crossing_range(N, h, q.y0t, q.x0t, q.b, q.a, lo, hi);
+    ny = hi >= lo ? hi - lo + 1 : 0;
+    if (q.b > 0.0) { iy0 = lo; sy = 1; }
+    else { iy0 = hi; sy = -1; }
+  }
+  // ---- the split: primary family P (more crossings), position mP of S,
+  // position pQ of the first crossing of the other family after S
+  bool split = false;
+  const bool px_primary = nx >= ny;  // P = x family (ties: x first, as the merge)
+  int mP = 0, pQ = 0;
+  double tS = 0.0;
+  if (nx + ny >= kSplitMin) {
+    const int nP = px_primary ? nx : ny, nQ = px_primary ? ny : nx;
+    const int iP0 = px_primary ? ix0 : iy0, sP = px_primary ? sx : sy;
+    const int iQ0 = px_primary ? iy0 : ix0, sQ = px_primary ? sy : sx;
+    const double oP = px_primary ? q.x0t : q.y0t, dP = px_primary ? q.a : q.b;
+    const double oQ = px_primary ? q.y0t : q.x0t, dQ = px_primary ? q.b : q.a;
+    for (int tryk = 0; tryk < 4 && !split; ++tryk) {
+      const int m = nP / 2 + ((tryk & 1) ? -((tryk + 1) / 2) : (tryk / 2));
+      if (m < 1 || m >= nP - 1) continue;
+      const double t = cross_t(iP0 + m * sP, h, oP, dP);
+      // Q position: crossings of Q before S in the merged order are those
+      // with t_Q < t (P = x: x first on equal t) or t_Q <= t (P = y)
+      int p = 0;
+      if (nQ > 0) {
+        const double est = __dmul_rn(__dsub_rn(__dadd_rn(__dadd_rn(h, oQ), __dmul_rn(dQ, t)), (double)iQ0),
+                                     (double)sQ);
+        p = (int)fmin(fmax(ceil(est), 0.0), (double)nQ);
+        // exact adjustment (the sequence is increasing in t); bounded steps
+        for (int it = 0; it < 4 && p > 0; ++it) {
+          const double tb = cross_t(iQ0 + (p - 1) * sQ, h, oQ, dQ);
+          if (px_primary ? tb < t : tb <= t) break;
+          --p;
+        }
+        for (int it = 0; it < 4 && p < nQ; ++it) {
+          const double ta = cross_t(iQ0 + p * sQ, h, oQ, dQ);
+          if (px_primary ? ta >= t : ta > t) break;
+          ++p;
+        }
+        // clean and certain: the Q neighbours of S are on the right sides of
+        // t(S) and farther than kSplitGap from it
+        const double tb = p > 0 ? cross_t(iQ0 + (p - 1) * sQ, h, oQ, dQ) : -INFINITY;
+        const double ta = p < nQ ? cross_t(iQ0 + p * sQ, h, oQ, dQ) : INFINITY;
+        if (!(tb < t - kSplitGap && ta > t + kSplitGap)) continue;
+      }
+      // S itself must lie inside the square (the box filter keeps it)
+      const double fixed = (double)(iP0 + m * sP) - h;
+      const double other = __dadd_rn(__dmul_rn(px_primary ? q.b : q.a, t), px_primary ? q.y0t : q.x0t);
+      if (!(fixed > -h && fixed < h && other > -h && other < h)) continue;
+      split = true;
+      mP = m;
+      pQ = p;
+      tS = t;
+    }
+  }
+  if (part == 1 && !split) return;
+  // ---- loop state of this part
+  int cx = 0, cy = 0, ix = ix0, iy = iy0;
+  int endx = nx, endy = ny;  // positions at which the families stop
+  bool have_pend = false, have_last = false;
+  double px = 0, py = 0, lx = 0, ly = 0;
+  if (split) {
+    const int endP = mP + 1;  // part 0 takes S (position mP) last
+    if (part == 0) {
+      if (px_primary) { endx = endP; endy = pQ; }
+      else { endy = endP; endx = pQ; }
+    } else {
+      if (px_primary) {
+        cx = mP + 1;
+        cy = pQ;
+        px = (double)(ix0 + mP * sx) - h;
+        py = __dadd_rn(__dmul_rn(q.b, tS), q.y0t);
+      } else {
+        cy = mP + 1;
+        cx = pQ;
+        py = (double)(iy0 + mP * sy) - h;
+        px = __dadd_rn(__dmul_rn(q.a, tS), q.x0t);
+      }
+      ix = ix0 + cx * sx;
+      iy = iy0 + cy * sy;
+      have_pend = true;
+    }
+  }
+  double tx = 0.0, ty = 0.0;
+  if (cx < endx) tx = cross_t(ix, h, q.x0t, q.a);
+  if (cy < endy) ty = cross_t(iy, h, q.y0t, q.b);
+  while (cx < endx || cy < endy) {
+    // the merge step of trace_segments, over this part's positions
+    const bool takex = cy >= endy || (cx < endx && tx <= ty);
+    const double t = takex ? tx : ty;
+    const double fixed = (double)(takex ? ix : iy) - h;
+    const double other = __dadd_rn(__dmul_rn(takex ? q.b : q.a, t), takex ? q.y0t : q.x0t);
+    const double xx = takex ? fixed : other;
+    const double yy = takex ? other : fixed;
+    if (takex) {
+      ++cx;
+      ix += sx;
+    } else {
+      ++cy;
+      iy += sy;
+    }
+    const double tn = __ddiv_rn(__dsub_rn((double)(takex ? ix : iy) - h, takex ? q.x0t : q.y0t),
+                                takex ? q.a : q.b);
+    if (takex) tx = tn;
+    else ty = tn;
+    if (!(xx >= -h && xx <= h && yy >= -h && yy <= h)) continue;
+    if (have_pend) {
+      const bool close = fabs(__dsub_rn(xx, px)) <= 1e-10 && fabs(__dsub_rn(yy, py)) <= 1e-10;
+      if (!close) {
+        if (have_last) {
+          const double dx = __dsub_rn(px, lx), dy = __dsub_rn(py, ly);
+          const double len = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+          const double xm = __dadd_rn(__dmul_rn(0.5, __dadd_rn(lx, px)), h);
+          const double ym = __dadd_rn(__dmul_rn(0.5, __dadd_rn(ly, py)), h);
+          seg((int)floor(xm) * N + (N - 1 - (int)floor(ym)), len);
+        }
+        lx = px;
+        ly = py;
+        have_last = true;
+      }
+    }
+    px = xx;
+    py = yy;
+    have_pend = true;
+  }
+  if (have_pend && have_last) {
+    const double dx = __dsub_rn(px, lx), dy = __dsub_rn(py, ly);
+    const double len = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+    const double xm = __dadd_rn(__dmul_rn(0.5, __dadd_rn(lx, px)), h);
+    const double ym = __dadd_rn(__dmul_rn(0.5, __dadd_rn(ly, py)), h);
+    seg((int)floor(xm) * N + (N - 1 - (int)floor(ym)), len);
+  }
+}
+
+// trace_entries over one part of a split ray (trace_segments_part): the
+// merged entries of the whole ray are exactly the union of the two parts'.
+template <class Emit>
+__device__ __forceinline__ void trace_entries_part(int N, const Ray &q, bool exclude_top_right, int part,
+                                                   Emit &&emit) {
+  MergeWindow w;
+  trace_segments_part(N, q, exclude_top_right, part, [&](int col, double len) { w.add(col, len, emit); });
+  w.flush(emit);
 }
 
 // sphericaltomo (testprobs/sphericaltomo.m:203-224): sample k of a circle of
@@ -254,6 +450,18 @@ __device__ __forceinline__ void row_entries(const RayGeom &g, int64_t r, bool ex
     return;
   }
   trace_entries(g.N, ray_of(g, r), exclude_top_right, emit);
+}
+
+// row_entries for one of the two threads that share row r (part 0 or 1):
+// straight rays are split by trace_entries_part; a circle goes to part 0.
+template <class Emit>
+__device__ __forceinline__ void row_entries_part(const RayGeom &g, int64_t r, bool exclude_top_right, int part,
+                                                 Emit &&emit) {
+  if (g.kind == GEO_SPHERE) {
+    if (part == 0) row_entries(g, r, exclude_top_right, emit);
+    return;
+  }
+  trace_entries_part(g.N, ray_of(g, r), exclude_top_right, part, emit);
 }
 
 }  // namespace airt

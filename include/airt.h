@@ -392,6 +392,11 @@ int airt_test_inject_stall(int on);
  * library succeed and the one after fails as an out-of-memory error
  * (AIRT_ERR_OOM, message "injected allocation failure"); k < 0 turns it off. */
 int airt_test_fail_alloc(int after);
+/* airt_test_split_trace: for every ray of a straight-ray geometry problem,
+ * compare the entries of the whole trace with those of the two halves the
+ * matrix-free kernels trace on two threads (count and an order-independent
+ * hash); *mismatched = rays that differ, *split = rays that were split. */
+int airt_test_split_trace(airt_problem *h, int64_t *mismatched, int64_t *split);
 
 /* ---- instrumentation ------------------------------------------------------- */
 /* When on, each SIRT kernel launch is bracketed by CUDA events on the problem

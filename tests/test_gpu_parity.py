@@ -694,3 +694,27 @@ def test_cart_residual_in_global_memory():
     X, info = airt.columnaction(A, b, [2, 4], None, opts)
     assert relerr(X, Xo) <= CART_TOL
     assert info["finaliter"] == io["finaliter"] == 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("geo", ["parallel_c2", "parallel_odd", "fan", "seismic"])
+def test_split_trace_has_the_whole_trace_entries(geo):
+    """The matrix-free kernels trace a long ray on two threads, each from one
+    side of a clean crossing near its middle.  For every ray, the union of
+    the two halves' merged entries must be the whole trace's entries, pixel
+    and FP64 value bits (count plus an order-independent hash), and most
+    long rays must actually be split."""
+    import ctypes as C
+    from airtoolsii_b200._lib import lib
+    if geo == "parallel_c2":
+        A, *_ = airt.paralleltomo(512, np.arange(360) * 0.5, 724, None, 0, 0)
+    elif geo == "parallel_odd":
+        A, *_ = airt.paralleltomo(255, np.arange(0.0, 180.0, 0.7), 301, None, 0, 0)
+    elif geo == "fan":
+        A, *_ = airt.fanlineartomo(384, np.arange(0.0, 360.0, 1.0), None, None, None, None, 0, 0)
+    else:
+        A, *_ = airt.seismictomo(256, None, None, 0, 0)
+    bad, split = C.c_int64(-1), C.c_int64(0)
+    assert lib().airt_test_split_trace(A.handle, C.byref(bad), C.byref(split)) == 0
+    assert bad.value == 0
+    assert split.value > A.m // 2, (split.value, A.m)
