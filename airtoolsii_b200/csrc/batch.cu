@@ -16,8 +16,8 @@
 // read through the row->instance and column->instance maps; stopped
 // instances skip their rows and columns entirely.  Rows and columns are cut
 // into tiles of 2048 segments; a tile's lane class follows its mean segment
-// length (<= 16, <= 128, > 128 nonzeros), so instances of any size mix in any
-// order still give at most three launches per direction.  An autotuner times
+// length (<= 16, 48, 96, 128, > 128 nonzeros), so instances of any size mix in
+// any order still give at most five launches per direction.  An autotuner times
 // the candidate lane widths on every class once.  A chunk of iterations is
 // captured as one CUDA graph (all loop state lives in device memory).
 // Kaczmarz runs one CTA per instance over a level schedule of the
@@ -44,16 +44,16 @@ struct InstGeom {
 // Segment tiles of the active-tile lists: 2048 rows or columns, in
 // kClasses lane classes by mean segment length.
 constexpr int kTileShift = 11;
-constexpr int kClasses = 3;
+constexpr int kClasses = 5;
 
 // Per-direction tile bookkeeping: class of every tile, tiles per class, and
 // the region of each class in the active list.
 struct TileSet {
   int ntiles = 0;
   DevBuf<int> cls, list;
-  int count[kClasses] = {0, 0, 0};
-  int off[kClasses] = {0, 0, 0};
-  int lanes[kClasses] = {2, 4, 8};
+  int count[kClasses] = {};
+  int off[kClasses] = {};
+  int lanes[kClasses] = {2, 4, 4, 8, 8};
 };
 
 struct ClassOffsets {
@@ -102,8 +102,8 @@ struct Batch {
   DevBuf<double> ncp_tw, ncp_pk, ncp_ccol, ncp_dk;
   // the lane classes of one direction run side by side: two more streams,
   // forked from and joined to P.stream by events (graph-capturable)
-  cudaStream_t aux[kClasses - 1] = {nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join[kClasses - 1] = {nullptr, nullptr};
+  cudaStream_t aux[kClasses - 1] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kClasses - 1] = {};
   ~Batch() {
     for (int i = 0; i < kClasses - 1; ++i) {
       if (aux[i]) cudaStreamDestroy(aux[i]);
@@ -309,7 +309,7 @@ __global__ void k_tile_class(int ntiles, int64_t nseg, const int64_t *__restrict
   const int64_t s0 = (int64_t)t << kTileShift;
   const int64_t s1 = min(nseg, s0 + ((int64_t)1 << kTileShift));
   const double avg = (double)(ptr[s1] - ptr[s0]) / (double)(s1 - s0);
-  cls[t] = avg > 128.0 ? 2 : avg > 16.0 ? 1 : 0;
+  cls[t] = avg > 128.0 ? 4 : avg > 96.0 ? 3 : avg > 48.0 ? 2 : avg > 16.0 ? 1 : 0;
 }
 
 // List the tiles (2^kTileShift segments each) that hold at least one
