@@ -53,10 +53,11 @@ def parse():
     ap.add_argument("--no-extra", action="store_true", help="skip the C2-methods / C3 / C4 legs")
     ap.add_argument("--warm-heldout", type=int, default=1000, help="held-out seeds of the time-to-DP leg")
     ap.add_argument("--warm-batch", type=int, default=250, help="instances per batched solve")
-    ap.add_argument("--leg", choices=["kaczmarz", "multi"], default=None,
+    ap.add_argument("--leg", choices=["kaczmarz", "multi", "batch"], default=None,
                     help="only one small leg, for profiling captures: 'kaczmarz' = 3 kaczmarz "
                          "sweeps on paralleltomo N=256, 180 angles; 'multi' = cimmino to the DP "
-                         "stop on 250 right-hand sides of paralleltomo N=256, 60 angles")
+                         "stop on 250 right-hand sides of paralleltomo N=256, 60 angles; 'batch' "
+                         "= 20 cimmino iterations on 40 N=128 instances of the 512-instance batch")
     ap.add_argument("--mf-only", action="store_true",
                     help="only the matrix-free projector leg: --iters iterations of --method on the "
                          "matrix-free operator of the (--small) paralleltomo workload (profiling)")
@@ -471,7 +472,10 @@ def warm_leg(a):
 def small_leg(which):
     """One small workload for profiling captures; prints one JSON line with
     its device time.  kaczmarz: paralleltomo N=256, 180 angles, 10-ellipse
-    phantom, 1% noise, 3 sweeps after a 1-sweep untimed pass.  multi: the
+    phantom, 1% noise, 3 sweeps after a 1-sweep untimed pass.  batch: the 40
+    N=128 instances (30-180 angles) of the 512-instance batch, noise-free
+    sinograms, 20 cimmino iterations with no stop rule after a 5-iteration
+    untimed pass.  multi: the
     warm-start geometry (N=256, 60 angles) with 250 seeded sinograms at 2%
     noise, cimmino to the per-instance DP stop (tau 1.02) on the
     multi-right-hand-side engine, after an untimed pass."""
@@ -485,6 +489,28 @@ def small_leg(which):
         airt.kaczmarz(A, b, [1])
         X, info = airt.kaczmarz(A, b, [3])
         print(json.dumps({"leg": which, "ms_per_sweep": round(info["gpu_ms"] / 3, 4)}), flush=True)
+        return
+    if which == "batch":
+        from airtoolsii_b200.batch import ParallelBatch
+        rng = np.random.default_rng(4)
+        Ns = rng.choice([64, 96, 128, 192, 256], 512)
+        nAs = rng.integers(30, 181, 512)
+        sel = np.nonzero(Ns == 128)[0][:40]
+        B = ParallelBatch([128] * len(sel), [np.arange(nAs[k]) * (180.0 / nAs[k]) for k in sel])
+        xs = [airt.random_ellipses(128, 10, seed=10_000 + int(k)) for k in sel]
+        dx = torch.from_numpy(np.concatenate(xs)).cuda()
+        db = torch.empty(B.m, dtype=torch.float64, device="cuda")
+        B.apply_device(dx.data_ptr(), db.data_ptr())
+        dxo = torch.empty(B.n, dtype=torch.float64, device="cuda")
+        rho = B.rho("cimmino")
+        B.sirt_device("cimmino", db.data_ptr(), dxo.data_ptr(), 5, rho=rho)
+        info = B.sirt_device("cimmino", db.data_ptr(), dxo.data_ptr(), 20, rho=rho)
+        nz = B.inst_nnz()
+        mi, ni = np.diff(B.row_off), np.diff(B.col_off)
+        byts = 20 * float(np.sum(16 * nz + 16 * mi + 16 * ni))
+        print(json.dumps({"leg": which, "instances": len(sel), "nnz": int(B.nnz),
+                          "ms_per_iteration": round(info["gpu_ms"] / 20, 4),
+                          "GBps_model": round(byts / (info["gpu_ms"] / 1e3) / 1e9, 1)}), flush=True)
         return
     A, *_ = airt.paralleltomo(256, np.arange(60) * 3.0)
     K = 250
