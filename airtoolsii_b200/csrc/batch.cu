@@ -44,6 +44,9 @@ struct InstGeom {
 // Segment tiles of the active-tile lists: 2048 rows or columns, in
 // kClasses lane classes by mean segment length.
 constexpr int kTileShift = 11;
+// Resident CTAs per SM of the batch walkers (register budget 48 per thread):
+// they are latency bound, so resident warps set their bandwidth.
+constexpr int kBatchCtas = 5;
 constexpr int kClasses = 5;
 
 // Per-direction tile bookkeeping: class of every tile, tiles per class, and
@@ -218,7 +221,7 @@ struct BFwd {
 // Residual pass; with idx16 (16-bit local column indices, voff = the
 // instances' first columns) the nonzeros stream at 6 bytes instead of 8.
 template <int L>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, kBatchCtas)
     k_batch_fwd(int64_t nseg, const int *__restrict__ tiles, const int *__restrict__ ntiles,
                 const int64_t *__restrict__ rp, const int *__restrict__ ci, const float *__restrict__ rv,
                 const float *__restrict__ x32, BFwd o, const uint16_t *__restrict__ idx16,
@@ -261,7 +264,7 @@ struct BUpd {
 // Update pass; idx16 / voff as in k_batch_fwd (16-bit local row indices,
 // the instances' first rows).
 template <int L>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, kBatchCtas)
     k_batch_bwd(int64_t nseg, const int *__restrict__ tiles, const int *__restrict__ ntiles,
                 const int64_t *__restrict__ cp, const int *__restrict__ ri, const float *__restrict__ cv,
                 const float *__restrict__ mr32, BUpd u, const uint16_t *__restrict__ idx16,
@@ -597,7 +600,7 @@ void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullp
   if (B.rt.count[c] == 0) return;
   cudaStream_t s = st ? st : P.stream;
   const int64_t ns = P.m;
-  const unsigned g = grid_for((int64_t)B.rt.count[c] * (1 << kTileShift) * L, 256, 4);
+  const unsigned g = grid_for((int64_t)B.rt.count[c] * (1 << kTileShift) * L, 256, kBatchCtas);
   const int *tl = B.rt.list.p + B.rt.off[c], *cnt = B.tcount.p + c;
   // 16-bit indices for the long-segment class only: with segments of 128
   // nonzeros or fewer the 8-aligned head and tail (up to 7 elements each,
@@ -623,7 +626,7 @@ void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = null
   if (B.ct.count[c] == 0) return;
   cudaStream_t s = st ? st : P.stream;
   const int64_t ns = P.n;
-  const unsigned g = grid_for((int64_t)B.ct.count[c] * (1 << kTileShift) * L, 256, 4);
+  const unsigned g = grid_for((int64_t)B.ct.count[c] * (1 << kTileShift) * L, 256, kBatchCtas);
   const int *tl = B.ct.list.p + B.ct.off[c], *cnt = B.tcount.p + kClasses + c;
   const uint16_t *i16 = c == kClasses - 1 ? B.ri16.p : nullptr;  // as in launch_bfwd
   switch (L) {
