@@ -236,21 +236,23 @@ __global__ void k_pool_back(int B, int H, int W, int C, const __nv_bfloat16 *__r
 
 // cat[..., 0:C1] = up2(prev) (prev at H/2 x W/2), cat[..., C1:C1+C2] = skip
 // cat = [nearest-2x(prev) | skip] along channels, 8 channels (16 bytes) per
-// thread; C1 and C2 are multiples of 8.
-__global__ void k_up_concat(int B, int H, int W, int C1, int C2, const __nv_bfloat16 *__restrict__ prev,
+// thread; C1 and C2 are multiples of 8.  Block x is one output row (b, h),
+// block y a run of that row's W * C8 16-byte groups, so a thread's indices
+// take one division instead of a chain of them per group.
+__global__ void k_up_concat(int H, int W, int C1, int C2, const __nv_bfloat16 *__restrict__ prev,
                             const __nv_bfloat16 *__restrict__ skip, __nv_bfloat16 *__restrict__ cat) {
-  const int C8 = (C1 + C2) / 8, c18 = C1 / 8;
-  AIRT_FOR32(t, B * H * W * C8) {
-    const int c8 = t % C8, p = t / C8;
-    uint4 v;
-    if (c8 < c18) {
-      const int w = p % W, h = (p / W) % H, b = p / (W * H);
-      v = reinterpret_cast<const uint4 *>(prev)[((b * (H / 2) + h / 2) * (W / 2) + w / 2) * c18 + c8];
-    } else {
-      v = reinterpret_cast<const uint4 *>(skip)[p * (C2 / 8) + (c8 - c18)];
-    }
-    reinterpret_cast<uint4 *>(cat)[t] = v;
-  }
+  const int C8 = (C1 + C2) / 8, c18 = C1 / 8, c28 = C2 / 8;
+  const int x = blockIdx.y * blockDim.x + threadIdx.x;
+  if (x >= W * C8) return;
+  const int r = (int)blockIdx.x, bi = r / H, h = r - bi * H;
+  const int64_t row = r, b = bi;
+  const int w = x / C8, c8 = x - w * C8;
+  uint4 v;
+  if (c8 < c18)
+    v = reinterpret_cast<const uint4 *>(prev)[((b * (H / 2) + h / 2) * (W / 2) + w / 2) * c18 + c8];
+  else
+    v = reinterpret_cast<const uint4 *>(skip)[(row * W + w) * c28 + (c8 - c18)];
+  reinterpret_cast<uint4 *>(cat)[row * W * C8 + x] = v;
 }
 
 // Backward of [nearest-2x(prev) | skip]: dskip += its channels of dcat,
@@ -946,8 +948,9 @@ void unet_forward_body(UNet &U, int B) {
   for (int l = U.levels - 2; l >= 0; --l) {
     Tensor *prev = (l == U.levels - 2) ? U.eb[U.levels - 1] : U.db[l + 1];
     Tensor *cat = U.cat[l];
-    k_up_concat<<<gsz((int64_t)B * cat->H * cat->W * cat->C / 8), kT, 0, U.s>>>(
-        B, cat->H, cat->W, prev->C, U.eb[l]->C, prev->y.p, U.eb[l]->y.p, cat->y.p);
+    const dim3 ug((unsigned)((int64_t)B * cat->H), (unsigned)((cat->W * (cat->C / 8) + kT - 1) / kT));
+    k_up_concat<<<ug, kT, 0, U.s>>>(cat->H, cat->W, prev->C, U.eb[l]->C, prev->y.p, U.eb[l]->y.p,
+                                    cat->y.p);
     conv_forward(U, U.convs[ci++], B);
     conv_forward(U, U.convs[ci++], B);
   }
