@@ -602,12 +602,13 @@ void launch_bfwd(Batch &B, int c, int L, const BFwd &o, const float *x32 = nullp
   const int64_t ns = P.m;
   const unsigned g = grid_for((int64_t)B.rt.count[c] * (1 << kTileShift) * L, 256, kBatchCtas);
   const int *tl = B.rt.list.p + B.rt.off[c], *cnt = B.tcount.p + c;
-  // 16-bit indices for the long-segment class only: with segments of 128
-  // nonzeros or fewer the 8-aligned head and tail (up to 7 elements each,
-  // element-wise) cost more than the index bytes save (measured on the
-  // 512-instance batch: all-active iterations 5 % faster, the short-segment
-  // tail 5 % slower when every class used them)
-  const uint16_t *i16 = c == kClasses - 1 ? B.ci16.p : nullptr;
+  // 16-bit indices for the two longest-segment classes (mean above 96
+  // nonzeros) only: on shorter segments the 8-aligned head and tail (up to 7
+  // elements each, element-wise) cost more than the index bytes save
+  // (measured on the 512-instance batch: all-active iterations 5 % faster,
+  // the short-segment tail 5 % slower when every class used them; the
+  // 97-128 class as well as the longest: the whole batch 0.8 % faster)
+  const uint16_t *i16 = c >= kClasses - 2 ? B.ci16.p : nullptr;
   switch (L) {
 #define AIRT_F(LV) \
   k_batch_fwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.rp.p, P.ci.p, P.rv.p, x32, o, i16, B.d_col_off.p)
@@ -628,7 +629,7 @@ void launch_bbwd(Batch &B, int c, int L, const BUpd &u, const float *mr32 = null
   const int64_t ns = P.n;
   const unsigned g = grid_for((int64_t)B.ct.count[c] * (1 << kTileShift) * L, 256, kBatchCtas);
   const int *tl = B.ct.list.p + B.ct.off[c], *cnt = B.tcount.p + kClasses + c;
-  const uint16_t *i16 = c == kClasses - 1 ? B.ri16.p : nullptr;  // as in launch_bfwd
+  const uint16_t *i16 = c >= kClasses - 2 ? B.ri16.p : nullptr;  // as in launch_bfwd
   switch (L) {
 #define AIRT_B(LV) \
   k_batch_bwd<LV><<<g, 256, 0, s>>>(ns, tl, cnt, P.cp.p, P.ri.p, P.cv.p, mr32, u, i16, B.d_row_off.p)
